@@ -1,0 +1,323 @@
+"""Benchmark of the GPUSimulators time-step path on B200.
+
+Workload: KP07_dimsplit shallow water on a 4096 x 4096 FP32 grid, circular dam
+break (h = 1 inside a seeded radius R ~ U(0.1, 0.3) * width, 0.1 outside,
+hu = hv = 0, g = 9.81, reflective walls), stepped with simulate()'s CFL
+schedule (dt recomputed every 100 steps).  One bench step is one full time
+step (two stage-kernel launches).  The state (2 x 201 MB) is larger than L2,
+so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mine|reference]
+
+N > 1 (launched with torch.distributed.run) runs one independent replica per
+GPU (the path does not shard: weak scaling, no collective on the data path).
+``--impl reference`` times the reference algorithm on the host CPU (the CPU
+restatement of the reference kernels; the reference itself has no CPU path),
+on rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX = NY = 4096  # may be overridden by --size (profiling captures use a smaller grid)
+SCHEME = "KP07_dimsplit"
+BYTES_PER_CELL_SUBSTEP = 24  # 3 FP32 variables read + written per stage launch
+SUBSTEPS = 2
+# FP32 operations per cell-substep of the algorithm (count of the restated
+# formulas for KP07_dimsplit: reconstruction, predictor, central-upwind flux and
+# update along both axes; see profiles/kp07_dimsplit_flops.md).
+ALG_FLOP_PER_CELL_SUBSTEP = None
+PROFILE_JSON = os.path.join(ROOT, "profiles", "kp07_dimsplit_stage_4096.json")
+
+
+def dam_break_4096(seed=0):
+    rng = np.random.default_rng(seed)
+    R = rng.uniform(0.1, 0.3) * NX
+    y, x = np.mgrid[0:NY, 0:NX] + 0.5
+    r = np.hypot(x - NX / 2.0, y - NY / 2.0)
+    h = np.where(r < R, 1.0, 0.1).astype(np.float32)
+    z = np.zeros_like(h)
+    return h, z, z.copy(), float(R)
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML during the timed region."""
+
+    REASONS = {
+        0x0000000000000004: "sw_power_cap",
+        0x0000000000000008: "hw_slowdown",
+        0x0000000000000020: "sw_thermal_slowdown",
+        0x0000000000000040: "hw_thermal_slowdown",
+        0x0000000000000080: "hw_power_brake_slowdown",
+    }
+
+    def __init__(self, device_index=0, period=0.005):
+        self.period = period
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._ok = False
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+            self._ok = True
+        except Exception:
+            self._ok = False
+
+    def _run(self):
+        nv = self._nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                mask = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                for bit, name in self.REASONS.items():
+                    if mask & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self._ok:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self._ok:
+            self._stop.set()
+            self._t.join()
+
+    def summary(self):
+        if not self._ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unavailable"]}
+        return {"sm_mhz": float(statistics.median(self.samples)), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0}, "fallback"
+
+
+def load_profile():
+    try:
+        with open(PROFILE_JSON) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def cpu_baseline_leg(steps=3):
+    """FP64 CPU oracle on the host cores: a bounded sample of the workload."""
+    from oracle.oracle import OracleSim
+
+    h, hu, hv, _ = dam_break_4096()
+    cores = len(os.sched_getaffinity(0))
+    sim = OracleSim(SCHEME, [h, hu, hv], NX, NY, 1.0, 1.0, 9.81, dtype=np.float64, nthreads=cores)
+    dt = sim.computeDt() * 0.9
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sim.step(dt)
+    el = time.perf_counter() - t0
+    return {"value": NX * NY * steps / el, "unit": "cell-updates/s", "cores": cores, "kind": "port",
+            "sample": "%d steps of the full 4096x4096 grid, FP64 C restatement (OpenMP, %d threads)" % (steps, cores)}
+
+
+def run_reference(args, rank, world):
+    """The reference algorithm on the host CPU (FP32 oracle), rank 0 only."""
+    if rank != 0:
+        return None
+    from oracle.oracle import OracleSim
+
+    cores = len(os.sched_getaffinity(0))
+    rows = 256  # bounded sample: a 4096 x 256 stripe of the grid per step
+    h, hu, hv, _ = dam_break_4096()
+    r0 = NY // 2 - rows // 2
+    q = [a[r0:r0 + rows].copy() for a in (h, hu, hv)]
+    sim = OracleSim(SCHEME, q, NX, rows, 1.0, 1.0, 9.81, dtype=np.float32, nthreads=cores)
+    dt = sim.computeDt() * 0.9
+    for _ in range(args.warmup):
+        sim.step(dt)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sim.step(dt)
+    el = time.perf_counter() - t0
+    v = NX * rows * args.steps / el
+    sample = "each step: one KP07_dimsplit time step of a 4096x%d stripe of the dam break, FP32, %d threads" % (
+        rows, cores)
+    return {
+        "metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+        "config": {"workload": "KP07_dimsplit 4096x4096 circular dam break (CPU sample 4096x%d)" % rows,
+                   "scheme": SCHEME, "nx": NX, "ny": NY, "parallelism": "host threads"},
+        "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def run_mine(args, rank, world, local_rank):
+    import torch
+
+    from finitevolumegpu_b200 import CudaContext, KP07_dimsplit, _lib
+
+    dist = world > 1
+    ctx = CudaContext.CudaContext(device=local_rank, autotuning=True)
+    h, hu, hv, R = dam_break_4096(seed=rank)
+    sim = KP07_dimsplit.KP07_dimsplit(ctx, h, hu, hv, NX, NY, 1.0, 1.0, 9.81)
+    sim.advance(args.warmup)
+    info = sim.tile_info()
+
+    def barrier():
+        if dist:
+            torch.distributed.barrier()
+        torch.cuda.synchronize(local_rank)
+
+    clocks = ClockSampler(local_rank)
+    barrier()
+    t0 = time.perf_counter()
+    with clocks:
+        sim.advance(args.steps)  # CUDA events on the simulation stream around the K steps
+        barrier()
+    wall = time.perf_counter() - t0
+    dev_ms_per_step = sim.last_advance_ms()
+    T = dev_ms_per_step * args.steps / 1e3
+    if dist:
+        t = torch.tensor([T], dtype=torch.float64, device="cuda:%d" % local_rank)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        T = float(t.item())
+    cells = NX * NY
+    value = world * cells * args.steps / T
+    launches = args.steps * info["launches_per_step"]
+
+    # roofline of the dominant kernel (the stage kernel)
+    pk, pk_kind = peaks()
+    launch_s = T / launches
+    alg_bytes = BYTES_PER_CELL_SUBSTEP * cells
+    achieved = alg_bytes / launch_s / 1e9
+    prof = load_profile()
+    traffic = prof.get("dram_bytes_per_launch")
+    roof = {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / pk["hbm_gbs"], "traffic": traffic, "peak_kind": pk_kind,
+            "kernel": "dimsplit_stage_kernel<KP07_DIMSPLIT,%d,%d,%d>" % (info["tile_w"], info["tile_h"], info["threads"]),
+            "algorithmic_bytes_per_launch": alg_bytes}
+    if prof.get("fp32_flop_per_launch"):
+        clk = clocks.summary().get("sm_mhz") or 1965.0
+        fp32_peak = 148 * 128 * 2 * clk * 1e6 / 1e12
+        ach = prof["fp32_flop_per_launch"] / launch_s / 1e12
+        roof["fp32"] = {"achieved_tflops": ach, "peak_tflops_at_clock": fp32_peak, "frac": ach / fp32_peak,
+                        "note": "executed FP32 ops per launch from ncu; peak = 148 SM x 128 lanes x 2 x SM clock"}
+
+    result = None
+    if rank == 0:
+        result = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": T / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "KP07_dimsplit 4096x4096 circular dam break (R=%.0f cells), reflective walls, "
+                                   "simulate() dt schedule, cfl_scale 0.9" % R,
+                       "scheme": SCHEME, "nx": NX, "ny": NY, "parallelism": "replicas" if world > 1 else "single",
+                       "tile": info, "l2": "state 403 MB > 126 MB L2; no flush"},
+            "roofline": roof,
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+            "wall_s_timed_region": wall,
+        }
+    # end-to-end through the public API: pinned upload, K steps, download
+    e2e = None
+    if rank == 0 and not args.no_e2e:
+        nbytes = cells * 4
+        L = _lib.lib()
+        bufs = []
+        import ctypes
+
+        def pinned(shape):
+            p = ctypes.c_void_p()
+            _lib.check(L.fv_host_alloc(ctypes.byref(p), nbytes))
+            bufs.append(p)
+            arr = np.ctypeslib.as_array((ctypes.c_float * (cells)).from_address(p.value)).reshape(shape)
+            return arr
+
+        hin = [pinned((NY, NX)) for _ in range(3)]
+        for a, b in zip(hin, (h, hu, hv)):
+            a[:] = b
+        hout = [pinned((NY, NX)) for _ in range(3)]
+        torch.cuda.synchronize(local_rank)
+        t0 = time.perf_counter()
+        s2 = KP07_dimsplit.KP07_dimsplit(ctx, hin[0], hin[1], hin[2], NX, NY, 1.0, 1.0, 9.81)
+        s2.advance(args.steps)
+        for v in range(3):
+            s2._download_var(v, hout[v])
+        e2e_s = time.perf_counter() - t0
+        del s2
+        for p in bufs:
+            L.fv_host_free(p)
+        e2e = {"value": cells * args.steps / e2e_s, "unit": "cell-updates/s",
+               "h2d_bytes_per_step": 3 * nbytes / args.steps, "d2h_bytes_per_step": 3 * nbytes / args.steps,
+               "what": "constructor with pinned host upload + %d steps + download of the final state" % args.steps}
+        result["e2e"] = e2e
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline_leg()
+    return result
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--size", type=int, default=4096, help="grid side (the benchmark workload is 4096)")
+    args = ap.parse_args()
+    global NX, NY
+    NX = NY = args.size
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        res = run_reference(args, rank, world)
+        if res is not None:
+            print(json.dumps(res), flush=True)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    res = run_mine(args, rank, world, local_rank)
+    if res is not None:
+        print(json.dumps(res), flush=True)
+    if world > 1:
+        import torch
+
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,29 @@
+"""HLL: first-order HLL scheme with dimensional splitting -- the counterpart of GPUSimulators/HLL.py.
+
+Constructor arguments and defaults follow GPUSimulators/HLL.py:51-84;
+one step is 1 launch(es) of the sm_100a stage kernel in libfvgpu.so.
+"""
+
+import numpy as np
+
+from . import Simulator
+from .Simulator import BoundaryCondition
+
+
+class HLL(Simulator.BaseSimulator):
+    _scheme = "HLL"
+    _gc = 1
+
+    def __init__(self,
+                 context,
+                 h0, hu0, hv0,
+                 nx, ny,
+                 dx, dy,
+                 g,
+                 cfl_scale=0.9,
+                 boundary_conditions=BoundaryCondition(),
+                 block_width=16, block_height=16):
+        super().__init__(context, nx, ny, dx, dy, boundary_conditions, cfl_scale, 1, block_width,
+                         block_height)
+        self.g = np.float32(g)
+        self._create([h0, hu0, hv0], g=g)

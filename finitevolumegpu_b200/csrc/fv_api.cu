@@ -1,0 +1,633 @@
+// Host runtime and C ABI of libfvgpu.so (declared in include/fvgpu.h).
+//
+// A simulation owns two state buffers per conserved variable (u0/u1 of the
+// reference, GPUSimulators/Common.py:741-755), a device control block with t,
+// nt, dt and the buffer parity, one TMA descriptor per buffer and variable,
+// and CUDA graphs of 1 and 16 steps.  simulate() reproduces the reference's
+// host loop (GPUSimulators/Simulator.py:176-217) with one synchronisation per
+// 100-step dt interval, where the reference reads back min(cfl_data).
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/fvgpu.h"
+#include "fv_stage.cuh"
+
+using fv::SimCtl;
+using fv::StageArgs;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define FV_CK(call)                                                                          \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) return fail(FV_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+#define FV_TRY(call)              \
+    do {                          \
+        int r_ = (call);          \
+        if (r_ != FV_OK) return r_; \
+    } while (0)
+
+using KernelFn = void (*)(StageArgs);
+
+struct KEntry {
+    int scheme;
+    int W, H, NT;
+    bool split;
+    KernelFn fn;
+};
+
+// Tile configurations per scheme; the first entry of a scheme is its default.
+const KEntry kTable[] = {
+    {FV_KP07_DIMSPLIT, 124, 60, 256, true, fv::dimsplit_stage_kernel<fv::KP07_DIMSPLIT, 124, 60, 256>},
+    {FV_KP07_DIMSPLIT, 124, 28, 128, true, fv::dimsplit_stage_kernel<fv::KP07_DIMSPLIT, 124, 28, 128>},
+    {FV_HLL2, 124, 60, 256, true, fv::dimsplit_stage_kernel<fv::HLL2, 124, 60, 256>},
+    {FV_HLL2, 124, 28, 128, true, fv::dimsplit_stage_kernel<fv::HLL2, 124, 28, 128>},
+    {FV_WAF, 124, 60, 256, true, fv::dimsplit_stage_kernel<fv::WAF, 124, 60, 256>},
+    {FV_WAF, 124, 28, 128, true, fv::dimsplit_stage_kernel<fv::WAF, 124, 28, 128>},
+    {FV_FORCE, 124, 60, 256, true, fv::dimsplit_stage_kernel<fv::FORCE, 124, 60, 256>},
+    {FV_FORCE, 124, 28, 128, true, fv::dimsplit_stage_kernel<fv::FORCE, 124, 28, 128>},
+    {FV_HLL, 124, 60, 256, true, fv::dimsplit_stage_kernel<fv::HLL, 124, 60, 256>},
+    {FV_HLL, 124, 28, 128, true, fv::dimsplit_stage_kernel<fv::HLL, 124, 28, 128>},
+    {FV_EE2D_KP07_DIMSPLIT, 124, 28, 128, true, fv::dimsplit_stage_kernel<fv::EE2D, 124, 28, 128>},
+    {FV_EE2D_KP07_DIMSPLIT, 124, 60, 256, true, fv::dimsplit_stage_kernel<fv::EE2D, 124, 60, 256>},
+    {FV_LXF, 124, 28, 256, false, fv::unsplit_stage_kernel<fv::LXF, 124, 28, 256>},
+    {FV_LXF, 124, 12, 256, false, fv::unsplit_stage_kernel<fv::LXF, 124, 12, 256>},
+    {FV_KP07, 124, 28, 256, false, fv::unsplit_stage_kernel<fv::KP07, 124, 28, 256>},
+    {FV_KP07, 124, 12, 256, false, fv::unsplit_stage_kernel<fv::KP07, 124, 12, 256>},
+};
+constexpr int kNumEntries = sizeof(kTable) / sizeof(kTable[0]);
+
+int scheme_nv(int scheme) { return scheme == FV_EE2D_KP07_DIMSPLIT ? 4 : 3; }
+int scheme_ghost(int scheme) { return (scheme == FV_LXF || scheme == FV_FORCE || scheme == FV_HLL) ? 1 : 2; }
+
+size_t entry_smem(const KEntry& e) {
+    const size_t tile = (size_t)(e.W + 8) * (e.H + 4) * sizeof(float);
+    if (e.split) return scheme_nv(e.scheme) * tile;
+    return 3 * tile + 3 * (size_t)e.H * (e.W + 1) * sizeof(float);
+}
+
+const KEntry* find_entry(int scheme, int cfg) {
+    int k = 0;
+    for (int i = 0; i < kNumEntries; ++i) {
+        if (kTable[i].scheme != scheme) continue;
+        if (k == cfg) return &kTable[i];
+        ++k;
+    }
+    return nullptr;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// Host replica of the reference's initial CFL estimate, in float32 with numpy's
+// NaN-propagating np.min (e.g. GPUSimulators/KP07_dimsplit.py:103-105).
+float initial_cfl(const float* const* v, size_t n, float dx, float dy, float c2) {
+    float mx = INFINITY, my = INFINITY;
+    bool nan_x = false, nan_y = false;
+    for (size_t i = 0; i < n; ++i) {
+        const float h = v[0][i];
+        const float c = std::sqrt(c2 * h);
+        const float ax = dx / (std::fabs(v[1][i] / h) + c);
+        const float ay = dy / (std::fabs(v[2][i] / h) + c);
+        if (std::isnan(ax)) nan_x = true; else if (ax < mx) mx = ax;
+        if (std::isnan(ay)) nan_y = true; else if (ay < my) my = ay;
+    }
+    if (nan_x) mx = NAN;
+    if (nan_y) my = NAN;
+    return (my < mx) ? my : mx;  // Python min(dt_x, dt_y)
+}
+
+__global__ void sum_rows_kernel(const float* __restrict__ a, int nx, int pitch, double* __restrict__ out) {
+    // one CTA per interior row, fixed reduction order
+    __shared__ double red[256 / 32];
+    const float* row = a + fv::cell_index(blockIdx.x, 0, pitch);
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < nx; i += 256) acc += (double)row[i];
+    const double r = fv::block_sum<256>(acc, red);
+    if (threadIdx.x == 0) out[blockIdx.x] = r;
+}
+
+__global__ void sum_final_kernel(const double* __restrict__ part, int n, double* __restrict__ out) {
+    __shared__ double red[256 / 32];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += 256) acc += part[i];
+    const double r = fv::block_sum<256>(acc, red);
+    if (threadIdx.x == 0) *out = r;
+}
+
+__global__ void nan_scan_kernel(const float* __restrict__ a, long long n, int* __restrict__ flag) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        if (isnan(a[i])) atomicOr(flag, 1);
+}
+
+}  // namespace
+
+struct fv_context {
+    int device = 0;
+    int sm_count = 0;
+    char name[256] = {0};
+};
+
+struct fv_sim {
+    fv_context* ctx = nullptr;
+    int scheme = 0, nx = 0, ny = 0, pitch = 0, nv = 0, gc = 0, num_substeps = 1;
+    float dx = 1, dy = 1;
+    fv_params p{};
+    int bc = 0;
+    float dt_scale = 1.0f;
+    float factor = 0.5f;
+    float* buf[2][4] = {{nullptr}};
+    SimCtl* ctl = nullptr;    // device
+    SimCtl* ctl_h = nullptr;  // pinned host mirror
+    float* block_cfl = nullptr;
+    double* block_sums = nullptr;
+    double* sum_part = nullptr;
+    int* flag = nullptr;
+    const KEntry* ke = nullptr;
+    dim3 grid;
+    cudaStream_t stream = nullptr;
+    alignas(64) StageArgs args;
+    cudaGraphExec_t graph1 = nullptr, graph16 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0.0;
+};
+
+namespace {
+
+int read_ctl(fv_sim* s) {
+    FV_CK(cudaMemcpyAsync(s->ctl_h, s->ctl, sizeof(SimCtl), cudaMemcpyDeviceToHost, s->stream));
+    FV_CK(cudaStreamSynchronize(s->stream));
+    if (s->ctl_h->error) return fail(FV_ERR_DEVICE, "a stage kernel gave up waiting for its tile load");
+    return FV_OK;
+}
+
+int write_ctl(fv_sim* s) {
+    FV_CK(cudaMemcpyAsync(s->ctl, s->ctl_h, sizeof(SimCtl), cudaMemcpyHostToDevice, s->stream));
+    FV_CK(cudaStreamSynchronize(s->stream));
+    return FV_OK;
+}
+
+int launch_stage(fv_sim* s, int substep, bool is_last, bool force_cfl, bool explicit_dt, float dt, bool sums) {
+    alignas(64) StageArgs a = s->args;
+    a.substep = substep;
+    a.is_last = is_last ? 1 : 0;
+    a.force_cfl = force_cfl ? 1 : 0;
+    a.explicit_dt = explicit_dt ? 1 : 0;
+    a.dt_step = dt;
+    a.want_sums = sums ? 1 : 0;
+    void* kargs[] = {&a};
+    FV_CK(cudaLaunchKernel(reinterpret_cast<const void*>(s->ke->fn), s->grid, dim3(s->ke->NT), kargs,
+                           entry_smem(*s->ke), s->stream));
+    return FV_OK;
+}
+
+int launch_step_graphless(fv_sim* s) {
+    for (int i = 0; i < s->num_substeps; ++i)
+        FV_TRY(launch_stage(s, i, i == s->num_substeps - 1, false, false, 0.0f, false));
+    return FV_OK;
+}
+
+int build_graph(fv_sim* s, int nsteps, cudaGraphExec_t* out) {
+    cudaGraph_t g = nullptr;
+    FV_CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = FV_OK;
+    for (int k = 0; k < nsteps && rc == FV_OK; ++k) rc = launch_step_graphless(s);
+    cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (rc != FV_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(FV_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(FV_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    return FV_OK;
+}
+
+int run_steps(fv_sim* s, long long k) {
+    if (!s->graph1) FV_TRY(build_graph(s, 1, &s->graph1));
+    if (!s->graph16) FV_TRY(build_graph(s, 16, &s->graph16));
+    while (k >= 16) {
+        FV_CK(cudaGraphLaunch(s->graph16, s->stream));
+        k -= 16;
+    }
+    while (k > 0) {
+        FV_CK(cudaGraphLaunch(s->graph1, s->stream));
+        --k;
+    }
+    return FV_OK;
+}
+
+// dt = computeDt() * cfl_scale at steps 0, 100, 200, ... (Simulator.py:195-196).
+void host_dt_update(fv_sim* s) {
+    SimCtl& c = *s->ctl_h;
+    if (c.update_dt && c.nt % 100 == 0) c.dt = (c.cfl_min * c.factor) * c.cfl_scale;
+}
+
+int check_sim(fv_sim* s) {
+    if (!s) return fail(FV_ERR_INVALID, "null simulation");
+    FV_CK(cudaSetDevice(s->ctx->device));
+    return FV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fv_version(void) { return 100; }
+
+const char* fv_last_error(void) { return g_err.c_str(); }
+
+int fv_context_create(int device, fv_context** out) {
+    if (!out) return fail(FV_ERR_INVALID, "out is null");
+    int n = 0;
+    FV_CK(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n) return fail(FV_ERR_INVALID, "device %d out of range (%d devices)", device, n);
+    FV_CK(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    FV_CK(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) return fail(FV_ERR_UNSUPPORTED, "libfvgpu is built for sm_100a; device is sm_%d%d", prop.major, prop.minor);
+    if (!encode_fn()) return fail(FV_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+    for (int i = 0; i < kNumEntries; ++i)
+        FV_CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(kTable[i].fn),
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)entry_smem(kTable[i])));
+    fv_context* c = new fv_context;
+    c->device = device;
+    c->sm_count = prop.multiProcessorCount;
+    snprintf(c->name, sizeof(c->name), "%s", prop.name);
+    *out = c;
+    return FV_OK;
+}
+
+int fv_context_destroy(fv_context* ctx) {
+    delete ctx;
+    return FV_OK;
+}
+
+int fv_context_device_name(fv_context* ctx, char* buf, int len) {
+    if (!ctx || !buf || len <= 0) return fail(FV_ERR_INVALID, "bad argument");
+    snprintf(buf, (size_t)len, "%s", ctx->name);
+    return FV_OK;
+}
+
+int fv_sim_create(fv_context* ctx, int scheme, int nx, int ny, float dx, float dy, const fv_params* params, int bc,
+                  const float* const* host_vars, int host_rows, int host_cols, fv_sim** out) {
+    if (!ctx || !params || !host_vars || !out) return fail(FV_ERR_INVALID, "null argument");
+    if (scheme < FV_LXF || scheme > FV_EE2D_KP07_DIMSPLIT) return fail(FV_ERR_INVALID, "unknown scheme %d", scheme);
+    if (nx < 1 || ny < 1 || nx > (1 << 20) || ny > (1 << 20)) return fail(FV_ERR_INVALID, "bad grid %d x %d", nx, ny);
+    for (int side = 0; side < 4; ++side)
+        if (((bc >> (8 * side)) & 0xF) == fv::BC_NEUMANN)
+            return fail(FV_ERR_UNSUPPORTED, "Neumann boundary condition not supported");
+    const int nv = scheme_nv(scheme), gc = scheme_ghost(scheme);
+    const bool halo = (host_rows == ny + 2 * gc && host_cols == nx + 2 * gc);
+    if (!halo && !(host_rows == ny && host_cols == nx))
+        return fail(FV_ERR_INVALID, "Wrong shape of data (%d, %d) vs (%d, %d) / (%d, %d)", host_rows, host_cols, ny, nx,
+                    ny + 2 * gc, nx + 2 * gc);
+    for (int v = 0; v < nv; ++v)
+        if (!host_vars[v]) return fail(FV_ERR_INVALID, "variable %d is null", v);
+    const int cfg = params->tile < 0 ? 0 : params->tile;
+    const KEntry* ke = find_entry(scheme, cfg);
+    if (!ke) return fail(FV_ERR_INVALID, "tile configuration %d does not exist for scheme %d", cfg, scheme);
+    FV_CK(cudaSetDevice(ctx->device));
+
+    fv_sim* s = new fv_sim;
+    s->ctx = ctx;
+    s->scheme = scheme;
+    s->nx = nx;
+    s->ny = ny;
+    s->nv = nv;
+    s->gc = gc;
+    s->dx = dx;
+    s->dy = dy;
+    s->p = *params;
+    s->bc = bc;
+    s->ke = ke;
+    s->pitch = ((nx + 8) + 31) / 32 * 32;  // 128-byte rows; column x at x+4
+    s->num_substeps = (scheme == FV_LXF || scheme == FV_FORCE || scheme == FV_HLL) ? 1
+                      : (scheme == FV_KP07)                                   ? (params->order == 1 ? 1 : 2)
+                                                                              : 2;
+    s->dt_scale = (scheme == FV_HLL2 || scheme == FV_WAF || scheme == FV_KP07_DIMSPLIT ||
+                   scheme == FV_EE2D_KP07_DIMSPLIT)
+                      ? 0.5f
+                      : 1.0f;
+    // computeDt factors (e.g. KP07_dimsplit.py:137, FORCE.py:129, KP07.py:138)
+    s->factor = (scheme == FV_FORCE) ? 1.0f : (scheme == FV_KP07 && params->order == 1) ? 1.0f : 0.5f;
+    s->grid = dim3((nx + ke->W - 1) / ke->W, (ny + ke->H - 1) / ke->H);
+
+    auto cleanup = [&](int rc) {
+        fv_sim_destroy(s);
+        return rc;
+    };
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return cleanup(fail(FV_ERR_CUDA, "stream creation failed"));
+    const size_t plane = (size_t)(ny + 4) * s->pitch * sizeof(float);
+    for (int b = 0; b < 2; ++b)
+        for (int v = 0; v < nv; ++v) {
+            if (cudaMalloc(&s->buf[b][v], plane) != cudaSuccess) return cleanup(fail(FV_ERR_NOMEM, "out of device memory"));
+            if (cudaMemsetAsync(s->buf[b][v], 0, plane, s->stream) != cudaSuccess)
+                return cleanup(fail(FV_ERR_CUDA, "memset failed"));
+        }
+    const size_t nblocks = (size_t)s->grid.x * s->grid.y;
+    if (cudaMalloc(&s->ctl, sizeof(SimCtl)) != cudaSuccess || cudaMallocHost(&s->ctl_h, sizeof(SimCtl)) != cudaSuccess ||
+        cudaMalloc(&s->block_cfl, nblocks * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&s->block_sums, nblocks * 4 * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&s->sum_part, (size_t)(ny + 1) * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&s->flag, sizeof(int)) != cudaSuccess)
+        return cleanup(fail(FV_ERR_NOMEM, "out of device memory"));
+    if (cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess)
+        return cleanup(fail(FV_ERR_CUDA, "event creation failed"));
+
+    // upload u0 (interior or full halo, Common.py:524-531)
+    const int off = halo ? gc : 0;
+    for (int v = 0; v < nv; ++v) {
+        float* dst = s->buf[0][v] + fv::cell_index(-off, -off, s->pitch);
+        if (cudaMemcpy2DAsync(dst, s->pitch * sizeof(float), host_vars[v], host_cols * sizeof(float),
+                              host_cols * sizeof(float), host_rows, cudaMemcpyHostToDevice, s->stream) != cudaSuccess)
+            return cleanup(fail(FV_ERR_CUDA, "upload failed"));
+    }
+
+    // control block
+    SimCtl& c = *s->ctl_h;
+    memset(&c, 0, sizeof(SimCtl));
+    const float c2 = (scheme == FV_EE2D_KP07_DIMSPLIT) ? params->gamma : params->g;
+    const float cfl0 = initial_cfl(host_vars, (size_t)host_rows * host_cols, dx, dy, c2);
+    c.t = 0.0;
+    c.t_end = 0.0;
+    c.nt = 0;
+    c.dt = cfl0;  // as EE2D_KP07_dimsplit.py:107 (the other classes leave dt unset until simulate())
+    c.cfl_min = cfl0;
+    c.factor = s->factor;
+    c.cfl_scale = params->cfl_scale;
+    c.update_dt = 1;
+    c.cur = 0;
+    if (write_ctl(s) != FV_OK) return cleanup(FV_ERR_CUDA);
+
+    // kernel arguments and TMA descriptors
+    StageArgs& a = s->args;
+    memset(&a, 0, sizeof(StageArgs));
+    auto enc = encode_fn();
+    for (int b = 0; b < 2; ++b)
+        for (int v = 0; v < nv; ++v) {
+            a.buf[b][v] = s->buf[b][v];
+            cuuint64_t dims[2] = {(cuuint64_t)(nx + 8), (cuuint64_t)(ny + 4)};
+            cuuint64_t strides[1] = {(cuuint64_t)s->pitch * sizeof(float)};
+            cuuint32_t box[2] = {(cuuint32_t)(ke->W + 8), (cuuint32_t)(ke->H + 4)};
+            cuuint32_t estr[2] = {1, 1};
+            CUresult r = enc(&a.tmap[b][v], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, s->buf[b][v], dims, strides, box, estr,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) return cleanup(fail(FV_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r));
+        }
+    a.ctl = s->ctl;
+    a.block_cfl = s->block_cfl;
+    a.block_sums = s->block_sums;
+    a.nx = nx;
+    a.ny = ny;
+    a.pitch = s->pitch;
+    a.dx = dx;
+    a.dy = dy;
+    a.g = params->g;
+    a.gamma = params->gamma;
+    a.theta = params->theta;
+    a.dt_scale = s->dt_scale;
+    a.bc = bc;
+    a.order = params->order;
+    *out = s;
+    return FV_OK;
+}
+
+int fv_sim_destroy(fv_sim* s) {
+    if (!s) return FV_OK;
+    cudaSetDevice(s->ctx->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->graph1) cudaGraphExecDestroy(s->graph1);
+    if (s->graph16) cudaGraphExecDestroy(s->graph16);
+    for (int b = 0; b < 2; ++b)
+        for (int v = 0; v < 4; ++v)
+            if (s->buf[b][v]) cudaFree(s->buf[b][v]);
+    if (s->ctl) cudaFree(s->ctl);
+    if (s->ctl_h) cudaFreeHost(s->ctl_h);
+    if (s->block_cfl) cudaFree(s->block_cfl);
+    if (s->block_sums) cudaFree(s->block_sums);
+    if (s->sum_part) cudaFree(s->sum_part);
+    if (s->flag) cudaFree(s->flag);
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return FV_OK;
+}
+
+int fv_sim_substep(fv_sim* s, float dt, int step_number) {
+    FV_TRY(check_sim(s));
+    if (step_number < 0 || step_number >= s->num_substeps)
+        return fail(FV_ERR_INVALID, "substep %d out of range", step_number);
+    return launch_stage(s, step_number, false, true, true, dt, false);
+}
+
+int fv_sim_step(fv_sim* s, float dt) {
+    FV_TRY(check_sim(s));
+    for (int i = 0; i < s->num_substeps; ++i)
+        FV_TRY(launch_stage(s, i, i == s->num_substeps - 1, true, true, dt, false));
+    return FV_OK;
+}
+
+int fv_sim_simulate(fv_sim* s, double t, float dt, int use_dt) {
+    FV_TRY(check_sim(s));
+    FV_TRY(read_ctl(s));
+    SimCtl& c = *s->ctl_h;
+    const double t_end = c.t + t;
+    c.t_end = t_end;
+    c.update_dt = use_dt ? 0 : 1;
+    if (use_dt) c.dt = dt;
+    for (;;) {
+        if (!(c.t < t_end)) break;
+        host_dt_update(s);
+        FV_TRY(write_ctl(s));
+        // steps until the next dt update or t_end, replaying the device arithmetic
+        const long long limit = c.update_dt ? 100 - (c.nt % 100) : 1000;
+        long long k = 0;
+        double tt = c.t;
+        while (k < limit && tt < t_end) {
+            const double rem = t_end - tt;
+            const double d = (double)c.dt;
+            const float cur = (float)((rem < d) ? rem : d);
+            if (cur <= 0.0f) break;
+            tt += (double)cur;
+            ++k;
+        }
+        if (k == 0) break;  // dt <= 0: the reference warns and stops (Simulator.py:202-204)
+        FV_TRY(run_steps(s, k));
+        FV_TRY(read_ctl(s));
+    }
+    return FV_OK;
+}
+
+int fv_sim_advance(fv_sim* s, long long n_steps) {
+    FV_TRY(check_sim(s));
+    if (n_steps < 0) return fail(FV_ERR_INVALID, "negative step count");
+    FV_TRY(read_ctl(s));
+    SimCtl& c = *s->ctl_h;
+    c.t_end = INFINITY;
+    c.update_dt = 1;
+    host_dt_update(s);
+    FV_TRY(write_ctl(s));
+    if (!s->graph1) FV_TRY(build_graph(s, 1, &s->graph1));
+    if (!s->graph16) FV_TRY(build_graph(s, 16, &s->graph16));
+    FV_CK(cudaEventRecord(s->ev0, s->stream));
+    FV_TRY(run_steps(s, n_steps));
+    FV_CK(cudaEventRecord(s->ev1, s->stream));
+    FV_CK(cudaEventSynchronize(s->ev1));
+    float ms = 0.0f;
+    FV_CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    s->last_ms = n_steps > 0 ? (double)ms / (double)n_steps : 0.0;
+    return read_ctl(s);
+}
+
+int fv_sim_compute_dt(fv_sim* s, float* dt) {
+    FV_TRY(check_sim(s));
+    if (!dt) return fail(FV_ERR_INVALID, "dt is null");
+    FV_TRY(read_ctl(s));
+    *dt = s->ctl_h->cfl_min * s->ctl_h->factor;
+    return FV_OK;
+}
+
+int fv_sim_download(fv_sim* s, int var, float* host, int host_pitch) {
+    FV_TRY(check_sim(s));
+    if (var < 0 || var >= s->nv || !host || host_pitch < s->nx) return fail(FV_ERR_INVALID, "bad download argument");
+    FV_TRY(read_ctl(s));
+    const float* src = s->buf[s->ctl_h->cur][var] + fv::cell_index(0, 0, s->pitch);
+    FV_CK(cudaMemcpy2DAsync(host, (size_t)host_pitch * sizeof(float), src, (size_t)s->pitch * sizeof(float),
+                            (size_t)s->nx * sizeof(float), s->ny, cudaMemcpyDeviceToHost, s->stream));
+    FV_CK(cudaStreamSynchronize(s->stream));
+    return FV_OK;
+}
+
+int fv_sim_upload(fv_sim* s, int var, const float* host, int host_pitch) {
+    FV_TRY(check_sim(s));
+    if (var < 0 || var >= s->nv || !host || host_pitch < s->nx) return fail(FV_ERR_INVALID, "bad upload argument");
+    FV_TRY(read_ctl(s));
+    float* dst = s->buf[s->ctl_h->cur][var] + fv::cell_index(0, 0, s->pitch);
+    FV_CK(cudaMemcpy2DAsync(dst, (size_t)s->pitch * sizeof(float), host, (size_t)host_pitch * sizeof(float),
+                            (size_t)s->nx * sizeof(float), s->ny, cudaMemcpyHostToDevice, s->stream));
+    FV_CK(cudaStreamSynchronize(s->stream));
+    return FV_OK;
+}
+
+int fv_sim_time(fv_sim* s, double* t, long long* nt, float* dt) {
+    FV_TRY(check_sim(s));
+    FV_TRY(read_ctl(s));
+    if (t) *t = s->ctl_h->t;
+    if (nt) *nt = s->ctl_h->nt;
+    if (dt) *dt = s->ctl_h->dt;
+    return FV_OK;
+}
+
+int fv_sim_conservation(fv_sim* s, double* sums) {
+    FV_TRY(check_sim(s));
+    if (!sums) return fail(FV_ERR_INVALID, "sums is null");
+    FV_TRY(read_ctl(s));
+    double* dev_tot = s->block_sums;  // scratch: reduced before any stage kernel reuses it
+    for (int v = 0; v < s->nv; ++v) {
+        sum_rows_kernel<<<s->ny, 256, 0, s->stream>>>(s->buf[s->ctl_h->cur][v], s->nx, s->pitch, s->sum_part);
+        sum_final_kernel<<<1, 256, 0, s->stream>>>(s->sum_part, s->ny, dev_tot + v);
+        FV_CK(cudaGetLastError());
+    }
+    FV_CK(cudaMemcpyAsync(sums, dev_tot, s->nv * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    FV_CK(cudaStreamSynchronize(s->stream));
+    return FV_OK;
+}
+
+int fv_sim_check(fv_sim* s, int* has_nan) {
+    FV_TRY(check_sim(s));
+    if (!has_nan) return fail(FV_ERR_INVALID, "has_nan is null");
+    FV_CK(cudaMemsetAsync(s->flag, 0, sizeof(int), s->stream));
+    const long long n = (long long)(s->ny + 4) * s->pitch;
+    for (int b = 0; b < 2; ++b)
+        for (int v = 0; v < s->nv; ++v) nan_scan_kernel<<<4 * s->ctx->sm_count, 256, 0, s->stream>>>(s->buf[b][v], n, s->flag);
+    FV_CK(cudaGetLastError());
+    int f = 0;
+    FV_CK(cudaMemcpyAsync(&f, s->flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    FV_CK(cudaStreamSynchronize(s->stream));
+    *has_nan = f;
+    return FV_OK;
+}
+
+int fv_sim_synchronize(fv_sim* s) {
+    FV_TRY(check_sim(s));
+    FV_CK(cudaStreamSynchronize(s->stream));
+    return FV_OK;
+}
+
+int fv_sim_set_boundary_conditions(fv_sim* s, int bc) {
+    FV_TRY(check_sim(s));
+    for (int side = 0; side < 4; ++side)
+        if (((bc >> (8 * side)) & 0xF) == fv::BC_NEUMANN)
+            return fail(FV_ERR_UNSUPPORTED, "Neumann boundary condition not supported");
+    FV_CK(cudaStreamSynchronize(s->stream));
+    s->bc = bc;
+    s->args.bc = bc;
+    if (s->graph1) cudaGraphExecDestroy(s->graph1);
+    if (s->graph16) cudaGraphExecDestroy(s->graph16);
+    s->graph1 = s->graph16 = nullptr;
+    return FV_OK;
+}
+
+int fv_sim_info(fv_sim* s, int* tile_w, int* tile_h, int* threads, int* launches_per_step) {
+    if (!s) return fail(FV_ERR_INVALID, "null simulation");
+    if (tile_w) *tile_w = s->ke->W;
+    if (tile_h) *tile_h = s->ke->H;
+    if (threads) *threads = s->ke->NT;
+    if (launches_per_step) *launches_per_step = s->num_substeps;
+    return FV_OK;
+}
+
+int fv_sim_last_advance_ms(fv_sim* s, double* ms) {
+    if (!s || !ms) return fail(FV_ERR_INVALID, "bad argument");
+    *ms = s->last_ms;
+    return FV_OK;
+}
+
+int fv_host_alloc(void** ptr, size_t bytes) {
+    if (!ptr) return fail(FV_ERR_INVALID, "ptr is null");
+    if (cudaMallocHost(ptr, bytes) != cudaSuccess) return fail(FV_ERR_NOMEM, "pinned allocation of %zu bytes failed", bytes);
+    return FV_OK;
+}
+
+int fv_host_free(void* ptr) {
+    FV_CK(cudaFreeHost(ptr));
+    return FV_OK;
+}
+
+}  // extern "C"

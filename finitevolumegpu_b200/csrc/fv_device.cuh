@@ -1,0 +1,371 @@
+// Device-side building blocks for the finite-volume stage kernels (sm_100a):
+// PTX wrappers for mbarrier / TMA, and the per-face physics of the shallow-water
+// and Euler schemes.
+//
+// The physics mirrors the reference formulas (file:line given per function),
+// rearranged so that values shared by neighbouring faces are computed once per
+// cell: a MUSCL-Hancock cell produces both of its predicted face states from one
+// flux difference, and each face state carries its flux, velocity and wave speed.
+// Arithmetic is FP32 and the library is compiled with --use_fast_math, the
+// options the reference compiles its kernels with (GPUSimulators/KP07_dimsplit.py:87).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fv {
+
+// ------------------------------------------------------------------ PTX helpers
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+// Makes the initialised barrier visible to the async (TMA) proxy.
+__device__ __forceinline__ void fence_barrier_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_shared() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: gives up after `limit` polls (each poll may suspend the thread
+// for a short hardware-defined time) and returns false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase, uint32_t limit) {
+    for (uint32_t i = 0; i < limit; ++i)
+        if (mbar_try_wait(bar, phase)) return true;
+    return false;
+}
+
+// 2-D tiled TMA load (no multicast) of one box into shared memory, completing
+// on `bar`.  x must be a multiple of 4 (16-byte rule for FP32).
+__device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+            "r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void prefetch_tmap(const void* tmap) {
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(tmap)) : "memory");
+}
+
+// ------------------------------------------------------------------ limiters
+
+// Generalised minmod slope (GPUSimulators/cuda/limiters.h:31-41).  The
+// reference's sign product 0.25*s(b)*(s(b)+s(c))*(s(c)+s(f)) is +-1 when the
+// three differences share a sign and 0 otherwise, so the slope is the smallest
+// magnitude with b's sign, or zero.
+__device__ __forceinline__ float minmod_slope(float left, float center, float right, float theta) {
+    const float b = (center - left) * theta;
+    const float c = (right - left) * 0.5f;
+    const float f = (right - center) * theta;
+    const float mag = fminf(fminf(fabsf(b), fabsf(c)), fabsf(f));
+    const uint32_t sb = __float_as_uint(b), sc = __float_as_uint(c), sf = __float_as_uint(f);
+    const bool same = (((sb ^ sc) | (sc ^ sf)) & 0x80000000u) == 0u;
+    return same ? copysignf(mag, b) : 0.0f;
+}
+
+// GPUSimulators/cuda/limiters.h:100-102
+__device__ __forceinline__ float generalized_minmod(float r, float theta) {
+    return fmaxf(0.0f, fminf(theta * r, fminf((1.0f + r) * 0.5f, theta)));
+}
+
+// GPUSimulators/cuda/common.h:81-83
+__device__ __forceinline__ float desingularize(float x, float eps) {
+    return copysignf(fmaxf(fabsf(x), fminf(x * x / (2.0f * eps) + 0.5f * eps, eps)), x);
+}
+
+// ------------------------------------------------------------------ shallow water
+
+// A state at a cell face together with its physical flux
+// (GPUSimulators/cuda/SWECommon.h:29-37), velocity and gravity-wave speed.
+struct SweFace {
+    float q[3];
+    float f[3];
+    float u, c;
+};
+
+__device__ __forceinline__ SweFace swe_face(float h, float hu, float hv, float g, float half_g) {
+    SweFace s;
+    s.q[0] = h;
+    s.q[1] = hu;
+    s.q[2] = hv;
+    const float rh = 1.0f / h;
+    s.u = hu * rh;
+    s.f[0] = hu;
+    s.f[1] = fmaf(hu, s.u, half_g * h * h);
+    s.f[2] = hv * s.u;
+    s.c = sqrtf(g * h);
+    return s;
+}
+
+// Central-upwind flux (GPUSimulators/cuda/SWECommon.h:228-241); m is the left
+// (minus) state, p the right (plus) state.
+__device__ __forceinline__ void swe_central_upwind(const SweFace& m, const SweFace& p, float out[3]) {
+    const float am = fminf(fminf(m.u - m.c, p.u - p.c), 0.0f);
+    const float ap = fmaxf(fmaxf(m.u + m.c, p.u + p.c), 0.0f);
+    const float inv = 1.0f / (ap - am);
+    const float apam = ap * am;
+#pragma unroll
+    for (int v = 0; v < 3; ++v) out[v] = (fmaf(ap, m.f[v], -am * p.f[v]) + apam * (p.q[v] - m.q[v])) * inv;
+}
+
+// HLL flux (GPUSimulators/cuda/SWECommon.h:274-313).
+__device__ __forceinline__ void swe_hll(const SweFace& l, const SweFace& r, float out[3]) {
+    const float h_l = l.q[0], h_r = r.q[0];
+    const float hsum = h_l + h_r;
+    const float h_dag = 0.5f * hsum - 0.25f * (r.u - l.u) * hsum / (l.c + r.c);
+    const float q_l = (h_dag > h_l) ? sqrtf(0.5f * ((h_dag + h_l) * h_dag / (h_l * h_l))) : 1.0f;
+    const float q_r = (h_dag > h_r) ? sqrtf(0.5f * ((h_dag + h_r) * h_dag / (h_r * h_r))) : 1.0f;
+    const float S_l = l.u - l.c * q_l;
+    const float S_r = r.u + r.c * q_r;
+    if (S_l >= 0.0f) {
+#pragma unroll
+        for (int v = 0; v < 3; ++v) out[v] = l.f[v];
+    } else if (S_r <= 0.0f) {
+#pragma unroll
+        for (int v = 0; v < 3; ++v) out[v] = r.f[v];
+    } else {
+        const float inv = 1.0f / (S_r - S_l);
+        const float srsl = S_r * S_l;
+#pragma unroll
+        for (int v = 0; v < 3; ++v) out[v] = (fmaf(S_r, l.f[v], -S_l * r.f[v]) + srsl * (r.q[v] - l.q[v])) * inv;
+    }
+}
+
+// MUSCL-Hancock reconstruction of one cell for the dimensionally split SWE
+// schemes (GPUSimulators/cuda/SWE2D_KP07_dimsplit.cu:38-58, SWE2D_HLL2.cu:39-59):
+// minmod slope, face values Q -+ slope/2, and the half-step predictor
+// Q_face + dt/(2dx) * (F(Q_west) - F(Q_east)), which is the same flux
+// difference for both faces of the cell.  w/e: predicted west/east face states.
+__device__ __forceinline__ void swe_muscl_hancock(const float qm[3], const float q0[3], const float qp[3],
+                                                  float theta, float g, float half_g, float k2, SweFace& w,
+                                                  SweFace& e) {
+    float W[3], E[3];
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        const float s = minmod_slope(qm[v], q0[v], qp[v], theta);
+        W[v] = fmaf(-0.5f, s, q0[v]);
+        E[v] = fmaf(0.5f, s, q0[v]);
+    }
+    const float uw = W[1] / W[0];
+    const float ue = E[1] / E[0];
+    float D[3];
+    D[0] = W[1] - E[1];
+    D[1] = fmaf(W[1], uw, half_g * W[0] * W[0]) - fmaf(E[1], ue, half_g * E[0] * E[0]);
+    D[2] = W[2] * uw - E[2] * ue;
+    w = swe_face(fmaf(k2, D[0], W[0]), fmaf(k2, D[1], W[1]), fmaf(k2, D[2], W[2]), g, half_g);
+    e = swe_face(fmaf(k2, D[0], E[0]), fmaf(k2, D[1], E[1]), fmaf(k2, D[2], E[2]), g, half_g);
+}
+
+// ------------------------------------------------------------------ Euler
+
+struct EulerFace {
+    float q[4];
+    float f[4];
+    float u, c;
+};
+
+// Face state with pressure (GPUSimulators/cuda/EulerCommon.h:83-90), flux
+// (EulerCommon.h:93-109) and sound speed sqrt(gamma*P/rho) (EulerCommon.h:130-131, :176).
+__device__ __forceinline__ EulerFace euler_face(float rho, float ru, float rv, float E, float gamma) {
+    EulerFace s;
+    s.q[0] = rho;
+    s.q[1] = ru;
+    s.q[2] = rv;
+    s.q[3] = E;
+    const float rr = 1.0f / rho;
+    const float P = (gamma - 1.0f) * (E - 0.5f * (ru * ru + rv * rv) * rr);
+    s.u = ru * rr;
+    s.f[0] = ru;
+    s.f[1] = fmaf(ru, s.u, P);
+    s.f[2] = rv * s.u;
+    s.f[3] = s.u * (E + P);
+    s.c = sqrtf(gamma * P * rr);
+    return s;
+}
+
+// GPUSimulators/cuda/EulerCommon.h:171-187
+__device__ __forceinline__ void euler_central_upwind(const EulerFace& m, const EulerFace& p, float out[4]) {
+    const float am = fminf(fminf(m.u - m.c, p.u - p.c), 0.0f);
+    const float ap = fmaxf(fmaxf(m.u + m.c, p.u + p.c), 0.0f);
+    const float inv = 1.0f / (ap - am);
+    const float apam = ap * am;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) out[v] = (fmaf(ap, m.f[v], -am * p.f[v]) + apam * (p.q[v] - m.q[v])) * inv;
+}
+
+// GPUSimulators/cuda/EulerCommon.h:117-160
+__device__ __forceinline__ void euler_hll(const EulerFace& l, const EulerFace& r, float out[4]) {
+    const float h_l = l.q[0], h_r = r.q[0];
+    const float hsum = h_l + h_r;
+    const float h_dag = 0.5f * hsum - 0.25f * (r.u - l.u) * hsum / (l.c + r.c);
+    const float q_l = (h_dag > h_l) ? sqrtf(0.5f * ((h_dag + h_l) * h_dag / (h_l * h_l))) : 1.0f;
+    const float q_r = (h_dag > h_r) ? sqrtf(0.5f * ((h_dag + h_r) * h_dag / (h_r * h_r))) : 1.0f;
+    const float S_l = l.u - l.c * q_l;
+    const float S_r = r.u + r.c * q_r;
+    if (S_l >= 0.0f) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) out[v] = l.f[v];
+    } else if (S_r <= 0.0f) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) out[v] = r.f[v];
+    } else {
+        const float inv = 1.0f / (S_r - S_l);
+        const float srsl = S_r * S_l;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) out[v] = (fmaf(S_r, l.f[v], -S_l * r.f[v]) + srsl * (r.q[v] - l.q[v])) * inv;
+    }
+}
+
+// MUSCL-Hancock reconstruction for the Euler kernel
+// (GPUSimulators/cuda/EE2D_KP07_dimsplit.cu:33-58 and :78-103).  The reference's
+// predictor calls F_func(Q, gamma_), whose second argument is the pressure, so
+// the predictor flux uses gamma in place of P; that is reproduced here.
+__device__ __forceinline__ void euler_muscl_hancock(const float qm[4], const float q0[4], const float qp[4],
+                                                    float theta, float gamma, float k2, EulerFace& w,
+                                                    EulerFace& e) {
+    float W[4], E[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+        const float s = minmod_slope(qm[v], q0[v], qp[v], theta);
+        W[v] = fmaf(-0.5f, s, q0[v]);
+        E[v] = fmaf(0.5f, s, q0[v]);
+    }
+    const float uw = W[1] / W[0];
+    const float ue = E[1] / E[0];
+    float D[4];
+    D[0] = W[1] - E[1];
+    D[1] = fmaf(W[1], uw, gamma) - fmaf(E[1], ue, gamma);
+    D[2] = W[2] * uw - E[2] * ue;
+    D[3] = uw * (W[3] + gamma) - ue * (E[3] + gamma);
+    w = euler_face(fmaf(k2, D[0], W[0]), fmaf(k2, D[1], W[1]), fmaf(k2, D[2], W[2]), fmaf(k2, D[3], W[3]), gamma);
+    e = euler_face(fmaf(k2, D[0], E[0]), fmaf(k2, D[1], E[1]), fmaf(k2, D[2], E[2]), fmaf(k2, D[3], E[3]), gamma);
+}
+
+// ------------------------------------------------------------------ WAF
+
+// Per-cell quantities of the WAF flux (GPUSimulators/cuda/SWECommon.h:131-210):
+// state, velocities, wave speed and physical flux.
+struct WafCell {
+    float q[3];
+    float f[3];
+    float u, v, c;
+};
+
+__device__ __forceinline__ WafCell waf_cell(const float q[3], float g, float half_g) {
+    WafCell s;
+    s.q[0] = q[0];
+    s.q[1] = q[1];
+    s.q[2] = q[2];
+    const float rh = 1.0f / q[0];
+    s.u = q[1] * rh;
+    s.v = q[2] * rh;
+    s.c = sqrtf(g * q[0]);
+    s.f[0] = q[1];
+    s.f[1] = fmaf(q[1], s.u, half_g * q[0] * q[0]);
+    s.f[2] = q[2] * s.u;
+    return s;
+}
+
+// h in the star region between two cells (GPUSimulators/cuda/SWECommon.h:114-121).
+__device__ __forceinline__ float waf_h_star(const WafCell& l, const WafCell& r, float inv_g) {
+    const float t = 0.5f * (l.c + r.c) + 0.25f * (l.u - r.u);
+    return t * t * inv_g;
+}
+
+// WAF flux at the face between l1 and r1 (GPUSimulators/cuda/SWECommon.h:131-210);
+// hd_l, hd, hd_r are the star depths of the pairs (l2,l1), (l1,r1), (r1,r2).
+__device__ __forceinline__ void waf_flux(const WafCell& l2, const WafCell& l1, const WafCell& r1,
+                                         const WafCell& r2, float hd_l, float hd, float hd_r, float dtdx,
+                                         float out[3]) {
+    const float h_l = l1.q[0], h_r = r1.q[0];
+    const float q_l = (hd > h_l) ? sqrtf(0.5f * ((hd + h_l) * hd)) / h_l : 1.0f;
+    const float q_r = (hd > h_r) ? sqrtf(0.5f * ((hd + h_r) * hd)) / h_r : 1.0f;
+    const float S_l = l1.u - l1.c * q_l;
+    const float S_r = r1.u + r1.c * q_r;
+    const float a_r = h_r * (r1.u - S_r);
+    const float a_l = h_l * (l1.u - S_l);
+    const float S_star = (S_l * a_r - S_r * a_l) / (a_r - a_l);
+    const float sl = h_l * (S_l - l1.u) / (S_l - S_star);
+    const float sr = h_r * (S_r - r1.u) / (S_r - S_star);
+    const float Qsl[3] = {sl, sl * S_star, sl * l1.v};
+    const float Qsr[3] = {sr, sr * S_star, sr * r1.v};
+    const float c_1 = S_l * dtdx;
+    const float c_2 = S_star * dtdx;
+    const float c_3 = S_r * dtdx;
+    const float eps = 1.0e-6f;
+    const float r_1 = desingularize((c_1 > 0.0f) ? (hd_l - l2.q[0]) : (hd_r - h_r), eps) / desingularize(hd - h_l, eps);
+    const float r_2 = desingularize((c_2 > 0.0f) ? (l1.v - l2.v) : (r2.v - r1.v), eps) / desingularize(r1.v - l1.v, eps);
+    const float r_3 = desingularize((c_3 > 0.0f) ? (h_l - hd_l) : (r2.q[0] - hd_r), eps) / desingularize(h_r - hd, eps);
+    // A_k = sign(c_k) * (1 - (1 - |c_k|) * limiter(r_k)) (SWECommon.h:109-111, :199-201)
+    const float A_1 = copysignf(1.0f, c_1) * (1.0f - (1.0f - fabsf(c_1)) * generalized_minmod(r_1, 1.9f));
+    const float A_2 = copysignf(1.0f, c_2) * (1.0f - (1.0f - fabsf(c_2)) * generalized_minmod(r_2, 1.9f));
+    const float A_3 = copysignf(1.0f, c_3) * (1.0f - (1.0f - fabsf(c_3)) * generalized_minmod(r_3, 1.9f));
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        const float F1 = l1.f[v], F4 = r1.f[v];
+        const float F2 = fmaf(S_l, Qsl[v] - l1.q[v], F1);
+        const float F3 = fmaf(S_r, Qsr[v] - r1.q[v], F4);
+        out[v] = 0.5f * (F1 + F4) - 0.5f * (A_1 * (F2 - F1) + A_2 * (F3 - F2) + A_3 * (F4 - F3));
+    }
+}
+
+// ------------------------------------------------------------------ first-order fluxes
+
+// FORCE = (LxF + Lax-Wendroff two-step) / 2 (GPUSimulators/cuda/SWECommon.h:404-409,
+// :443-450, :466-470).  kx = dx/(2dt), kw = dt/(2dx).
+__device__ __forceinline__ void swe_force(const SweFace& l, const SweFace& r, float g, float half_g, float kx,
+                                          float kw, float out[3]) {
+    float qlw[3];
+#pragma unroll
+    for (int v = 0; v < 3; ++v) qlw[v] = fmaf(kw, l.f[v] - r.f[v], 0.5f * (l.q[v] + r.q[v]));
+    const SweFace w = swe_face(qlw[0], qlw[1], qlw[2], g, half_g);
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        const float lxf = fmaf(kx, l.q[v] - r.q[v], 0.5f * (l.f[v] + r.f[v]));
+        out[v] = 0.5f * (lxf + w.f[v]);
+    }
+}
+
+// Lax-Friedrichs flux with the 2-D diffusion dx/(4dt) (GPUSimulators/cuda/SWECommon.h:421-427).
+__device__ __forceinline__ void swe_lxf_2d(const SweFace& l, const SweFace& r, float k4, float out[3]) {
+#pragma unroll
+    for (int v = 0; v < 3; ++v) out[v] = fmaf(k4, l.q[v] - r.q[v], 0.5f * (l.f[v] + r.f[v]));
+}
+
+// Per-cell CFL time step (GPUSimulators/cuda/SWECommon.h:497-504; EulerCommon.h:42-49
+// with sqrt(gamma*rho)).
+__device__ __forceinline__ float cell_cfl(float h, float hu, float hv, float dx, float dy, float gg) {
+    const float rh = 1.0f / h;
+    const float c = sqrtf(gg * h);
+    const float max_u = dx / (fabsf(hu * rh) + c);
+    const float max_v = dy / (fabsf(hv * rh) + c);
+    return fminf(max_u, max_v);
+}
+
+}  // namespace fv

@@ -1,0 +1,834 @@
+// Stage kernels: one launch advances every cell of one simulation by one
+// substep of its scheme (the work of one reference kernel launch, e.g.
+// GPUSimulators/cuda/SWE2D_KP07_dimsplit.cu:123-205).
+//
+// Tile: a CTA owns W x H interior cells.  One TMA box per variable brings the
+// tile plus a 4-column / 2-row halo into shared memory ((H+4) x (W+8) floats,
+// box x aligned to 4 floats).  Ghost cells are then completed in shared memory
+// (periodic wrap from global memory, reflective mirror in the reference's
+// N, S, E, W order), the sweeps run in place, and the interior is written back
+// with 128-bit stores.  The CFL minimum and the FP64 conservation sums are
+// reduced in the same pass; the last CTA to finish advances the simulation's
+// control block (t, nt, dt, buffer parity), so a whole step sequence can be
+// captured in a CUDA graph without host round trips.
+//
+// Sweep mapping:
+//   x sweeps: a thread walks one row segment of W/4 cells (lanes = 8 rows x
+//     4 segments).  With a shared row pitch of W+8 = 4 (mod 32) floats and
+//     W/4 = -1 (mod 32) the 32 lanes hit 32 distinct banks.
+//   y sweeps: a thread walks one column segment (lanes = consecutive columns).
+// Each thread keeps a 3-cell window in registers and reconstructs every cell
+// once; the halo cells of its segment are read before a barrier so that
+// in-place updates by neighbouring segments cannot race with them.
+#pragma once
+
+#include <cuda.h>
+
+#include "fv_device.cuh"
+
+namespace fv {
+
+enum Scheme { LXF = 0, FORCE = 1, HLL = 2, HLL2 = 3, WAF = 4, KP07 = 5, KP07_DIMSPLIT = 6, EE2D = 7 };
+
+// Reference boundary codec (GPUSimulators/cuda/common.h:109-130).
+enum BoundaryType { BC_DIRICHLET = 0, BC_NEUMANN = 1, BC_PERIODIC = 2, BC_REFLECTIVE = 3 };
+__host__ __device__ inline int bc_north(int bc) { return (bc >> 24) & 0xF; }
+__host__ __device__ inline int bc_south(int bc) { return (bc >> 16) & 0xF; }
+__host__ __device__ inline int bc_east(int bc) { return (bc >> 8) & 0xF; }
+__host__ __device__ inline int bc_west(int bc) { return bc & 0xF; }
+
+// Control block of one simulation, resident in device memory.
+struct SimCtl {
+    double t;          // simulation time (BaseSimulator.t, FP64)
+    double t_end;      // end time of the current simulate() call
+    long long nt;      // completed steps (BaseSimulator.nt)
+    float dt;          // CFL step in use (BaseSimulator.dt)
+    float cfl_min;     // min of the last CFL field (gpuarray.min(cfl_data))
+    float factor;      // the scheme's computeDt factor
+    float cfl_scale;   // Courant number
+    int update_dt;     // recompute dt every 100 steps (simulate(t) without dt)
+    int cur;           // buffer index holding u0
+    unsigned int arrive;  // CTA arrival counter for the last-CTA epilogue
+    int error;         // nonzero once a bounded wait gave up
+    double sums[4];    // FP64 sums of the interior of u0 after the last step that asked for them
+};
+
+// Launch arguments (passed as a __grid_constant__ parameter; the tensor maps
+// must live in parameter, constant or global memory).
+struct StageArgs {
+    CUtensorMap tmap[2][4];  // [buffer][variable]
+    float* buf[2][4];
+    SimCtl* ctl;
+    float* block_cfl;    // one float per CTA
+    double* block_sums;  // 4 doubles per CTA
+    int nx, ny, pitch;   // pitch in floats
+    float dx, dy, g, gamma, theta;
+    float dt_scale;      // kernel dt = step dt * dt_scale (0.5 for split substeps)
+    int bc;
+    int substep;         // sweep order (split schemes) or RK stage (KP07)
+    int order;           // RK order (KP07)
+    int is_last;         // this launch completes a step
+    int force_cfl;       // compute the CFL field in this launch
+    int explicit_dt;     // take the step dt from dt_step instead of the control block
+    float dt_step;
+    int want_sums;       // compute FP64 sums of the new state at the end of a step
+};
+
+// Storage: per variable, rows y = -2 .. ny+1 and columns x = -4 .. pitch-5,
+// element (y, x) at [(y + 2) * pitch + (x + 4)].
+__host__ __device__ inline long long cell_index(int y, int x, int pitch) {
+    return (long long)(y + 2) * pitch + (x + 4);
+}
+
+constexpr uint32_t kWaitPolls = 1u << 20;
+
+struct StepCtl {
+    float dt;      // step dt (before dt_scale)
+    double t_new;  // t after this step
+    int cur;
+    bool active;
+    bool do_cfl;
+};
+
+// dt of the current step: float32(min(dt, t_end - t)) (GPUSimulators/Simulator.py:199),
+// with Python's min() tie and NaN behaviour; a step runs while t < t_end and
+// dt > 0 (Simulator.py:192, :202).
+__device__ __forceinline__ StepCtl read_step(const StageArgs& A) {
+    const volatile SimCtl* c = A.ctl;
+    StepCtl s;
+    s.cur = c->cur;
+    const double t = c->t;
+    const double t_end = c->t_end;
+    if (A.explicit_dt) {
+        s.dt = A.dt_step;
+        s.active = true;
+    } else {
+        const double rem = t_end - t;
+        const double d = (double)c->dt;
+        s.dt = (float)((rem < d) ? rem : d);
+        s.active = (t < t_end) && !(s.dt <= 0.0f);
+    }
+    s.t_new = t + (double)s.dt;
+    const long long nt = c->nt;
+    const bool sched = c->update_dt && ((nt + 1) % 100 == 0);
+    s.do_cfl = A.force_cfl || (A.is_last && !A.explicit_dt && (sched || !(s.t_new < t_end)));
+    return s;
+}
+
+template <int NT>
+__device__ __forceinline__ float block_min(float v, float* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int w = threadIdx.x >> 5;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[w] = v;
+    __syncthreads();
+    float r = red[0];
+#pragma unroll
+    for (int i = 1; i < NT / 32; ++i) r = fminf(r, red[i]);
+    return r;
+}
+
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[w] = v;
+    __syncthreads();
+    double r = red[0];
+#pragma unroll
+    for (int i = 1; i < NT / 32; ++i) r += red[i];
+    return r;
+}
+
+// CTA epilogue: per-CTA CFL minimum and FP64 sums, arrival count, and (last
+// CTA) the reduction over all CTAs in fixed order plus the control-block update
+// of Simulator.step / simulate (GPUSimulators/Simulator.py:195-196, :227-228).
+template <int NT, int NV>
+__device__ void stage_epilogue(const StageArgs& A, const StepCtl& s, float my_cfl, const double (&my_sums)[NV],
+                               bool sums) {
+    __shared__ float red_f[NT / 32];
+    __shared__ double red_d[NT / 32];
+    __shared__ int am_last;
+    const int nblocks = gridDim.x * gridDim.y;
+    const int bid = blockIdx.y * gridDim.x + blockIdx.x;
+    if (s.do_cfl) {
+        const float m = block_min<NT>(my_cfl, red_f);
+        if (threadIdx.x == 0) A.block_cfl[bid] = m;
+    }
+    if (sums) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            const double t = block_sum<NT>(my_sums[v], red_d);
+            if (threadIdx.x == 0) A.block_sums[(size_t)bid * 4 + v] = t;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned prev = atomicAdd(&A.ctl->arrive, 1u);
+        am_last = (prev == (unsigned)nblocks - 1u);
+    }
+    __syncthreads();
+    if (!am_last) return;
+    __threadfence();
+    float m = __int_as_float(0x7f800000);
+    if (s.do_cfl) {
+        for (int i = threadIdx.x; i < nblocks; i += NT) m = fminf(m, __ldcg(&A.block_cfl[i]));
+        m = block_min<NT>(m, red_f);
+    }
+    double tot[NV];
+    if (sums) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            // fixed per-thread striding and tree: deterministic for a given grid
+            double acc = 0.0;
+            for (int i = threadIdx.x; i < nblocks; i += NT) acc += __ldcg(&A.block_sums[(size_t)i * 4 + v]);
+            tot[v] = block_sum<NT>(acc, red_d);
+        }
+    }
+    if (threadIdx.x == 0) {
+        SimCtl* c = A.ctl;
+        c->cur = s.cur ^ 1;
+        if (s.do_cfl) c->cfl_min = m;
+        if (sums) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) c->sums[v] = tot[v];
+        }
+        if (A.is_last) {
+            c->t = s.t_new;
+            c->nt = c->nt + 1;
+            if (!A.explicit_dt && c->update_dt && (c->nt % 100 == 0)) c->dt = (c->cfl_min * c->factor) * c->cfl_scale;
+        }
+        c->arrive = 0u;
+        __threadfence();
+    }
+}
+
+// ------------------------------------------------------------------ tile load + ghost cells
+
+// Issues the TMA loads of the tile (thread 0) and waits for them with a bounded
+// wait.  Returns false (uniformly across the CTA) if the wait gave up.
+template <int NV, int SP, int TR>
+__device__ __forceinline__ bool load_tile(float* Qs, const StageArgs& A, int cur, int x0, int y0, uint64_t* bar) {
+    constexpr int PS = SP * TR;
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        fence_barrier_init();
+        mbar_arrive_expect_tx(bar, NV * PS * (uint32_t)sizeof(float));
+#pragma unroll
+        for (int v = 0; v < NV; ++v) tma_load_2d(Qs + v * PS, &A.tmap[cur][v], x0, y0, bar);
+    }
+    __syncthreads();
+    const bool ok = mbar_wait_bounded(bar, 0, kWaitPolls);
+    const int failed = __syncthreads_or(ok ? 0 : 1);
+    if (failed) {
+        if (threadIdx.x == 0) atomicExch(&A.ctl->error, 1);
+        mbar_wait_bounded(bar, 0, kWaitPolls);  // let copies in flight land before the CTA exits
+        return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ float sign_x(int v) { return v == 1 ? -1.0f : 1.0f; }
+__device__ __forceinline__ float sign_y(int v) { return v == 2 ? -1.0f : 1.0f; }
+
+// Ghost cells of a tile that reaches the domain boundary, with readBlock's
+// semantics (GPUSimulators/cuda/common.h:248-351): periodic sides read the
+// wrapped cell from global memory, then reflective sides mirror interior cells
+// with the normal momentum negated, north, south, east, west in turn.
+// Dirichlet ghosts keep the stored values the TMA load brought in.
+template <int NV, int W, int H, int NT>
+__device__ void apply_boundary(float* Qs, const StageArgs& A, int cur, int x0, int y0) {
+    constexpr int SP = W + 8, TR = H + 4, PS = SP * TR;
+    const int nx = A.nx, ny = A.ny, bc = A.bc;
+    const bool pw = bc_west(bc) == BC_PERIODIC, pe = bc_east(bc) == BC_PERIODIC;
+    const bool ps = bc_south(bc) == BC_PERIODIC, pn = bc_north(bc) == BC_PERIODIC;
+    if (pw || pe || ps || pn) {
+        for (int i = threadIdx.x; i < TR * SP; i += NT) {
+            const int t = i / SP, s = i - t * SP;
+            const int x = x0 - 4 + s, y = y0 - 2 + t;
+            if (x < -2 || x >= nx + 2 || y < -2 || y >= ny + 2) continue;
+            int xs = x, ys = y;
+            if (x < 0 && pw) xs = x + nx;
+            else if (x >= nx && pe) xs = x - nx;
+            if (y < 0 && ps) ys = y + ny;
+            else if (y >= ny && pn) ys = y - ny;
+            if (xs == x && ys == y) continue;
+            const long long gi = cell_index(ys, xs, A.pitch);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) Qs[v * PS + i] = __ldg(A.buf[cur][v] + gi);
+        }
+        __syncthreads();
+    }
+    // Tile row of domain row y: t = y - y0 + 2; tile column of x: s = x - x0 + 4.
+    if (bc_north(bc) == BC_REFLECTIVE && y0 + H + 2 > ny) {
+        for (int i = threadIdx.x; i < 2 * SP; i += NT) {
+            const int m = i / SP, s = i - m * SP;
+            const int t = ny + m - y0 + 2, ts = ny - 1 - m - y0 + 2;
+            if (t < TR) {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) Qs[v * PS + t * SP + s] = sign_y(v) * Qs[v * PS + ts * SP + s];
+            }
+        }
+        __syncthreads();
+    }
+    if (bc_south(bc) == BC_REFLECTIVE && y0 == 0) {
+        for (int i = threadIdx.x; i < 2 * SP; i += NT) {
+            const int m = i / SP, s = i - m * SP;
+            const int t = -1 - m + 2, ts = m + 2;
+            if (ts < TR) {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) Qs[v * PS + t * SP + s] = sign_y(v) * Qs[v * PS + ts * SP + s];
+            }
+        }
+        __syncthreads();
+    }
+    if (bc_east(bc) == BC_REFLECTIVE && x0 + W + 2 > nx) {
+        for (int i = threadIdx.x; i < 2 * TR; i += NT) {
+            const int m = i / TR, t = i - m * TR;
+            const int s = nx + m - x0 + 4, ss = nx - 1 - m - x0 + 4;
+            if (s < SP) {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) Qs[v * PS + t * SP + s] = sign_x(v) * Qs[v * PS + t * SP + ss];
+            }
+        }
+        __syncthreads();
+    }
+    if (bc_west(bc) == BC_REFLECTIVE && x0 == 0) {
+        for (int i = threadIdx.x; i < 2 * TR; i += NT) {
+            const int m = i / TR, t = i - m * TR;
+            const int s = -1 - m + 4, ss = m + 4;
+            if (ss < SP) {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) Qs[v * PS + t * SP + s] = sign_x(v) * Qs[v * PS + t * SP + ss];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------ line walkers
+
+// Variable slot of logical component v along a line: y lines see (h, hv, hu)
+// ("transposing" the domain, GPUSimulators/cuda/SWE2D_KP07_dimsplit.cu:81-107).
+template <bool SWAP> __device__ __forceinline__ constexpr int vslot(int v) {
+    return SWAP ? (v == 1 ? 2 : (v == 2 ? 1 : v)) : v;
+}
+
+template <int NV, bool SWAP, int PS>
+__device__ __forceinline__ void ld_cell(const float* line, int k, int step, float (&q)[NV]) {
+    const float* p = line + k * step;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) q[v] = p[vslot<SWAP>(v) * PS];
+}
+
+template <int NV, bool SWAP, int PS>
+__device__ __forceinline__ void st_cell(float* line, int k, int step, const float (&q)[NV]) {
+    float* p = line + k * step;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) p[vslot<SWAP>(v) * PS] = q[v];
+}
+
+// Physics policies for the MUSCL-Hancock walker.
+struct SwePhys {
+    static constexpr int NV = 3;
+    using Face = SweFace;
+    float theta, g, half_g, k2;
+    __device__ __forceinline__ void recon(const float (&qm)[3], const float (&q0)[3], const float (&qp)[3], Face& w,
+                                          Face& e) const {
+        swe_muscl_hancock(qm, q0, qp, theta, g, half_g, k2, w, e);
+    }
+    template <bool HLLF> __device__ __forceinline__ static void flux(const Face& l, const Face& r, float (&F)[3]) {
+        if (HLLF) swe_hll(l, r, F);
+        else swe_central_upwind(l, r, F);
+    }
+};
+
+struct EulerPhys {
+    static constexpr int NV = 4;
+    using Face = EulerFace;
+    float theta, gamma, k2;
+    __device__ __forceinline__ void recon(const float (&qm)[4], const float (&q0)[4], const float (&qp)[4], Face& w,
+                                          Face& e) const {
+        euler_muscl_hancock(qm, q0, qp, theta, gamma, k2, w, e);
+    }
+    template <bool HLLF> __device__ __forceinline__ static void flux(const Face& l, const Face& r, float (&F)[4]) {
+        if (HLLF) euler_hll(l, r, F);
+        else euler_central_upwind(l, r, F);
+    }
+};
+
+// One MUSCL-Hancock window step at cell c: shift in Q[c+1], reconstruct c,
+// flux at c-1/2, update cell c-1 (GPUSimulators/cuda/common.h:444-475).
+template <class Phys, bool HLLF, bool SWAP, int PS>
+__device__ __forceinline__ void mh_step(float* line, int step, int c, float (&qm)[Phys::NV], float (&q0)[Phys::NV],
+                                        float (&qp)[Phys::NV], const float (&qn)[Phys::NV],
+                                        typename Phys::Face& eL, float (&Fprev)[Phys::NV], const Phys& P,
+                                        float kdx, bool update) {
+    constexpr int NV = Phys::NV;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        qm[v] = q0[v];
+        q0[v] = qp[v];
+        qp[v] = qn[v];
+    }
+    typename Phys::Face w, e;
+    P.recon(qm, q0, qp, w, e);
+    float F[NV];
+    Phys::template flux<HLLF>(eL, w, F);
+    if (update) {
+        float out[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) out[v] = fmaf(Fprev[v] - F[v], kdx, qm[v]);
+        st_cell<NV, SWAP, PS>(line, c - 1, step, out);
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) Fprev[v] = F[v];
+    eL = e;
+}
+
+// Updates cells [a, b) of a line in place.  pre holds Q[a-2], Q[a-1], Q[b], Q[b+1].
+template <class Phys, bool HLLF, bool SWAP, int PS>
+__device__ __forceinline__ void walk_mh(float* line, int step, int a, int b, const float (&pre)[4][Phys::NV],
+                                        const Phys& P, float kdx) {
+    constexpr int NV = Phys::NV;
+    float qm[NV], q0[NV], qp[NV], qn[NV], Fprev[NV];
+    typename Phys::Face eL;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        q0[v] = pre[0][v];
+        qp[v] = pre[1][v];
+        Fprev[v] = 0.0f;
+    }
+    // c = a-1: reconstruct only
+    ld_cell<NV, SWAP, PS>(line, a, step, qn);
+    {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            qm[v] = q0[v];
+            q0[v] = qp[v];
+            qp[v] = qn[v];
+        }
+        typename Phys::Face w;
+        P.recon(qm, q0, qp, w, eL);
+    }
+    // c = a: first face, no update
+    ld_cell<NV, SWAP, PS>(line, a + 1, step, qn);
+    mh_step<Phys, HLLF, SWAP, PS>(line, step, a, qm, q0, qp, qn, eL, Fprev, P, kdx, false);
+    for (int c = a + 1; c < b - 1; ++c) {
+        ld_cell<NV, SWAP, PS>(line, c + 1, step, qn);
+        mh_step<Phys, HLLF, SWAP, PS>(line, step, c, qm, q0, qp, qn, eL, Fprev, P, kdx, true);
+    }
+    mh_step<Phys, HLLF, SWAP, PS>(line, step, b - 1, qm, q0, qp, pre[2], eL, Fprev, P, kdx, true);
+    mh_step<Phys, HLLF, SWAP, PS>(line, step, b, qm, q0, qp, pre[3], eL, Fprev, P, kdx, true);
+}
+
+// Two-point flux walker (FORCE, HLL: GPUSimulators/cuda/SWE2D_FORCE.cu:29-81,
+// SWE2D_HLL.cu:32-86).  pre holds Q[a-1] (slot 1) and Q[b] (slot 2).
+template <int SCHEME, bool SWAP, int PS>
+__device__ __forceinline__ void walk_2pt(float* line, int step, int a, int b, const float (&pre)[4][3], float g,
+                                         float half_g, float kx, float kw, float kdx) {
+    auto face_flux = [&](const SweFace& l, const SweFace& r, float (&F)[3]) {
+        if (SCHEME == FORCE) swe_force(l, r, g, half_g, kx, kw, F);
+        else swe_hll(l, r, F);
+    };
+    SweFace sL = swe_face(pre[1][0], pre[1][1], pre[1][2], g, half_g);
+    float qa[3];
+    ld_cell<3, SWAP, PS>(line, a, step, qa);
+    SweFace s = swe_face(qa[0], qa[1], qa[2], g, half_g);
+    float Fprev[3];
+    face_flux(sL, s, Fprev);
+    float qprev[3] = {qa[0], qa[1], qa[2]};
+    sL = s;
+    for (int c = a + 1; c <= b; ++c) {
+        float q[3];
+        if (c < b) {
+            ld_cell<3, SWAP, PS>(line, c, step, q);
+        } else {
+#pragma unroll
+            for (int v = 0; v < 3; ++v) q[v] = pre[2][v];
+        }
+        s = swe_face(q[0], q[1], q[2], g, half_g);
+        float F[3];
+        face_flux(sL, s, F);
+        float out[3];
+#pragma unroll
+        for (int v = 0; v < 3; ++v) out[v] = fmaf(Fprev[v] - F[v], kdx, qprev[v]);
+        st_cell<3, SWAP, PS>(line, c - 1, step, out);
+#pragma unroll
+        for (int v = 0; v < 3; ++v) {
+            Fprev[v] = F[v];
+            qprev[v] = q[v];
+        }
+        sL = s;
+    }
+}
+
+// WAF walker (GPUSimulators/cuda/SWE2D_WAF.cu:35-87): the flux at c-1/2 uses
+// cells c-2 .. c+1; per-cell quantities and the star depths of neighbouring
+// pairs are carried along the window.
+template <bool SWAP, int PS>
+__device__ __forceinline__ void walk_waf(float* line, int step, int a, int b, const float (&pre)[4][3], float g,
+                                         float half_g, float inv_g, float dtdx, float kdx) {
+    WafCell C0 = waf_cell(pre[0], g, half_g);
+    WafCell C1 = waf_cell(pre[1], g, half_g);
+    float q[3];
+    ld_cell<3, SWAP, PS>(line, a, step, q);
+    WafCell C2 = waf_cell(q, g, half_g);
+    ld_cell<3, SWAP, PS>(line, a + 1, step, q);
+    WafCell C3 = waf_cell(q, g, half_g);
+    float hs01 = waf_h_star(C0, C1, inv_g), hs12 = waf_h_star(C1, C2, inv_g), hs23 = waf_h_star(C2, C3, inv_g);
+    float Fprev[3];
+    waf_flux(C0, C1, C2, C3, hs01, hs12, hs23, dtdx, Fprev);  // face a-1/2
+    for (int c = a + 1; c <= b; ++c) {
+        if (c + 1 < b) {
+            ld_cell<3, SWAP, PS>(line, c + 1, step, q);
+        } else {
+            const int k = (c + 1 == b) ? 2 : 3;
+#pragma unroll
+            for (int v = 0; v < 3; ++v) q[v] = pre[k][v];
+        }
+        C0 = C1;
+        C1 = C2;
+        C2 = C3;
+        C3 = waf_cell(q, g, half_g);
+        hs01 = hs12;
+        hs12 = hs23;
+        hs23 = waf_h_star(C2, C3, inv_g);
+        float F[3];
+        waf_flux(C0, C1, C2, C3, hs01, hs12, hs23, dtdx, F);  // face c-1/2
+        float out[3];
+#pragma unroll
+        for (int v = 0; v < 3; ++v) out[v] = fmaf(Fprev[v] - F[v], kdx, C1.q[v]);
+        st_cell<3, SWAP, PS>(line, c - 1, step, out);
+#pragma unroll
+        for (int v = 0; v < 3; ++v) Fprev[v] = F[v];
+    }
+}
+
+// Per-scheme parameters of one sweep direction.
+struct SweepPar {
+    float theta, g, half_g, inv_g, gamma;
+    float kdt;   // kernel dt
+    float dxx;   // cell size along the sweep
+};
+
+template <int SCHEME, bool SWAP, int PS>
+__device__ __forceinline__ void walk_line(float* line, int step, int a, int b, const float (&pre)[4][(SCHEME == EE2D) ? 4 : 3],
+                                          const SweepPar& p) {
+    const float kdx = p.kdt / p.dxx;
+    if constexpr (SCHEME == KP07_DIMSPLIT || SCHEME == HLL2) {
+        const SwePhys P{p.theta, p.g, p.half_g, p.kdt / (2.0f * p.dxx)};
+        walk_mh<SwePhys, SCHEME == HLL2, SWAP, PS>(line, step, a, b, pre, P, kdx);
+    } else if constexpr (SCHEME == EE2D) {
+        const EulerPhys P{p.theta, p.gamma, p.kdt / (2.0f * p.dxx)};
+        // x sweeps use HLL, y sweeps central-upwind (GPUSimulators/cuda/EE2D_KP07_dimsplit.cu:62, :106)
+        walk_mh<EulerPhys, !SWAP, SWAP, PS>(line, step, a, b, pre, P, kdx);
+    } else if constexpr (SCHEME == WAF) {
+        walk_waf<SWAP, PS>(line, step, a, b, pre, p.g, p.half_g, p.inv_g, kdx, kdx);
+    } else {
+        walk_2pt<SCHEME, SWAP, PS>(line, step, a, b, pre, p.g, p.half_g, p.dxx / (2.0f * p.kdt),
+                                   p.kdt / (2.0f * p.dxx), kdx);
+    }
+}
+
+// x sweep over tile rows [t0, t1): interior columns updated in place.
+template <int SCHEME, int NV, int W, int H, int NT>
+__device__ __forceinline__ void sweep_x(float* Qs, int t0, int t1, const SweepPar& p) {
+    constexpr int SP = W + 8, PS = SP * (H + 4), NSEG = 4, R = W / NSEG;
+    const int item = threadIdx.x;
+    const bool has = item < (t1 - t0) * NSEG;
+    const int t = t0 + item / NSEG, seg = item % NSEG;
+    const int a = 4 + seg * R, b = a + R;
+    float* line = Qs + t * SP;
+    float pre[4][NV];
+    if (has) {
+        ld_cell<NV, false, PS>(line, a - 2, 1, pre[0]);
+        ld_cell<NV, false, PS>(line, a - 1, 1, pre[1]);
+        ld_cell<NV, false, PS>(line, b, 1, pre[2]);
+        ld_cell<NV, false, PS>(line, b + 1, 1, pre[3]);
+    }
+    __syncthreads();
+    if (has) walk_line<SCHEME, false, PS>(line, 1, a, b, pre, p);
+    __syncthreads();
+}
+
+// y sweep over tile columns [s0, s1): interior rows updated in place.
+template <int SCHEME, int NV, int W, int H, int NT>
+__device__ __forceinline__ void sweep_y(float* Qs, int s0, int s1, const SweepPar& p) {
+    constexpr int SP = W + 8, PS = SP * (H + 4);
+    constexpr int NSEG = NT / (W + 4), R = H / NSEG;
+    const int ncols = s1 - s0;
+    const int item = threadIdx.x;
+    const bool has = item < ncols * NSEG;
+    const int s = s0 + item % ncols, seg = item / ncols;
+    const int a = 2 + seg * R, b = a + R;
+    float* line = Qs + s;
+    float pre[4][NV];
+    if (has) {
+        ld_cell<NV, true, PS>(line, a - 2, SP, pre[0]);
+        ld_cell<NV, true, PS>(line, a - 1, SP, pre[1]);
+        ld_cell<NV, true, PS>(line, b, SP, pre[2]);
+        ld_cell<NV, true, PS>(line, b + 1, SP, pre[3]);
+    }
+    __syncthreads();
+    if (has) walk_line<SCHEME, true, PS>(line, SP, a, b, pre, p);
+    __syncthreads();
+}
+
+// ------------------------------------------------------------------ split-scheme stage kernel
+
+template <int SCHEME, int W, int H, int NT>
+__global__ void __launch_bounds__(NT) dimsplit_stage_kernel(const __grid_constant__ StageArgs A) {
+    constexpr int NV = (SCHEME == EE2D) ? 4 : 3;
+    constexpr int G = (SCHEME == FORCE || SCHEME == HLL) ? 1 : 2;
+    constexpr int SP = W + 8, TR = H + 4, PS = SP * TR;
+    static_assert(W % 4 == 0 && (W / 4) % 2 == 1, "row segments must be odd for conflict-free x sweeps");
+    static_assert(TR * 4 <= NT, "one x-sweep segment per thread");
+    static_assert(NT % (W + 4) == 0 && H % (NT / (W + 4)) == 0, "y-sweep segments must tile the block");
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    float* Qs = reinterpret_cast<float*>(smem_raw);
+    __shared__ __align__(8) uint64_t bar;
+
+    StepCtl sc = read_step(A);
+    if (!sc.active) return;
+    if (SCHEME == WAF) sc.do_cfl = false;  // WAFKernel has no CFL output (GPUSimulators/cuda/SWE2D_WAF.cu:103-119)
+    const int x0 = blockIdx.x * W, y0 = blockIdx.y * H;
+    float my_cfl = __int_as_float(0x7f800000);
+    double my_sums[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) my_sums[v] = 0.0;
+    const bool sums = A.want_sums && A.is_last;
+
+    if (load_tile<NV, SP, TR>(Qs, A, sc.cur, x0, y0, &bar)) {
+        if (x0 == 0 || x0 + W + 2 > A.nx || y0 == 0 || y0 + H + 2 > A.ny)
+            apply_boundary<NV, W, H, NT>(Qs, A, sc.cur, x0, y0);
+
+        SweepPar p;
+        p.theta = A.theta;
+        p.g = A.g;
+        p.half_g = 0.5f * A.g;
+        p.inv_g = 1.0f / A.g;
+        p.gamma = A.gamma;
+        p.kdt = sc.dt * A.dt_scale;
+        const bool x_first = (SCHEME == FORCE || SCHEME == HLL) ? true : (A.substep == 0);
+        if (x_first) {
+            p.dxx = A.dx;
+            sweep_x<SCHEME, NV, W, H, NT>(Qs, 2 - G, H + 2 + G, p);
+            p.dxx = A.dy;
+            sweep_y<SCHEME, NV, W, H, NT>(Qs, 4, W + 4, p);
+        } else {
+            p.dxx = A.dy;
+            sweep_y<SCHEME, NV, W, H, NT>(Qs, 4 - G, W + 4 + G, p);
+            p.dxx = A.dx;
+            sweep_x<SCHEME, NV, W, H, NT>(Qs, 2, H + 2, p);
+        }
+
+        // copy-out of the interior (+ gravity source, CFL, sums)
+        constexpr int QW = W / 4;
+        const float gg = (SCHEME == EE2D) ? A.gamma : A.g;
+        const int out = sc.cur ^ 1;
+        for (int i = threadIdx.x; i < H * QW; i += NT) {
+            const int r = i / QW, q = i - r * QW;
+            const int y = y0 + r, x = x0 + 4 * q;
+            if (y >= A.ny || x >= A.nx) continue;
+            float4 val[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v)
+                val[v] = *reinterpret_cast<const float4*>(Qs + v * PS + (r + 2) * SP + 4 + 4 * q);
+            if (SCHEME == EE2D) {
+                if (A.g > 0.0f) {
+                    // gravity source (GPUSimulators/cuda/EE2D_KP07_dimsplit.cu:197-205)
+                    const float gdt = A.g;
+                    float* r0 = &val[0].x;
+                    float* r2 = &val[2].x;
+                    float* r3 = &val[3].x;
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const float rho_v = r2[j];
+                        r2[j] = r2[j] - gdt * r0[j] * p.kdt;
+                        r3[j] = r3[j] - gdt * rho_v * p.kdt;
+                    }
+                }
+            }
+            const long long gi = cell_index(y, x, A.pitch);
+            const int nvalid = min(4, A.nx - x);
+            if (nvalid == 4) {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) *reinterpret_cast<float4*>(A.buf[out][v] + gi) = val[v];
+            } else {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    const float* e = &val[v].x;
+                    for (int j = 0; j < nvalid; ++j) A.buf[out][v][gi + j] = e[j];
+                }
+            }
+            if (sc.do_cfl || sums) {
+                const float* h = &val[0].x;
+                const float* hu = &val[1].x;
+                const float* hv = &val[2].x;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    if (j < nvalid) {
+                        if (sc.do_cfl) my_cfl = fminf(my_cfl, cell_cfl(h[j], hu[j], hv[j], A.dx, A.dy, gg));
+                        if (sums) {
+#pragma unroll
+                            for (int v = 0; v < NV; ++v) my_sums[v] += (double)(&val[v].x)[j];
+                        }
+                    }
+                }
+            }
+        }
+    }
+    stage_epilogue<NT, NV>(A, sc, my_cfl, my_sums, sums);
+}
+
+// ------------------------------------------------------------------ unsplit stage kernel (LxF, KP07)
+
+// Phase 1 computes the x-face fluxes of the interior rows into shared memory
+// (lanes along x); phase 2 walks columns, computes the y-face fluxes on the fly
+// and writes the updated cells straight to global memory
+// (GPUSimulators/cuda/SWE2D_LxF.cu:137-153, SWE2D_KP07.cu:187-225).
+template <int SCHEME, int W, int H, int NT>
+__global__ void __launch_bounds__(NT) unsplit_stage_kernel(const __grid_constant__ StageArgs A) {
+    constexpr int SP = W + 8, TR = H + 4, PS = SP * TR;
+    constexpr int FW = W + 1;            // faces per row
+    constexpr int NSEG = NT / W, R = H / NSEG;
+    static_assert(NSEG >= 1 && H % NSEG == 0, "column segments must tile the block");
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    float* Qs = reinterpret_cast<float*>(smem_raw);
+    float* Fs = Qs + 3 * PS;  // [3][H][FW]
+    __shared__ __align__(8) uint64_t bar;
+
+    const StepCtl sc = read_step(A);
+    if (!sc.active) return;
+    const int x0 = blockIdx.x * W, y0 = blockIdx.y * H;
+    float my_cfl = __int_as_float(0x7f800000);
+    double my_sums[3] = {0.0, 0.0, 0.0};
+    const bool sums = A.want_sums && A.is_last;
+
+    if (load_tile<3, SP, TR>(Qs, A, sc.cur, x0, y0, &bar)) {
+        if (x0 == 0 || x0 + W + 2 > A.nx || y0 == 0 || y0 + H + 2 > A.ny)
+            apply_boundary<3, W, H, NT>(Qs, A, sc.cur, x0, y0);
+        const float kdt = sc.dt * A.dt_scale;
+        const float g = A.g, half_g = 0.5f * g, theta = A.theta;
+        const float k4x = A.dx / (4.0f * kdt), k4y = A.dy / (4.0f * kdt);
+
+        // phase 1: x faces; face f of row r lies between tile columns 3+f and 4+f.
+        for (int i = threadIdx.x; i < H * FW; i += NT) {
+            const int r = i / FW, f = i - r * FW;
+            const float* row = Qs + (r + 2) * SP;
+            float F[3];
+            if (SCHEME == LXF) {
+                const SweFace l = swe_face(row[3 + f], row[PS + 3 + f], row[2 * PS + 3 + f], g, half_g);
+                const SweFace rr = swe_face(row[4 + f], row[PS + 4 + f], row[2 * PS + 4 + f], g, half_g);
+                swe_lxf_2d(l, rr, k4x, F);
+            } else {
+                float qm[3], qp[3];
+#pragma unroll
+                for (int v = 0; v < 3; ++v) {
+                    const float* c = row + v * PS + 3 + f;
+                    qm[v] = fmaf(0.5f, minmod_slope(c[-1], c[0], c[1], theta), c[0]);
+                    qp[v] = fmaf(-0.5f, minmod_slope(c[0], c[1], c[2], theta), c[1]);
+                }
+                const SweFace l = swe_face(qm[0], qm[1], qm[2], g, half_g);
+                const SweFace rr = swe_face(qp[0], qp[1], qp[2], g, half_g);
+                swe_central_upwind(l, rr, F);
+            }
+#pragma unroll
+            for (int v = 0; v < 3; ++v) Fs[(v * H + r) * FW + f] = F[v];
+        }
+        __syncthreads();
+
+        // phase 2: one column segment per thread
+        const int out = sc.cur ^ 1;
+        const bool blend = (SCHEME == KP07) && A.order == 2 && A.substep == 1;
+        const int item = threadIdx.x;
+        if (item < W * NSEG) {
+            const int i = item % W, seg = item / W;
+            const int x = x0 + i;
+            const int s = 4 + i;
+            const int a = 2 + seg * R, b = a + R;  // tile rows updated
+            const float kdx = kdt / A.dx, kdy = kdt / A.dy;
+            // y-face state of row m toward north (n) and toward south (s), swapped (h, hv, hu)
+            auto qcell = [&](int t, float (&q)[3]) {
+                q[0] = Qs[t * SP + s];
+                q[1] = Qs[2 * PS + t * SP + s];
+                q[2] = Qs[PS + t * SP + s];
+            };
+            SweFace north_prev;  // north face state of row m-1
+            auto face_states = [&](int t, SweFace& sface, SweFace& nface) {
+                if (SCHEME == LXF) {
+                    float q[3];
+                    qcell(t, q);
+                    sface = nface = swe_face(q[0], q[1], q[2], g, half_g);
+                } else {
+                    float qm[3], q0[3], qp[3], sv[3], nv[3];
+                    qcell(t - 1, qm);
+                    qcell(t, q0);
+                    qcell(t + 1, qp);
+#pragma unroll
+                    for (int v = 0; v < 3; ++v) {
+                        const float sl = minmod_slope(qm[v], q0[v], qp[v], theta);
+                        sv[v] = fmaf(-0.5f, sl, q0[v]);
+                        nv[v] = fmaf(0.5f, sl, q0[v]);
+                    }
+                    sface = swe_face(sv[0], sv[1], sv[2], g, half_g);
+                    nface = swe_face(nv[0], nv[1], nv[2], g, half_g);
+                }
+            };
+            auto yflux = [&](const SweFace& l, const SweFace& r, float (&Gf)[3]) {
+                float tmp[3];
+                if (SCHEME == LXF) swe_lxf_2d(l, r, k4y, tmp);
+                else swe_central_upwind(l, r, tmp);
+                Gf[0] = tmp[0];  // swap back to (h, hu, hv)
+                Gf[1] = tmp[2];
+                Gf[2] = tmp[1];
+            };
+            {
+                SweFace sdummy;
+                face_states(a - 1, sdummy, north_prev);
+            }
+            SweFace s_cur, n_cur;
+            face_states(a, s_cur, n_cur);
+            float Gs[3];
+            yflux(north_prev, s_cur, Gs);  // south face of row a
+            for (int t = a; t < b; ++t) {
+                SweFace s_nxt, n_nxt;
+                face_states(t + 1, s_nxt, n_nxt);
+                float Gn[3];
+                yflux(n_cur, s_nxt, Gn);  // north face of row t
+                const int y = y0 + t - 2;
+                const int r = t - 2;
+                if (x < A.nx && y < A.ny) {
+                    float qn[3];
+                    const long long gi = cell_index(y, x, A.pitch);
+#pragma unroll
+                    for (int v = 0; v < 3; ++v) {
+                        const float q = Qs[v * PS + t * SP + s];
+                        const float Fw = Fs[(v * H + r) * FW + i], Fe = Fs[(v * H + r) * FW + i + 1];
+                        qn[v] = q + ((Fw - Fe) * kdx + (Gs[v] - Gn[v]) * kdy);
+                    }
+#pragma unroll
+                    for (int v = 0; v < 3; ++v) {
+                        float* dst = A.buf[out][v] + gi;
+                        const float o = blend ? 0.5f * (*dst + qn[v]) : qn[v];
+                        *dst = o;
+                        if (sums) my_sums[v] += (double)o;
+                    }
+                    if (sc.do_cfl) my_cfl = fminf(my_cfl, cell_cfl(qn[0], qn[1], qn[2], A.dx, A.dy, g));
+                }
+#pragma unroll
+                for (int v = 0; v < 3; ++v) Gs[v] = Gn[v];
+                s_cur = s_nxt;
+                n_cur = n_nxt;
+            }
+        }
+    }
+    stage_epilogue<NT, 3>(A, sc, my_cfl, my_sums, sums);
+}
+
+}  // namespace fv

@@ -1,0 +1,155 @@
+/*
+ * fvgpu.h -- C ABI of libfvgpu.so, the B200 (sm_100a) implementation of the
+ * GPUSimulators time-step path (babrodtk/FiniteVolumeGPU).
+ *
+ * Every entry point returns an int status (FV_OK == 0); the message of the
+ * last failure on the calling thread is available from fv_last_error().
+ * No C++ exception crosses this boundary.  All host arrays are float32,
+ * C-ordered, row pitch given in elements.
+ *
+ * Each declaration names the reference interface it replaces (paths relative
+ * to the reference project).
+ */
+#ifndef FVGPU_H
+#define FVGPU_H
+
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define FV_API __attribute__((visibility("default")))
+#else
+#define FV_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FV_OK 0
+#define FV_ERR_INVALID 1     /* bad argument: shape, size, pointer (reference: AssertionError) */
+#define FV_ERR_UNSUPPORTED 2 /* e.g. Neumann boundaries (reference: NotImplementedError, Simulator.py:68-72) */
+#define FV_ERR_CUDA 3        /* a CUDA runtime call failed */
+#define FV_ERR_DEVICE 4      /* a kernel's bounded wait gave up; the simulation state is not trustworthy */
+#define FV_ERR_NOMEM 5       /* device or pinned host allocation failed */
+
+/* Scheme ids: the reference classes GPUSimulators/{LxF,FORCE,HLL,HLL2,WAF,KP07,
+ * KP07_dimsplit,EE2D_KP07_dimsplit}.py. */
+enum fv_scheme {
+    FV_LXF = 0,
+    FV_FORCE = 1,
+    FV_HLL = 2,
+    FV_HLL2 = 3,
+    FV_WAF = 4,
+    FV_KP07 = 5,
+    FV_KP07_DIMSPLIT = 6,
+    FV_EE2D_KP07_DIMSPLIT = 7
+};
+
+typedef struct fv_context fv_context;
+typedef struct fv_sim fv_sim;
+
+/* Scheme parameters (constructor keywords of the reference classes). */
+typedef struct fv_params {
+    float g;         /* gravitational acceleration (all classes) */
+    float gamma;     /* ratio of specific heats (EE2D_KP07_dimsplit only) */
+    float theta;     /* minmod parameter (HLL2, KP07, KP07_dimsplit, EE2D) */
+    float cfl_scale; /* Courant number used by simulate() */
+    int order;       /* Runge-Kutta order of KP07 (1 or 2) */
+    int tile;        /* tile configuration index, or -1 for the scheme default */
+} fv_params;
+
+/* Library version (major*10000 + minor*100 + patch). */
+FV_API int fv_version(void);
+
+/* Message of the last failing call on this thread ("" if none). */
+FV_API const char* fv_last_error(void);
+
+/* Replaces CudaContext(device=...) (GPUSimulators/CudaContext.py:47-101):
+ * selects the device and prepares the kernels.  No JIT: kernels are built
+ * ahead of time for sm_100a. */
+FV_API int fv_context_create(int device, fv_context** out);
+FV_API int fv_context_destroy(fv_context* ctx);
+/* Device name, e.g. "NVIDIA B200" (CudaContext.__str__, CudaContext.py:103-108). */
+FV_API int fv_context_device_name(fv_context* ctx, char* buf, int len);
+
+/* Replaces the constructors of the eight scheme classes (e.g.
+ * GPUSimulators/KP07_dimsplit.py:55-106): uploads the initial state into two
+ * state buffers (u0 with the data, u1 zeroed, as ArakawaA2D does,
+ * GPUSimulators/Common.py:741-755) and seeds the CFL value with the host
+ * estimate min(dx/(|u|+sqrt(g h)), dy/(|v|+sqrt(g h))) (KP07_dimsplit.py:102-106;
+ * sqrt(gamma*rho) for Euler, EE2D_KP07_dimsplit.py:105-108).
+ * host_vars: nv pointers (3, or 4 for Euler) to arrays of host_rows x host_cols
+ * floats, either (ny, nx) interior data or (ny+2g, nx+2g) data with ghost cells
+ * (Common.py:524-531), with g = 1 for LxF/FORCE/HLL and 2 otherwise.
+ * bc: BoundaryCondition.asCodedInt() (GPUSimulators/Simulator.py:78-92). */
+FV_API int fv_sim_create(fv_context* ctx, int scheme, int nx, int ny, float dx, float dy, const fv_params* params, int bc,
+                  const float* const* host_vars, int host_rows, int host_cols, fv_sim** out);
+FV_API int fv_sim_destroy(fv_sim* sim);
+
+/* Replaces <Scheme>.substep(dt, step_number) (e.g. KP07_dimsplit.py:108-126):
+ * one stage-kernel launch and the buffer swap.  The split schemes apply dt/2,
+ * as the reference classes do.  Always writes the CFL field. */
+FV_API int fv_sim_substep(fv_sim* sim, float dt, int step_number);
+
+/* Replaces BaseSimulator.step(dt) (GPUSimulators/Simulator.py:220-228). */
+FV_API int fv_sim_step(fv_sim* sim, float dt);
+
+/* Replaces BaseSimulator.simulate(t, dt=None) (GPUSimulators/Simulator.py:176-217):
+ * advances until simTime() >= start + t.  use_dt == 0: dt = computeDt()*cfl_scale,
+ * recomputed every 100 steps; use_dt != 0: the given dt.  The step sequence runs
+ * as CUDA graphs with the time step kept on the device. */
+FV_API int fv_sim_simulate(fv_sim* sim, double t, float dt, int use_dt);
+
+/* Advances exactly n_steps steps with the simulate() dt schedule and no end
+ * time (benchmark helper; same kernels and graphs as fv_sim_simulate). */
+FV_API int fv_sim_advance(fv_sim* sim, long long n_steps);
+
+/* Replaces <Scheme>.computeDt() (e.g. KP07_dimsplit.py:135-137):
+ * min(cfl_data) times the scheme's factor. */
+FV_API int fv_sim_compute_dt(fv_sim* sim, float* dt);
+
+/* Replaces BaseSimulator.download(variables) / ArakawaA2D.download
+ * (GPUSimulators/Common.py:757-770): copies the interior (ny x nx) of variable
+ * `var` of u0 into host memory (row pitch in floats) and waits for the copy,
+ * which the reference leaves unsynchronised (Common.py:769). */
+FV_API int fv_sim_download(fv_sim* sim, int var, float* host, int host_pitch);
+
+/* Uploads new interior data (ny x nx) for variable `var` of u0 (CudaArray2D.upload,
+ * GPUSimulators/Common.py:587-616). */
+FV_API int fv_sim_upload(fv_sim* sim, int var, const float* host, int host_pitch);
+
+/* simTime(), simSteps() and the current dt (Simulator.py:236-240). */
+FV_API int fv_sim_time(fv_sim* sim, double* t, long long* nt, float* dt);
+
+/* FP64 sums of each conserved variable over the interior of u0 (no
+ * counterpart in the reference; supports its conservation checks). */
+FV_API int fv_sim_conservation(fv_sim* sim, double* sums);
+
+/* Replaces check() (GPUSimulators/Common.py:772-780): *has_nan != 0 if any
+ * value of u0 or u1 (ghost cells included) is NaN. */
+FV_API int fv_sim_check(fv_sim* sim, int* has_nan);
+
+/* synchronize() (Simulator.py:233-234). */
+FV_API int fv_sim_synchronize(fv_sim* sim);
+
+/* setBoundaryConditions (Simulator.py:245-247). */
+FV_API int fv_sim_set_boundary_conditions(fv_sim* sim, int bc);
+
+/* Device-side launches per step of the graph path, and the tile used
+ * (introspection for benchmarks and tests). */
+FV_API int fv_sim_info(fv_sim* sim, int* tile_w, int* tile_h, int* threads, int* launches_per_step);
+
+/* Average device time of the stage kernels over the last fv_sim_advance
+ * call, measured with CUDA events on the simulation's stream (0 if unknown). */
+FV_API int fv_sim_last_advance_ms(fv_sim* sim, double* ms);
+
+/* Pinned host memory for end-to-end transfers (CudaArray2D uses page-locked
+ * buffers for downloads, Common.py:563-564). */
+FV_API int fv_host_alloc(void** ptr, size_t bytes);
+FV_API int fv_host_free(void* ptr);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FVGPU_H */

@@ -17,8 +17,9 @@ C restatement of the stage kernels in ``fv_oracle.cpp``:
   ``u0`` holds the upload, ``u1`` starts as zeros, including ghost cells, and the
   kernels never write ghost cells;
 * the initial CFL fill computed on the host (e.g. KP07_dimsplit.py:102-106) and
-  each class's ``computeDt`` factor (section "Scheme semantics" in DESIGN.md of
-  this repository lists them).
+  each class's ``computeDt`` factor: 1.0 for FORCE (GPUSimulators/FORCE.py:129),
+  0.5**(order-1) for KP07 (GPUSimulators/KP07.py:138), 0.5 for the others
+  (e.g. GPUSimulators/KP07_dimsplit.py:137).
 
 EE2D_KP07_dimsplit swaps its buffers after every substep here, which is what
 MPISimulator does (GPUSimulators/MPISimulator.py:326); the plain reference class
@@ -92,7 +93,7 @@ def num_vars(scheme: str) -> int:
 
 
 def substep_factor(scheme: str) -> float:
-    """Factor applied by each class's computeDt to min(cfl_data) (section 2.4 of the survey)."""
+    """Factor each class's computeDt applies to min(cfl_data) (FORCE.py:129; 0.5 elsewhere but KP07)."""
     return 1.0 if scheme == "FORCE" else 0.5
 
 
@@ -167,7 +168,11 @@ class OracleSim:
         self.cfl = T(min(dt_x, dt_y))
         self.t = 0.0
         self.nt = 0
-        self.dt = None
+        # Only EE2D_KP07_dimsplit.py:107 sets dt in its constructor; the other
+        # classes have no dt until simulate() computes one.  Seeding it with the
+        # initial CFL estimate everywhere keeps simulate() usable after manual
+        # step() calls.
+        self.dt = self.cfl
 
     # -- Simulator.py:176-217
     def simulate(self, t, dt=None):
@@ -201,12 +206,15 @@ class OracleSim:
         T = self.dtype.type
         dt = T(dt)
         kdt = T(dt * T(0.5)) if self.scheme in DIMSPLIT_HALF_DT else dt
-        cfl = oracle_substep(self.scheme, self.u0, self.u1, self.nx, self.ny, self.dx, self.dy, kdt, self.g,
-                             self.gamma, self.theta, int(step_number), self.order, self.bc,
-                             want_cfl=True, nthreads=self.nthreads)
+        cfl = self._launch(kdt, int(step_number))
         if self.scheme != "WAF":  # WAFKernel writes no CFL (GPUSimulators/cuda/SWE2D_WAF.cu:103-119)
             self.cfl = cfl
         self.u0, self.u1 = self.u1, self.u0
+
+    def _launch(self, kdt, step_number):
+        return oracle_substep(self.scheme, self.u0, self.u1, self.nx, self.ny, self.dx, self.dy, kdt, self.g,
+                              self.gamma, self.theta, step_number, self.order, self.bc,
+                              want_cfl=True, nthreads=self.nthreads)
 
     def computeDt(self):
         T = self.dtype.type

@@ -1,0 +1,121 @@
+"""CPU tests of the drop-in boundary: the C ABI library loads and exports every
+declared entry point, and the Python layer keeps the reference's codecs and
+error behaviour without touching a GPU."""
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+import finitevolumegpu_b200 as fv
+from finitevolumegpu_b200 import _lib
+from finitevolumegpu_b200.Simulator import BoundaryCondition, stepOrderToCodedInt
+
+HEADER = os.path.join(ROOT, "include", "fvgpu.h")
+
+
+def declared_symbols():
+    src = open(HEADER).read()
+    return sorted(set(re.findall(r"^FV_API\s+[\w\s\*]+?\b(fv_\w+)\s*\(", src, flags=re.M)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    assert len(syms) >= 20
+    for s in ("fv_sim_create", "fv_sim_simulate", "fv_sim_step", "fv_sim_substep", "fv_sim_download",
+              "fv_sim_compute_dt", "fv_context_create", "fv_last_error"):
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.lib()
+    for s in declared_symbols():
+        assert hasattr(L, s), s
+    assert L.fv_version() >= 100
+
+
+def test_python_binding_covers_header():
+    assert set(declared_symbols()) <= set(_lib._SIGNATURES)
+
+
+def test_oracle_library_exports():
+    from oracle import oracle
+
+    L = oracle.lib()
+    for s in ("fvo_substep_f32", "fvo_substep_f64", "fvo_ghost_cells", "fvo_num_vars"):
+        assert hasattr(L, s)
+    assert L.fvo_ghost_cells(0) == 1 and L.fvo_ghost_cells(6) == 2 and L.fvo_num_vars(7) == 4
+
+
+def test_boundary_condition_codec():
+    T = BoundaryCondition.Type
+    bc = BoundaryCondition({"north": T.Periodic, "south": T.Reflective, "east": T.Dirichlet, "west": T.Periodic})
+    code = int(bc.asCodedInt())
+    assert code == (2 << 24) | (3 << 16) | (0 << 8) | 2
+    back = BoundaryCondition.getTypes(code)
+    assert back == {"north": T.Periodic, "south": T.Reflective, "east": T.Dirichlet, "west": T.Periodic}
+    assert int(BoundaryCondition().asCodedInt()) == 0x03030303
+
+
+def test_neumann_rejected():
+    T = BoundaryCondition.Type
+    with pytest.raises(NotImplementedError):
+        BoundaryCondition({"north": T.Neumann, "south": T.Reflective, "east": T.Reflective, "west": T.Reflective})
+
+
+def test_step_order_codec():
+    assert int(stepOrderToCodedInt(1, 2)) == (1 << 16) | 2
+    assert int(stepOrderToCodedInt(0, 1)) == 1
+
+
+class _NoGpuContext:
+    handle = None
+    autotuner = None
+    device_name = "none"
+
+
+@pytest.mark.parametrize("shape", [(10, 9), (13, 13), (12, 10, 1)])
+def test_constructor_rejects_bad_shapes(shape):
+    a = np.ones(shape, np.float32)
+    with pytest.raises(AssertionError):
+        fv.KP07_dimsplit.KP07_dimsplit(_NoGpuContext(), a, a, a, 10, 8, 1.0, 1.0, 9.81)
+
+
+def test_constructor_rejects_wrong_itemsize():
+    a = np.ones((8, 10), np.float64)
+    with pytest.raises(AssertionError):
+        fv.HLL.HLL(_NoGpuContext(), a, a, a, 10, 8, 1.0, 1.0, 9.81)
+
+
+def test_class_signatures_match_reference():
+    import inspect
+
+    sig = inspect.signature(fv.KP07_dimsplit.KP07_dimsplit.__init__)
+    assert list(sig.parameters)[1:] == ["context", "h0", "hu0", "hv0", "nx", "ny", "dx", "dy", "g", "theta",
+                                        "cfl_scale", "boundary_conditions", "block_width", "block_height"]
+    assert sig.parameters["theta"].default == 1.3 and sig.parameters["cfl_scale"].default == 0.9
+    sig = inspect.signature(fv.EE2D_KP07_dimsplit.EE2D_KP07_dimsplit.__init__)
+    assert list(sig.parameters)[1:11] == ["context", "rho", "rho_u", "rho_v", "E", "nx", "ny", "dx", "dy", "g"]
+    assert sig.parameters["block_height"].default == 8
+    assert inspect.signature(fv.HLL2.HLL2.__init__).parameters["theta"].default == 1.8
+    assert inspect.signature(fv.KP07.KP07.__init__).parameters["order"].default == 2
+    for name in ("LxF", "FORCE", "HLL", "WAF"):
+        assert "theta" not in inspect.signature(fv.SCHEMES[name].__init__).parameters
+
+
+def test_no_cpu_fallback():
+    """Without a usable GPU the context raises; nothing silently computes on the host."""
+    import subprocess
+    import sys
+
+    code = ("import sys; sys.path.insert(0, %r)\n"
+            "from finitevolumegpu_b200 import CudaContext\n"
+            "try:\n    CudaContext.CudaContext()\nexcept Exception as e:\n    print('raised', type(e).__name__)\n"
+            "else:\n    print('ok')\n" % ROOT)
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=dict(
+        os.environ, CUDA_VISIBLE_DEVICES=""))
+    assert "raised" in out.stdout, out.stdout + out.stderr

@@ -1,0 +1,49 @@
+"""Speed of the stage kernels against the reference's own kernels on the same
+B200 and the same 4096-cell-wide inputs (device time per full step, CUDA
+events).  The test fails if libfvgpu is slower than the reference kernels."""
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import dam_break, kelvin_helmholtz
+
+import finitevolumegpu_b200 as fv
+from oracle import ref_kernels
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("scheme", ["KP07_dimsplit", "HLL2", "WAF", "FORCE", "HLL", "LxF", "KP07",
+                                    "EE2D_KP07_dimsplit"])
+def test_faster_than_reference_kernels(ctx, scheme):
+    if scheme == "EE2D_KP07_dimsplit":
+        nx, ny = 4096, 2048
+        from conftest import kelvin_helmholtz as kh
+        q = kh(nx, ny)
+        sim = fv.SCHEMES[scheme](ctx, *q, nx, ny, 1.0 / nx, 1.0 / ny, 0.0, 1.4,
+                                 boundary_conditions=fv.BoundaryCondition(
+                                     fv.BoundaryCondition.getTypes(0x02020202)))
+        ref = ref_kernels.RefKernelSim(scheme, q, nx, ny, 1.0 / nx, 1.0 / ny, 0.0, gamma=1.4, bc=0x02020202)
+    else:
+        nx, ny = 4096, 4096
+        q = list(dam_break(nx, ny))
+        sim = fv.SCHEMES[scheme](ctx, *q, nx, ny, 1.0, 1.0, 9.81)
+        ref = ref_kernels.RefKernelSim(scheme, q, nx, ny, 1.0, 1.0, 9.81)
+    dt = np.float32(ref.computeDt() * np.float32(0.5))
+    ref.time_steps(3, dt)
+    ref_ms = ref.time_steps(20, dt)
+    sim.advance(3)
+    sim.advance(20)
+    my_ms = sim.last_advance_ms()
+    rec = {"scheme": scheme, "nx": nx, "ny": ny, "ref_ms_per_step": ref_ms, "fvgpu_ms_per_step": my_ms,
+           "speedup": ref_ms / my_ms, "ref_block": [ref.bw, ref.bh], "tile": sim.tile_info()}
+    print(json.dumps(rec))
+    out = os.environ.get("FVGPU_TIMING_OUT")
+    if out:
+        with open(out, "a") as f:
+            f.write(json.dumps(rec) + "\n")
+    ref.close()
+    assert my_ms < ref_ms, rec
