@@ -156,9 +156,9 @@ class RefKernelSim(OracleSim):
         return out
 
     def close(self):
-        for p in self.d0 + self.d1 + [self.dcfl]:
+        for p in self.d0 + self.d1 + ([self.dcfl] if self.dcfl is not None else []):
             self.L.ref_free(p)
-        self.d0, self.d1 = [], []
+        self.d0, self.d1, self.dcfl = [], [], None
 
     def __del__(self):
         try:

@@ -67,6 +67,7 @@ int ref_event_destroy(void* ev) { return check(cudaEventDestroy((cudaEvent_t)ev)
 // in/out: nv device pointers; pitch in bytes; cfl: device float[grid.x*grid.y] or NULL.
 int ref_substep(int nx, int ny, float dx, float dy, float dt, float g, float gamma, float theta, int step,
                 int order, int bc, float* const* in, float* const* out, int pitch, float* cfl) {
+    (void)cudaGetLastError();  // clear any error left by an earlier, unrelated runtime call
     const dim3 block(BLOCK_WIDTH, BLOCK_HEIGHT);
     const dim3 grid((nx + BLOCK_WIDTH - 1) / BLOCK_WIDTH, (ny + BLOCK_HEIGHT - 1) / BLOCK_HEIGHT);
     (void)gamma;
