@@ -63,3 +63,23 @@ def rel_l1(a, b):
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
     return float(np.sum(np.abs(a - b)) / max(float(np.sum(np.abs(b))), 1e-30))
+
+
+def ulp_sensitivity(run, q):
+    """Spread of a run under a one-ulp nudge of the first input variable.
+
+    run(q) -> list of output arrays.  Returns per-variable (rel L-inf, rel L1)
+    between run(q) and run(q with q[0] nudged up by one ulp): the rounding
+    amplification of the scheme itself, used where a fixed bound would not
+    reflect the conditioning of the problem (WAF at shocks, states next to
+    zero-depth ghost cells).
+    """
+    a = run(q)
+    q2 = [np.array(x, copy=True) for x in q]
+    q2[0] = np.nextafter(q2[0], np.float32(np.inf)).astype(q2[0].dtype)
+    b = run(q2)
+    out = []
+    for x, y in zip(a, b):
+        m = np.isfinite(x) & np.isfinite(y)
+        out.append((rel_linf(x[m], y[m]) if m.any() else 0.0, rel_l1(x[m], y[m]) if m.any() else 0.0))
+    return out
