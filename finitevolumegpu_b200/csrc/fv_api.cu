@@ -153,6 +153,9 @@ __global__ void nan_scan_kernel(const float* __restrict__ a, long long n, int* _
 
 }  // namespace
 
+// Shared with the other translation units of the library (not exported).
+void fv_internal_set_error(const char* msg) { g_err = msg; }
+
 struct fv_context {
     int device = 0;
     int sm_count = 0;

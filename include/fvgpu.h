@@ -143,6 +143,25 @@ FV_API int fv_sim_info(fv_sim* sim, int* tile_w, int* tile_h, int* threads, int*
  * call, measured with CUDA events on the simulation's stream (0 if unknown). */
 FV_API int fv_sim_last_advance_ms(fv_sim* sim, double* ms);
 
+/* One KP07_dimsplit substep (GPUSimulators/cuda/SWE2D_KP07_dimsplit.cu semantics)
+ * that allocates no memory: for callers that may not call cudaMalloc, such as
+ * applications that own all device memory through their own pool, or loops
+ * that must not pay allocation latency or risk running out of memory mid-run.
+ * No counterpart in the reference.
+ * in/out: 3 device pointers (h, hu, hv), each (ny+4) x pitch floats, element
+ * (y, x) at [(y+2)*pitch + x+4], 16-byte aligned, pitch a multiple of 4 and
+ * >= nx+8; dt is the kernel dt (half the step dt, as KP07_dimsplit.py:109
+ * passes); step selects the sweep order; cfl_min (device float*, may be NULL)
+ * receives min over cells of min(dx/(|u|+sqrt(gh)), dy/(|v|+sqrt(gh))).
+ * Scratch is a static device array of about 33 KB per GPU, limiting a call to
+ * 8192 tiles of 124 x 60 cells (FV_ERR_INVALID beyond).  Calls that overlap on
+ * the GPU share that array and race.  The first call on a device performs its
+ * set-up (symbol lookup, kernel attribute); make it before any stream capture.
+ * Asynchronous on `stream` (a cudaStream_t, or NULL). */
+FV_API int fv_kp07_dimsplit_substep_noalloc(const float* const* in, float* const* out, int pitch, int nx, int ny,
+                                            float dx, float dy, float dt, float g, float theta, int step, int bc,
+                                            float* cfl_min, void* stream);
+
 /* Pinned host memory for end-to-end transfers (CudaArray2D uses page-locked
  * buffers for downloads, Common.py:563-564). */
 FV_API int fv_host_alloc(void** ptr, size_t bytes);
