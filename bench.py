@@ -179,6 +179,174 @@ def run_reference(args, rank, world):
     }
 
 
+def bump_ic(nx, ny, rng):
+    """Gaussian bump: h = 1 + A exp(-r^2/(2 sigma^2)), A ~ U(0.1, 0.5), centre ~ U(0.3, 0.7) x domain, sigma = 20 cells."""
+    A = rng.uniform(0.1, 0.5)
+    cx, cy = rng.uniform(0.3, 0.7) * nx, rng.uniform(0.3, 0.7) * ny
+    x = np.arange(nx, dtype=np.float32) + 0.5
+    y = np.arange(ny, dtype=np.float32) + 0.5
+    h = 1.0 + A * np.exp(-((x[None, :] - cx) ** 2 + (y[:, None] - cy) ** 2) / (2 * 20.0 ** 2))
+    z = np.zeros((ny, nx), np.float32)
+    return [h.astype(np.float32), z, z.copy()]
+
+
+def dam_ic(nx, ny, rng):
+    """Circular dam break: h = 1 inside R ~ U(0.1, 0.3) x width of the centre, 0.1 outside."""
+    R = rng.uniform(0.1, 0.3) * nx
+    x = np.arange(nx, dtype=np.float32) + 0.5 - nx / 2.0
+    y = np.arange(ny, dtype=np.float32) + 0.5 - ny / 2.0
+    h = np.where(x[None, :] ** 2 + y[:, None] ** 2 < R * R, 1.0, 0.1).astype(np.float32)
+    z = np.zeros((ny, nx), np.float32)
+    return [h, z, z.copy()]
+
+
+def kh_ic(nx, ny, rng, gamma=1.4):
+    """Kelvin-Helmholtz: rho = 2, u = +0.5 in the middle half band, rho = 1, u = -0.5 outside, p = 2.5,
+    v = 0.01 sin(4 pi x + phi) with seeded phase."""
+    phi = rng.uniform(0, 2 * np.pi)
+    yy = (np.arange(ny, dtype=np.float32) + 0.5) / ny
+    xx = (np.arange(nx, dtype=np.float32) + 0.5) / nx
+    band = ((yy >= 0.25) & (yy < 0.75))[:, None]
+    rho = np.where(band, 2.0, 1.0) * np.ones((1, nx))
+    u = np.where(band, 0.5, -0.5) * np.ones((1, nx))
+    v = 0.01 * np.sin(4 * np.pi * xx[None, :] + phi) * np.ones((ny, 1))
+    E = 2.5 / (gamma - 1.0) + 0.5 * rho * (u ** 2 + v ** 2)
+    return [a.astype(np.float32) for a in (rho, rho * u, rho * v, E)]
+
+
+def run_batched(ctx, n_inst=512, seed=4, check=4):
+    """Config 4: 512 KP07_dimsplit simulations, sides log-uniform in [64, 1024], bump or dam break,
+    t_end ~ U(5, 50): one batch of the persistent kernel vs the plain simulators one after another."""
+    from finitevolumegpu_b200 import KP07_dimsplit
+    from finitevolumegpu_b200.batch import Batch
+
+    rng = np.random.default_rng(seed)
+    cases = []
+    for i in range(n_inst):
+        nx = int(round(np.exp(rng.uniform(np.log(64), np.log(1024)))))
+        ny = int(round(np.exp(rng.uniform(np.log(64), np.log(1024)))))
+        q = bump_ic(nx, ny, rng) if rng.random() < 0.5 else dam_ic(nx, ny, rng)
+        cases.append((q, nx, ny, float(rng.uniform(5.0, 50.0))))
+    # batched: admit all, run to completion, download all
+    import torch
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b = Batch(ctx, "KP07_dimsplit", max_instances=n_inst)
+    slots = [b.add(q, nx, ny, 1.0, 1.0, t_end) for (q, nx, ny, t_end) in cases]
+    t_add = time.perf_counter()
+    dev_ms = 0.0
+    steps = 0
+    while True:
+        b.sync()
+        dev_ms += b.info()["last_run_ms"] if steps else 0.0
+        if all(b.status(s)["done"] for s in slots):
+            break
+        b.run(16)
+        steps += 16
+    t_run = time.perf_counter()
+    batched_out = [b.download(s) for s in slots]
+    nts = [b.status(s)["nt"] for s in slots]
+    t1 = time.perf_counter()
+    info = b.info()
+    del b
+    total = sum(nx * ny * nt for (q, nx, ny, t_end), nt in zip(cases, nts))
+    # plain: one simulator after the other
+    t2 = time.perf_counter()
+    max_diff = 0.0
+    plain_nts = []
+    for i, (q, nx, ny, t_end) in enumerate(cases):
+        sim = KP07_dimsplit.KP07_dimsplit(ctx, q[0], q[1], q[2], nx, ny, 1.0, 1.0, 9.81)
+        sim.simulate(t_end)
+        out = sim.download()
+        plain_nts.append(sim.simSteps())
+        for a, w in zip(out, batched_out[i]):
+            d = float(np.max(np.abs(a - w)))
+            max_diff = max(max_diff, d)
+        del sim
+    t3 = time.perf_counter()
+    # FP64 oracle on the smallest few simulations
+    l1 = 0.0
+    from oracle.oracle import OracleSim
+
+    small = sorted(range(n_inst), key=lambda i: cases[i][1] * cases[i][2])[:check]
+    for i in small:
+        q, nx, ny, t_end = cases[i]
+        o = OracleSim("KP07_dimsplit", q, nx, ny, 1.0, 1.0, 9.81, dtype=np.float64)
+        o.simulate(t_end)
+        for a, w in zip(batched_out[i], o.download()):
+            l1 = max(l1, float(np.sum(np.abs(a - w)) / max(np.sum(np.abs(w)), 1e-30)))
+    return {
+        "workload": "512 KP07_dimsplit simulations, sides log-uniform [64,1024] (seed %d), bump or dam break, "
+                    "t_end ~ U(5,50), each with its own CFL dt" % seed,
+        "cell_updates": total,
+        "batched_cell_updates_per_s": total / (t1 - t0),
+        "batched_device_cell_updates_per_s": total / (dev_ms / 1e3) if dev_ms else None,
+        "plain_cell_updates_per_s": total / (t3 - t2),
+        "speedup_vs_plain": (t3 - t2) / (t1 - t0),
+        "batched_s": {"admit": t_add - t0, "run": t_run - t_add, "download": t1 - t_run, "total": t1 - t0},
+        "plain_s": t3 - t2,
+        "steps_identical": nts == plain_nts,
+        "max_abs_diff_batched_vs_plain": max_diff,
+        "max_rel_l1_vs_fp64_oracle": l1,
+        "oracle_checked": len(small),
+        "tile": {k: info[k] for k in ("tile_w", "tile_h", "threads", "grid")},
+    }
+
+
+def run_served(ctx, n_req=400, rate=300.0, seed=5, plain_sample=60):
+    """Config 5: scenario requests with Poisson arrivals, scheme uniform over {KP07_dimsplit, HLL, EE2D},
+    sides log-uniform [128, 2048], t_end ~ U(1, 20), served with continuous batching under a 120 GB budget."""
+    from finitevolumegpu_b200 import SCHEMES, BoundaryCondition
+    from finitevolumegpu_b200.server import Request, Server
+
+    rng = np.random.default_rng(seed)
+    schemes = ["KP07_dimsplit", "HLL", "EE2D_KP07_dimsplit"]
+    periodic = BoundaryCondition(BoundaryCondition.getTypes(0x02020202))
+    reqs = []
+    t = 0.0
+    for i in range(n_req):
+        t += rng.exponential(1.0 / rate)
+        s = schemes[int(rng.integers(0, 3))]
+        nx = int(round(np.exp(rng.uniform(np.log(128), np.log(2048)))))
+        ny = int(round(np.exp(rng.uniform(np.log(128), np.log(2048)))))
+        if s == "EE2D_KP07_dimsplit":
+            q, bc = kh_ic(nx, ny, rng), periodic  # unit cells: the Kelvin-Helmholtz family scaled to the grid
+        else:
+            q, bc = (bump_ic(nx, ny, rng) if rng.random() < 0.5 else dam_ic(nx, ny, rng)), None
+        reqs.append(Request(i, s, q, nx, ny, 1.0, 1.0, float(rng.uniform(1.0, 20.0)), arrival=t,
+                            boundary_conditions=bc))
+    server = Server(ctx, budget_bytes=120e9, chunk_steps=8)
+    results, stats = server.serve(reqs)
+    # plain one-at-a-time path on a sample of the same requests
+    by_id = {r.rid: r for r in results}
+    t0 = time.perf_counter()
+    cells = 0
+    same = True
+    for r in reqs[:plain_sample]:
+        cls = SCHEMES[r.scheme]
+        kw = {} if r.boundary_conditions is None else {"boundary_conditions": r.boundary_conditions}
+        if r.scheme == "EE2D_KP07_dimsplit":
+            sim = cls(ctx, *r.variables, r.nx, r.ny, 1.0, 1.0, 0.0, 1.4, **kw)
+        else:
+            sim = cls(ctx, *r.variables, r.nx, r.ny, 1.0, 1.0, 9.81, **kw)
+        sim.simulate(r.t_end)
+        out = sim.download()
+        cells += r.nx * r.ny * sim.simSteps()
+        same = same and all(np.array_equal(a, w) for a, w in zip(out, by_id[r.rid].state))
+        del sim
+    plain_rate = cells / (time.perf_counter() - t0)
+    stats.update({
+        "workload": "%d requests, Poisson arrivals at %.0f/s (seed %d), schemes KP07_dimsplit/HLL/EE2D, sides "
+                    "log-uniform [128,2048], t_end ~ U(1,20), 120 GB budget" % (n_req, rate, seed),
+        "plain_one_at_a_time_cell_updates_per_s": plain_rate,
+        "plain_sample_requests": plain_sample,
+        "speedup_vs_plain": stats["cell_updates_per_s"] / plain_rate,
+        "results_identical_to_plain": same,
+    })
+    return stats
+
+
 def run_mine(args, rank, world, local_rank):
     import torch
 
@@ -280,6 +448,10 @@ def run_mine(args, rank, world, local_rank):
                "h2d_bytes_per_step": 3 * nbytes / args.steps, "d2h_bytes_per_step": 3 * nbytes / args.steps,
                "what": "constructor with pinned host upload + %d steps + download of the final state" % args.steps}
         result["e2e"] = e2e
+    if rank == 0 and world == 1 and not args.no_batched:
+        result["batched"] = run_batched(ctx)
+    if rank == 0 and world == 1 and not args.no_served:
+        result["served"] = run_served(ctx, n_req=args.served_requests, rate=args.served_rate)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline_leg()
     return result
@@ -293,6 +465,10 @@ def main():
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 512-simulation batched workload")
+    ap.add_argument("--no-served", action="store_true", help="skip the served request stream")
+    ap.add_argument("--served-requests", type=int, default=400)
+    ap.add_argument("--served-rate", type=float, default=300.0, help="Poisson arrival rate (requests/s)")
     ap.add_argument("--size", type=int, default=4096, help="grid side (the benchmark workload is 4096)")
     args = ap.parse_args()
     global NX, NY

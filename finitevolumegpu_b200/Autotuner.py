@@ -25,14 +25,23 @@ import numpy as np
 
 # Number of tile configurations per scheme in libfvgpu's kernel table.
 TILE_CONFIGS = {
-    "KP07_dimsplit": 2,
+    "KP07_dimsplit": 3,
     "HLL2": 2,
     "WAF": 2,
     "FORCE": 2,
-    "HLL": 2,
-    "EE2D_KP07_dimsplit": 2,
+    "HLL": 3,
+    "EE2D_KP07_dimsplit": 3,
     "LxF": 2,
     "KP07": 2,
+}
+# Tile configurations of the batched (persistent) kernels per scheme.
+BATCH_TILE_CONFIGS = {
+    "KP07_dimsplit": 3,
+    "HLL": 3,
+    "EE2D_KP07_dimsplit": 2,
+    "HLL2": 2,
+    "WAF": 2,
+    "FORCE": 2,
 }
 
 DEFAULT_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "autotuning_data.json")
@@ -72,6 +81,37 @@ class Autotuner(object):
             keys = sorted(entry, key=lambda s: abs(int(s.split("^")[1]) - k))
             best = entry[keys[0]]
         return int(best["tile"]) if best is not None else -1
+
+    def get_batch_tile(self, scheme, device_name="NVIDIA B200"):
+        """Tile configuration of the batched kernel, or -1 for the default."""
+        best = self._load().get(device_name, {}).get("batch:" + scheme)
+        return int(best["tile"]) if best is not None else -1
+
+    def benchmark_batch(self, context, scheme, scenarios, steps=40):
+        """Time every batched-kernel tile configuration on a list of scenarios
+        (variables, nx, ny, dx, dy) and record the fastest.  Returns {tile: ms per step}."""
+        from .batch import Batch
+
+        results = {}
+        for tile in range(BATCH_TILE_CONFIGS[scheme]):
+            b = Batch(context, scheme, tile=tile, max_instances=len(scenarios) + 1,
+                      g=0.0 if scheme == "EE2D_KP07_dimsplit" else 9.81)
+            for (q, nx, ny, dx, dy) in scenarios:
+                b.add(q, nx, ny, dx, dy, 1e30)
+            b.run(4)
+            b.sync()
+            b.run(steps)
+            b.sync()
+            results[tile] = b.info()["last_run_ms"] / steps
+            del b
+        best = min(results, key=results.get)
+        cache = self._load()
+        cache.setdefault(context.device_name, {})["batch:" + scheme] = {
+            "tile": best, "ms_per_step": results[best], "all": {str(k): v for k, v in results.items()},
+            "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime())}
+        with open(self.cache_file, "w") as f:
+            json.dump(cache, f, indent=1, sort_keys=True)
+        return results
 
     def benchmark(self, context, scheme, nx, ny, steps=20, warmup=5):
         """Time every tile configuration of `scheme` on an nx x ny dam break and

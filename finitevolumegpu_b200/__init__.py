@@ -7,7 +7,7 @@ Module layout mirrors the reference package so that
 simulator, as with GPUSimulators.
 """
 
-from . import Simulator, CudaContext  # noqa: F401
+from . import Simulator, CudaContext, batch  # noqa: F401
 from . import LxF, FORCE, HLL, HLL2, WAF, KP07, KP07_dimsplit, EE2D_KP07_dimsplit  # noqa: F401
 from .Simulator import BoundaryCondition, BaseSimulator  # noqa: F401
 

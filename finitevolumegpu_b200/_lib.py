@@ -81,6 +81,18 @@ _SIGNATURES = {
     "fv_sim_last_advance_ms": ([_P, ctypes.POINTER(_D)], _I),
     "fv_kp07_dimsplit_substep_noalloc": ([ctypes.POINTER(_FP), ctypes.POINTER(_FP), _I, _I, _I, _F, _F, _F, _F, _F,
                                           _I, _I, _FP, _P], _I),
+    "fv_batch_create": ([_P, _I, ctypes.POINTER(fv_params), _I, ctypes.POINTER(_P)], _I),
+    "fv_batch_destroy": ([_P], _I),
+    "fv_batch_add": ([_P, _I, _I, _F, _F, _I, ctypes.POINTER(_FP), _I, _I, _D, ctypes.POINTER(_I)], _I),
+    "fv_batch_remove": ([_P, _I], _I),
+    "fv_batch_run": ([_P, _I], _I),
+    "fv_batch_sync": ([_P], _I),
+    "fv_batch_status": ([_P, _I, ctypes.POINTER(_D), ctypes.POINTER(_LL), ctypes.POINTER(_F), ctypes.POINTER(_I)],
+                        _I),
+    "fv_batch_download": ([_P, _I, _I, _FP, _I], _I),
+    "fv_batch_info": ([_P, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(_I), ctypes.POINTER(_I),
+                       ctypes.POINTER(_D)], _I),
+    "fv_batch_tile": ([_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)], _I),
     "fv_host_alloc": ([ctypes.POINTER(_P), ctypes.c_size_t], _I),
     "fv_host_free": ([_P], _I),
 }

@@ -1,0 +1,121 @@
+"""Batched simulation: many grids of uneven sizes advanced together on one GPU.
+
+The reference runs one simulator per class instance, one kernel launch per
+substep.  A ``Batch`` holds many simulations of one dimensionally split scheme
+(FORCE, HLL, HLL2, WAF, KP07_dimsplit, EE2D_KP07_dimsplit) resident in HBM and
+advances all of them with one persistent kernel per substep that walks a tile
+work list; the step sequence is replayed from CUDA graphs.  Each simulation
+follows the reference's ``simulate(t_end)`` semantics on its own: its own CFL
+time step recomputed every 100 of its steps, its last step shortened to hit
+its t_end (GPUSimulators/Simulator.py:176-217).  Its result is therefore the
+same as that of a plain simulator run alone.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .Simulator import BoundaryCondition
+
+BATCH_SCHEMES = ("FORCE", "HLL", "HLL2", "WAF", "KP07_dimsplit", "EE2D_KP07_dimsplit")
+GHOST = {"FORCE": 1, "HLL": 1}
+DEFAULT_THETA = {"HLL2": 1.8}
+
+def _L():
+    return _lib.lib()
+
+
+class Batch(object):
+    """Simulations of one split scheme advanced together by a persistent kernel."""
+
+    def __init__(self, context, scheme, g=9.81, gamma=1.4, theta=None, cfl_scale=0.9, max_instances=1024,
+                 tile=None):
+        if scheme not in BATCH_SCHEMES:
+            raise ValueError("batched kernels exist for %s" % (BATCH_SCHEMES,))
+        self.context = context
+        self.scheme = scheme
+        self.nv = 4 if scheme == "EE2D_KP07_dimsplit" else 3
+        self.gc = GHOST.get(scheme, 2)
+        if tile is None:
+            tile = -1
+            tuner = getattr(context, "autotuner", None)
+            if tuner is not None and hasattr(tuner, "get_batch_tile"):
+                tile = tuner.get_batch_tile(scheme, context.device_name)
+        theta = DEFAULT_THETA.get(scheme, 1.3) if theta is None else theta
+        p = _lib.fv_params(float(g), float(gamma), float(theta), float(cfl_scale), 2, int(tile))
+        h = ctypes.c_void_p()
+        _lib.check(_L().fv_batch_create(context.handle, _lib.SCHEME_IDS[scheme], ctypes.byref(p), int(max_instances),
+                                        ctypes.byref(h)))
+        self._h = h
+        self.shapes = {}
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib._lib is not None:
+            _L().fv_batch_destroy(h)
+            self._h = None
+
+    def add(self, variables, nx, ny, dx, dy, t_end, boundary_conditions=None):
+        """Admit one simulation; returns its slot.  Raises MemoryError when the GPU has no room."""
+        bc = (boundary_conditions or BoundaryCondition()).asCodedInt()
+        arrays = []
+        for a in variables:
+            a = np.ascontiguousarray(a, dtype=np.float32)
+            assert a.shape in ((ny, nx), (ny + 2 * self.gc, nx + 2 * self.gc)), "Wrong shape of data %s" % (a.shape,)
+            arrays.append(a)
+        assert len(arrays) == self.nv
+        rows, cols = arrays[0].shape
+        ptrs = (_lib._FP * self.nv)(*[a.ctypes.data_as(_lib._FP) for a in arrays])
+        slot = ctypes.c_int()
+        _lib.check(_L().fv_batch_add(self._h, int(nx), int(ny), float(dx), float(dy), int(bc), ptrs, rows, cols,
+                                     float(t_end), ctypes.byref(slot)))
+        self.shapes[slot.value] = (int(ny), int(nx))
+        return slot.value
+
+    def remove(self, slot):
+        _lib.check(_L().fv_batch_remove(self._h, int(slot)))
+        self.shapes.pop(slot, None)
+
+    def run(self, n_steps):
+        """Queue n_steps steps for every simulation (asynchronous)."""
+        _lib.check(_L().fv_batch_run(self._h, int(n_steps)))
+
+    def sync(self):
+        _lib.check(_L().fv_batch_sync(self._h))
+
+    def status(self, slot):
+        t, nt, dt, done = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_float(), ctypes.c_int()
+        _lib.check(_L().fv_batch_status(self._h, int(slot), ctypes.byref(t), ctypes.byref(nt), ctypes.byref(dt),
+                                        ctypes.byref(done)))
+        return {"t": t.value, "nt": nt.value, "dt": dt.value, "done": bool(done.value)}
+
+    def download(self, slot):
+        ny, nx = self.shapes[slot]
+        out = []
+        for v in range(self.nv):
+            a = np.empty((ny, nx), dtype=np.float32)
+            _lib.check(_L().fv_batch_download(self._h, int(slot), v, a.ctypes.data_as(_lib._FP), nx))
+            out.append(a)
+        return out
+
+    def info(self):
+        b, a, w, ms = ctypes.c_size_t(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        _lib.check(_L().fv_batch_info(self._h, ctypes.byref(b), ctypes.byref(a), ctypes.byref(w), ctypes.byref(ms)))
+        tw, th, nt, gr = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _lib.check(_L().fv_batch_tile(self._h, ctypes.byref(tw), ctypes.byref(th), ctypes.byref(nt),
+                                      ctypes.byref(gr)))
+        return {"device_bytes": b.value, "active": a.value, "work_items": w.value, "last_run_ms": ms.value,
+                "tile_w": tw.value, "tile_h": th.value, "threads": nt.value, "grid": gr.value}
+
+    def run_to_completion(self, chunk=16):
+        """Advance until every simulation reached its t_end; returns the steps run."""
+        steps = 0
+        while True:
+            self.sync()
+            if all(self.status(s)["done"] for s in self.shapes):
+                return steps
+            self.run(chunk)
+            steps += chunk

@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../include/fvgpu.h"
 #include "fv_stage.cuh"
@@ -49,6 +50,9 @@ int fail(int code, const char* fmt, ...) {
         if (r_ != FV_OK) return r_; \
     } while (0)
 
+int scheme_nv(int scheme) { return scheme == FV_EE2D_KP07_DIMSPLIT ? 4 : 3; }
+int scheme_ghost(int scheme) { return (scheme == FV_LXF || scheme == FV_FORCE || scheme == FV_HLL) ? 1 : 2; }
+
 using KernelFn = void (*)(StageArgs);
 
 struct KEntry {
@@ -62,6 +66,7 @@ struct KEntry {
 const KEntry kTable[] = {
     {FV_KP07_DIMSPLIT, 124, 60, 256, true, fv::dimsplit_stage_kernel<fv::KP07_DIMSPLIT, 124, 60, 256>},
     {FV_KP07_DIMSPLIT, 124, 28, 128, true, fv::dimsplit_stage_kernel<fv::KP07_DIMSPLIT, 124, 28, 128>},
+    {FV_KP07_DIMSPLIT, 60, 28, 128, true, fv::dimsplit_stage_kernel<fv::KP07_DIMSPLIT, 60, 28, 128>},
     {FV_HLL2, 124, 60, 256, true, fv::dimsplit_stage_kernel<fv::HLL2, 124, 60, 256>},
     {FV_HLL2, 124, 28, 128, true, fv::dimsplit_stage_kernel<fv::HLL2, 124, 28, 128>},
     {FV_WAF, 124, 60, 256, true, fv::dimsplit_stage_kernel<fv::WAF, 124, 60, 256>},
@@ -70,8 +75,10 @@ const KEntry kTable[] = {
     {FV_FORCE, 124, 28, 128, true, fv::dimsplit_stage_kernel<fv::FORCE, 124, 28, 128>},
     {FV_HLL, 124, 60, 256, true, fv::dimsplit_stage_kernel<fv::HLL, 124, 60, 256>},
     {FV_HLL, 124, 28, 128, true, fv::dimsplit_stage_kernel<fv::HLL, 124, 28, 128>},
+    {FV_HLL, 60, 28, 128, true, fv::dimsplit_stage_kernel<fv::HLL, 60, 28, 128>},
     {FV_EE2D_KP07_DIMSPLIT, 124, 28, 128, true, fv::dimsplit_stage_kernel<fv::EE2D, 124, 28, 128>},
     {FV_EE2D_KP07_DIMSPLIT, 124, 60, 256, true, fv::dimsplit_stage_kernel<fv::EE2D, 124, 60, 256>},
+    {FV_EE2D_KP07_DIMSPLIT, 60, 28, 128, true, fv::dimsplit_stage_kernel<fv::EE2D, 60, 28, 128>},
     {FV_LXF, 124, 28, 256, false, fv::unsplit_stage_kernel<fv::LXF, 124, 28, 256>},
     {FV_LXF, 124, 12, 256, false, fv::unsplit_stage_kernel<fv::LXF, 124, 12, 256>},
     {FV_KP07, 124, 28, 256, false, fv::unsplit_stage_kernel<fv::KP07, 124, 28, 256>},
@@ -79,8 +86,43 @@ const KEntry kTable[] = {
 };
 constexpr int kNumEntries = sizeof(kTable) / sizeof(kTable[0]);
 
-int scheme_nv(int scheme) { return scheme == FV_EE2D_KP07_DIMSPLIT ? 4 : 3; }
-int scheme_ghost(int scheme) { return (scheme == FV_LXF || scheme == FV_FORCE || scheme == FV_HLL) ? 1 : 2; }
+using BatchFn = void (*)(fv::BatchArgs);
+struct BEntry {
+    int scheme;
+    int W, H, NT;
+    BatchFn fn;
+};
+// Batched (persistent) kernels; the first entry of a scheme is its default.
+const BEntry kBatchTable[] = {
+    {FV_KP07_DIMSPLIT, 60, 28, 128, fv::batched_stage_kernel<fv::KP07_DIMSPLIT, 60, 28, 128>},
+    {FV_KP07_DIMSPLIT, 124, 28, 128, fv::batched_stage_kernel<fv::KP07_DIMSPLIT, 124, 28, 128>},
+    {FV_KP07_DIMSPLIT, 124, 60, 256, fv::batched_stage_kernel<fv::KP07_DIMSPLIT, 124, 60, 256>},
+    {FV_HLL, 60, 28, 128, fv::batched_stage_kernel<fv::HLL, 60, 28, 128>},
+    {FV_HLL, 124, 28, 128, fv::batched_stage_kernel<fv::HLL, 124, 28, 128>},
+    {FV_HLL, 124, 60, 256, fv::batched_stage_kernel<fv::HLL, 124, 60, 256>},
+    {FV_EE2D_KP07_DIMSPLIT, 60, 28, 128, fv::batched_stage_kernel<fv::EE2D, 60, 28, 128>},
+    {FV_EE2D_KP07_DIMSPLIT, 124, 28, 128, fv::batched_stage_kernel<fv::EE2D, 124, 28, 128>},
+    {FV_HLL2, 60, 28, 128, fv::batched_stage_kernel<fv::HLL2, 60, 28, 128>},
+    {FV_HLL2, 124, 28, 128, fv::batched_stage_kernel<fv::HLL2, 124, 28, 128>},
+    {FV_WAF, 60, 28, 128, fv::batched_stage_kernel<fv::WAF, 60, 28, 128>},
+    {FV_WAF, 124, 28, 128, fv::batched_stage_kernel<fv::WAF, 124, 28, 128>},
+    {FV_FORCE, 60, 28, 128, fv::batched_stage_kernel<fv::FORCE, 60, 28, 128>},
+    {FV_FORCE, 124, 28, 128, fv::batched_stage_kernel<fv::FORCE, 124, 28, 128>},
+};
+constexpr int kNumBatchEntries = sizeof(kBatchTable) / sizeof(kBatchTable[0]);
+
+size_t batch_smem(const BEntry& e) { return scheme_nv(e.scheme) * (size_t)(e.W + 8) * (e.H + 4) * sizeof(float); }
+
+const BEntry* find_batch_entry(int scheme, int cfg) {
+    int k = 0;
+    for (int i = 0; i < kNumBatchEntries; ++i) {
+        if (kBatchTable[i].scheme != scheme) continue;
+        if (k == cfg) return &kBatchTable[i];
+        ++k;
+    }
+    return nullptr;
+}
+
 
 size_t entry_smem(const KEntry& e) {
     const size_t tile = (size_t)(e.W + 8) * (e.H + 4) * sizeof(float);
@@ -630,6 +672,400 @@ int fv_host_alloc(void** ptr, size_t bytes) {
 
 int fv_host_free(void* ptr) {
     FV_CK(cudaFreeHost(ptr));
+    return FV_OK;
+}
+
+}  // extern "C"
+
+// ====================================================================== batches
+//
+// A batch advances many simulations of one split scheme together: the
+// persistent kernel walks a device-resident work list of (simulation, tile)
+// pairs, every simulation keeps its own control block (t, dt, t_end, buffer
+// parity), and graphs of 1 and 16 steps are captured once.  Adding or
+// removing a simulation rewrites the work list between graph replays.
+
+struct fv_batch {
+    fv_context* ctx = nullptr;
+    int scheme = 0, nv = 3, gc = 2, num_substeps = 2;
+    fv_params p{};
+    float dt_scale = 0.5f, factor = 0.5f;
+    const BEntry* be = nullptr;
+    int max_inst = 0;
+    cudaStream_t stream = nullptr;
+    fv::BatchInstance* d_inst = nullptr;  // device, max_inst entries
+    fv::BatchInstance* h_inst = nullptr;  // pinned staging
+    SimCtl* d_ctl = nullptr;              // device, one control block per slot
+    SimCtl* h_ctl = nullptr;              // pinned host view
+    int2* d_work = nullptr;
+    int2* h_work = nullptr;
+    int work_cap = 0;
+    int* d_nwork = nullptr;
+    int* h_nwork = nullptr;
+    int* d_err = nullptr;
+    std::vector<int> used;               // slot in use
+    std::vector<void*> slot_mem;          // per-slot device allocation (planes + tile scratch)
+    std::vector<size_t> slot_bytes;
+    size_t bytes = 0;
+    int grid = 0;
+    cudaGraphExec_t graph1 = nullptr, graph16 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0.0;
+};
+
+namespace {
+
+void batch_drop_graphs(fv_batch* b) {
+    if (b->graph1) cudaGraphExecDestroy(b->graph1);
+    if (b->graph16) cudaGraphExecDestroy(b->graph16);
+    b->graph1 = b->graph16 = nullptr;
+}
+
+int batch_launch_step(fv_batch* b) {
+    for (int i = 0; i < b->num_substeps; ++i) {
+        fv::BatchArgs a;
+        a.inst = b->d_inst;
+        a.work = b->d_work;
+        a.nwork = b->d_nwork;
+        a.substep = i;
+        a.is_last = (i == b->num_substeps - 1) ? 1 : 0;
+        a.want_sums = 0;
+        a.err = b->d_err;
+        void* kargs[] = {&a};
+        FV_CK(cudaLaunchKernel(reinterpret_cast<const void*>(b->be->fn), dim3(b->grid), dim3(b->be->NT), kargs,
+                               batch_smem(*b->be), b->stream));
+    }
+    return FV_OK;
+}
+
+int batch_build_graph(fv_batch* b, int nsteps, cudaGraphExec_t* out) {
+    cudaGraph_t g = nullptr;
+    FV_CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = FV_OK;
+    for (int k = 0; k < nsteps && rc == FV_OK; ++k) rc = batch_launch_step(b);
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (rc != FV_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(FV_ERR_CUDA, "batch graph capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(FV_ERR_CUDA, "batch graph instantiate: %s", cudaGetErrorString(e));
+    return FV_OK;
+}
+
+// Rebuilds the work list from the slots in use and queues its upload.  The
+// caller has synchronised the stream (the pinned staging buffers are free).
+int batch_publish(fv_batch* b) {
+    int n = 0;
+    for (int s = 0; s < b->max_inst; ++s)
+        if (b->used[s]) n += b->h_inst[s].ntiles;
+    if (n > b->work_cap) {
+        int cap = b->work_cap;
+        while (cap < n) cap *= 2;
+        if (b->d_work) cudaFreeAsync(b->d_work, b->stream);
+        if (b->h_work) cudaFreeHost(b->h_work);
+        b->d_work = nullptr;
+        b->h_work = nullptr;
+        FV_CK(cudaMallocAsync(reinterpret_cast<void**>(&b->d_work), (size_t)cap * sizeof(int2), b->stream));
+        FV_CK(cudaMallocHost(reinterpret_cast<void**>(&b->h_work), (size_t)cap * sizeof(int2)));
+        b->work_cap = cap;
+        batch_drop_graphs(b);  // the graphs captured the old work-list pointer
+    }
+    int k = 0;
+    for (int s = 0; s < b->max_inst; ++s) {
+        if (!b->used[s]) continue;
+        for (int t = 0; t < b->h_inst[s].ntiles; ++t) b->h_work[k++] = make_int2(s, t);
+    }
+    *b->h_nwork = n;
+    if (n > 0) FV_CK(cudaMemcpyAsync(b->d_work, b->h_work, (size_t)n * sizeof(int2), cudaMemcpyHostToDevice, b->stream));
+    FV_CK(cudaMemcpyAsync(b->d_nwork, b->h_nwork, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    FV_CK(cudaStreamSynchronize(b->stream));
+    return FV_OK;
+}
+
+int check_batch(fv_batch* b) {
+    if (!b) return fail(FV_ERR_INVALID, "null batch");
+    FV_CK(cudaSetDevice(b->ctx->device));
+    return FV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fv_batch_create(fv_context* ctx, int scheme, const fv_params* params, int max_instances, fv_batch** out) {
+    if (!ctx || !params || !out) return fail(FV_ERR_INVALID, "null argument");
+    if (max_instances < 1 || max_instances > (1 << 20)) return fail(FV_ERR_INVALID, "bad max_instances");
+    const int cfg = params->tile < 0 ? 0 : params->tile;
+    const BEntry* be = find_batch_entry(scheme, cfg);
+    if (!be) return fail(FV_ERR_INVALID, "no batched kernel for scheme %d (tile %d)", scheme, cfg);
+    FV_CK(cudaSetDevice(ctx->device));
+    FV_CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(be->fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)batch_smem(*be)));
+    int per_sm = 0;
+    FV_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reinterpret_cast<const void*>(be->fn), be->NT,
+                                                        batch_smem(*be)));
+    if (per_sm < 1) return fail(FV_ERR_CUDA, "batched kernel does not fit on an SM");
+    fv_batch* b = new fv_batch;
+    b->ctx = ctx;
+    b->scheme = scheme;
+    b->nv = scheme_nv(scheme);
+    b->gc = scheme_ghost(scheme);
+    b->num_substeps = (scheme == FV_FORCE || scheme == FV_HLL) ? 1 : 2;
+    b->dt_scale = (b->num_substeps == 2) ? 0.5f : 1.0f;
+    b->factor = (scheme == FV_FORCE) ? 1.0f : 0.5f;
+    b->p = *params;
+    b->be = be;
+    b->max_inst = max_instances;
+    b->grid = per_sm * ctx->sm_count;
+    b->used.assign(max_instances, 0);
+    b->slot_mem.assign(max_instances, nullptr);
+    b->slot_bytes.assign(max_instances, 0);
+    auto bail = [&](int rc) {
+        fv_batch_destroy(b);
+        return rc;
+    };
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess)
+        return bail(fail(FV_ERR_CUDA, "stream/event creation failed"));
+    b->work_cap = 4096;
+    if (cudaMalloc(&b->d_inst, (size_t)max_instances * sizeof(fv::BatchInstance)) != cudaSuccess ||
+        cudaMallocHost(&b->h_inst, (size_t)max_instances * sizeof(fv::BatchInstance)) != cudaSuccess ||
+        cudaMalloc(&b->d_ctl, (size_t)max_instances * sizeof(SimCtl)) != cudaSuccess ||
+        cudaMallocHost(&b->h_ctl, (size_t)max_instances * sizeof(SimCtl)) != cudaSuccess ||
+        cudaMalloc(&b->d_work, (size_t)b->work_cap * sizeof(int2)) != cudaSuccess ||
+        cudaMallocHost(&b->h_work, (size_t)b->work_cap * sizeof(int2)) != cudaSuccess ||
+        cudaMalloc(&b->d_nwork, sizeof(int)) != cudaSuccess || cudaMallocHost(&b->h_nwork, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&b->d_err, sizeof(int)) != cudaSuccess)
+        return bail(fail(FV_ERR_NOMEM, "out of memory creating the batch"));
+    memset(b->h_inst, 0, (size_t)max_instances * sizeof(fv::BatchInstance));
+    memset(b->h_ctl, 0, (size_t)max_instances * sizeof(SimCtl));
+    *b->h_nwork = 0;
+    if (cudaMemsetAsync(b->d_ctl, 0, (size_t)max_instances * sizeof(SimCtl), b->stream) != cudaSuccess ||
+        cudaMemsetAsync(b->d_err, 0, sizeof(int), b->stream) != cudaSuccess ||
+        cudaMemsetAsync(b->d_nwork, 0, sizeof(int), b->stream) != cudaSuccess ||
+        cudaStreamSynchronize(b->stream) != cudaSuccess)
+        return bail(fail(FV_ERR_CUDA, "batch initialisation failed"));
+    b->bytes = (size_t)max_instances * (sizeof(fv::BatchInstance) + sizeof(SimCtl)) + b->work_cap * sizeof(int2);
+    *out = b;
+    return FV_OK;
+}
+
+int fv_batch_destroy(fv_batch* b) {
+    if (!b) return FV_OK;
+    cudaSetDevice(b->ctx->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_drop_graphs(b);
+    for (size_t s = 0; s < b->slot_mem.size(); ++s)
+        if (b->slot_mem[s]) cudaFreeAsync(b->slot_mem[s], b->stream);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->d_inst) cudaFree(b->d_inst);
+    if (b->h_inst) cudaFreeHost(b->h_inst);
+    if (b->d_ctl) cudaFree(b->d_ctl);
+    if (b->h_ctl) cudaFreeHost(b->h_ctl);
+    if (b->d_work) cudaFree(b->d_work);
+    if (b->h_work) cudaFreeHost(b->h_work);
+    if (b->d_nwork) cudaFree(b->d_nwork);
+    if (b->h_nwork) cudaFreeHost(b->h_nwork);
+    if (b->d_err) cudaFree(b->d_err);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return FV_OK;
+}
+
+int fv_batch_add(fv_batch* b, int nx, int ny, float dx, float dy, int bc, const float* const* host_vars,
+                 int host_rows, int host_cols, double t_end, int* slot) {
+    FV_TRY(check_batch(b));
+    if (!host_vars || !slot) return fail(FV_ERR_INVALID, "null argument");
+    if (nx < 1 || ny < 1 || nx > (1 << 16) || ny > (1 << 16)) return fail(FV_ERR_INVALID, "bad grid %d x %d", nx, ny);
+    for (int side = 0; side < 4; ++side)
+        if (((bc >> (8 * side)) & 0xF) == fv::BC_NEUMANN)
+            return fail(FV_ERR_UNSUPPORTED, "Neumann boundary condition not supported");
+    const int gc = b->gc;
+    const bool halo = (host_rows == ny + 2 * gc && host_cols == nx + 2 * gc);
+    if (!halo && !(host_rows == ny && host_cols == nx)) return fail(FV_ERR_INVALID, "Wrong shape of data");
+    for (int v = 0; v < b->nv; ++v)
+        if (!host_vars[v]) return fail(FV_ERR_INVALID, "variable %d is null", v);
+    int s = -1;
+    for (int i = 0; i < b->max_inst; ++i)
+        if (!b->used[i]) {
+            s = i;
+            break;
+        }
+    if (s < 0) return fail(FV_ERR_NOMEM, "batch is full (%d simulations)", b->max_inst);
+    FV_CK(cudaStreamSynchronize(b->stream));  // staging buffers are free once the stream is idle
+
+    const int W = b->be->W, H = b->be->H;
+    const int pitch = ((nx + 8) + 31) / 32 * 32;
+    const int tiles_x = (nx + W - 1) / W, tiles_y = (ny + H - 1) / H, ntiles = tiles_x * tiles_y;
+    const size_t plane = (size_t)(ny + 4) * pitch * sizeof(float);
+    const size_t scratch = (size_t)ntiles * (sizeof(float) + 4 * sizeof(double));
+    const size_t total = 2 * b->nv * plane + scratch + 256;
+    void* mem = nullptr;
+    if (cudaMallocAsync(&mem, total, b->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(FV_ERR_NOMEM, "out of device memory for a %d x %d simulation", nx, ny);
+    }
+    FV_CK(cudaMemsetAsync(mem, 0, total, b->stream));
+    fv::BatchInstance& I = b->h_inst[s];
+    memset(&I, 0, sizeof(I));
+    char* base = static_cast<char*>(mem);
+    for (int k = 0; k < 2; ++k)
+        for (int v = 0; v < b->nv; ++v) I.buf[k][v] = reinterpret_cast<float*>(base + (size_t)(k * b->nv + v) * plane);
+    I.block_cfl = reinterpret_cast<float*>(base + 2 * b->nv * plane);
+    I.block_sums = reinterpret_cast<double*>(base + 2 * b->nv * plane + ((ntiles * sizeof(float) + 255) / 256 * 256));
+    I.ctl = b->d_ctl + s;
+    I.nx = nx;
+    I.ny = ny;
+    I.pitch = pitch;
+    I.bc = bc;
+    I.tiles_x = tiles_x;
+    I.ntiles = ntiles;
+    I.dx = dx;
+    I.dy = dy;
+    I.g = b->p.g;
+    I.gamma = b->p.gamma;
+    I.theta = b->p.theta;
+    I.dt_scale = b->dt_scale;
+    auto enc = encode_fn();
+    for (int k = 0; k < 2; ++k)
+        for (int v = 0; v < b->nv; ++v) {
+            cuuint64_t dims[2] = {(cuuint64_t)(nx + 8), (cuuint64_t)(ny + 4)};
+            cuuint64_t strides[1] = {(cuuint64_t)pitch * sizeof(float)};
+            cuuint32_t box[2] = {(cuuint32_t)(W + 8), (cuuint32_t)(H + 4)};
+            cuuint32_t estr[2] = {1, 1};
+            CUresult r = enc(&I.tmap[k][v], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, I.buf[k][v], dims, strides, box, estr,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) {
+                cudaFreeAsync(mem, b->stream);
+                return fail(FV_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+            }
+        }
+    const int off = halo ? gc : 0;
+    for (int v = 0; v < b->nv; ++v)
+        FV_CK(cudaMemcpy2DAsync(I.buf[0][v] + fv::cell_index(-off, -off, pitch), pitch * sizeof(float), host_vars[v],
+                                host_cols * sizeof(float), host_cols * sizeof(float), host_rows, cudaMemcpyHostToDevice,
+                                b->stream));
+    SimCtl& c = b->h_ctl[s];
+    memset(&c, 0, sizeof(c));
+    const float c2 = (b->scheme == FV_EE2D_KP07_DIMSPLIT) ? b->p.gamma : b->p.g;
+    const float cfl0 = initial_cfl(host_vars, (size_t)host_rows * host_cols, dx, dy, c2);
+    c.t_end = t_end;
+    c.cfl_min = cfl0;
+    c.factor = b->factor;
+    c.cfl_scale = b->p.cfl_scale;
+    c.update_dt = 1;
+    c.dt = (cfl0 * c.factor) * c.cfl_scale;  // simulate() computes dt at step 0
+    FV_CK(cudaMemcpyAsync(b->d_ctl + s, &c, sizeof(SimCtl), cudaMemcpyHostToDevice, b->stream));
+    FV_CK(cudaMemcpyAsync(b->d_inst + s, &I, sizeof(fv::BatchInstance), cudaMemcpyHostToDevice, b->stream));
+    b->used[s] = 1;
+    b->slot_mem[s] = mem;
+    b->slot_bytes[s] = total;
+    b->bytes += total;
+    FV_TRY(batch_publish(b));
+    *slot = s;
+    return FV_OK;
+}
+
+int fv_batch_remove(fv_batch* b, int slot) {
+    FV_TRY(check_batch(b));
+    if (slot < 0 || slot >= b->max_inst || !b->used[slot]) return fail(FV_ERR_INVALID, "slot %d is not in use", slot);
+    FV_CK(cudaStreamSynchronize(b->stream));
+    b->used[slot] = 0;
+    FV_TRY(batch_publish(b));
+    FV_CK(cudaFreeAsync(b->slot_mem[slot], b->stream));
+    b->slot_mem[slot] = nullptr;
+    b->bytes -= b->slot_bytes[slot];
+    b->slot_bytes[slot] = 0;
+    return FV_OK;
+}
+
+int fv_batch_run(fv_batch* b, int n_steps) {
+    FV_TRY(check_batch(b));
+    if (n_steps < 0) return fail(FV_ERR_INVALID, "negative step count");
+    if (!b->graph1) FV_TRY(batch_build_graph(b, 1, &b->graph1));
+    if (!b->graph16) FV_TRY(batch_build_graph(b, 16, &b->graph16));
+    FV_CK(cudaEventRecord(b->ev0, b->stream));
+    int k = n_steps;
+    while (k >= 16) {
+        FV_CK(cudaGraphLaunch(b->graph16, b->stream));
+        k -= 16;
+    }
+    while (k > 0) {
+        FV_CK(cudaGraphLaunch(b->graph1, b->stream));
+        --k;
+    }
+    FV_CK(cudaEventRecord(b->ev1, b->stream));
+    return FV_OK;
+}
+
+int fv_batch_sync(fv_batch* b) {
+    FV_TRY(check_batch(b));
+    FV_CK(cudaMemcpyAsync(b->h_ctl, b->d_ctl, (size_t)b->max_inst * sizeof(SimCtl), cudaMemcpyDeviceToHost,
+                          b->stream));
+    int err = 0;
+    FV_CK(cudaMemcpyAsync(b->h_nwork, b->d_nwork, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+    FV_CK(cudaStreamSynchronize(b->stream));
+    FV_CK(cudaMemcpy(&err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, b->ev0, b->ev1) == cudaSuccess) b->last_ms = ms;
+    cudaGetLastError();
+    if (err) return fail(FV_ERR_DEVICE, "a batched stage kernel gave up waiting for a tile load");
+    return FV_OK;
+}
+
+int fv_batch_status(fv_batch* b, int slot, double* t, long long* nt, float* dt, int* done) {
+    if (!b || slot < 0 || slot >= b->max_inst || !b->used[slot]) return fail(FV_ERR_INVALID, "slot not in use");
+    const SimCtl& c = b->h_ctl[slot];
+    if (t) *t = c.t;
+    if (nt) *nt = c.nt;
+    if (dt) *dt = c.dt;
+    if (done) {
+        const double rem = c.t_end - c.t;
+        const float cur = (float)((rem < (double)c.dt) ? rem : (double)c.dt);
+        *done = (!(c.t < c.t_end) || cur <= 0.0f) ? 1 : 0;
+    }
+    return FV_OK;
+}
+
+int fv_batch_download(fv_batch* b, int slot, int var, float* host, int host_pitch) {
+    FV_TRY(check_batch(b));
+    if (slot < 0 || slot >= b->max_inst || !b->used[slot] || var < 0 || var >= b->nv || !host)
+        return fail(FV_ERR_INVALID, "bad download argument");
+    const fv::BatchInstance& I = b->h_inst[slot];
+    if (host_pitch < I.nx) return fail(FV_ERR_INVALID, "host pitch too small");
+    const int cur = b->h_ctl[slot].cur;
+    FV_CK(cudaMemcpy2DAsync(host, (size_t)host_pitch * sizeof(float), I.buf[cur][var] + fv::cell_index(0, 0, I.pitch),
+                            (size_t)I.pitch * sizeof(float), (size_t)I.nx * sizeof(float), I.ny, cudaMemcpyDeviceToHost,
+                            b->stream));
+    FV_CK(cudaStreamSynchronize(b->stream));
+    return FV_OK;
+}
+
+int fv_batch_info(fv_batch* b, size_t* device_bytes, int* active, int* work_items, double* last_run_ms) {
+    if (!b) return fail(FV_ERR_INVALID, "null batch");
+    if (device_bytes) *device_bytes = b->bytes;
+    if (active) {
+        int n = 0;
+        for (int s = 0; s < b->max_inst; ++s) n += b->used[s];
+        *active = n;
+    }
+    if (work_items) *work_items = *b->h_nwork;
+    if (last_run_ms) *last_run_ms = b->last_ms;
+    return FV_OK;
+}
+
+int fv_batch_tile(fv_batch* b, int* tile_w, int* tile_h, int* threads, int* grid) {
+    if (!b) return fail(FV_ERR_INVALID, "null batch");
+    if (tile_w) *tile_w = b->be->W;
+    if (tile_h) *tile_h = b->be->H;
+    if (threads) *threads = b->be->NT;
+    if (grid) *grid = b->grid;
     return FV_OK;
 }
 

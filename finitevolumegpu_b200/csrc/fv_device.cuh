@@ -6,8 +6,12 @@
 // rearranged so that values shared by neighbouring faces are computed once per
 // cell: a MUSCL-Hancock cell produces both of its predicted face states from one
 // flux difference, and each face state carries its flux, velocity and wave speed.
-// Arithmetic is FP32 and the library is compiled with --use_fast_math, the
-// options the reference compiles its kernels with (GPUSimulators/KP07_dimsplit.py:87).
+// Arithmetic is FP32 with fast-math division and square root and flush to
+// zero, as the reference compiles its kernels (--use_fast_math,
+// GPUSimulators/KP07_dimsplit.py:87).  The library is built with -fmad=false
+// and every fused multiply-add is written out with fmaf, so the rounding of
+// each formula does not depend on how the compiler inlines it: a cell's result
+// is the same whichever tile shape, kernel or batch computes it.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -67,6 +71,13 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, 
             "r"(smem_u32(dst)),
         "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(smem_u32(bar))
         : "memory");
+}
+
+// Orders a tensor map written to global memory by earlier (host-issued) copies
+// before its use by this thread's TMA operations.
+__device__ __forceinline__ void fence_tmap_acquire(const void* tmap) {
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(tmap))
+                 : "memory");
 }
 
 __device__ __forceinline__ void prefetch_tmap(const void* tmap) {
@@ -131,7 +142,7 @@ __device__ __forceinline__ void swe_central_upwind(const SweFace& m, const SweFa
     const float inv = 1.0f / (ap - am);
     const float apam = ap * am;
 #pragma unroll
-    for (int v = 0; v < 3; ++v) out[v] = (fmaf(ap, m.f[v], -am * p.f[v]) + apam * (p.q[v] - m.q[v])) * inv;
+    for (int v = 0; v < 3; ++v) out[v] = fmaf(apam, p.q[v] - m.q[v], fmaf(ap, m.f[v], -am * p.f[v])) * inv;
 }
 
 // HLL flux (GPUSimulators/cuda/SWECommon.h:274-313).
@@ -141,8 +152,8 @@ __device__ __forceinline__ void swe_hll(const SweFace& l, const SweFace& r, floa
     const float h_dag = 0.5f * hsum - 0.25f * (r.u - l.u) * hsum / (l.c + r.c);
     const float q_l = (h_dag > h_l) ? sqrtf(0.5f * ((h_dag + h_l) * h_dag / (h_l * h_l))) : 1.0f;
     const float q_r = (h_dag > h_r) ? sqrtf(0.5f * ((h_dag + h_r) * h_dag / (h_r * h_r))) : 1.0f;
-    const float S_l = l.u - l.c * q_l;
-    const float S_r = r.u + r.c * q_r;
+    const float S_l = fmaf(-l.c, q_l, l.u);
+    const float S_r = fmaf(r.c, q_r, r.u);
     if (S_l >= 0.0f) {
 #pragma unroll
         for (int v = 0; v < 3; ++v) out[v] = l.f[v];
@@ -153,7 +164,7 @@ __device__ __forceinline__ void swe_hll(const SweFace& l, const SweFace& r, floa
         const float inv = 1.0f / (S_r - S_l);
         const float srsl = S_r * S_l;
 #pragma unroll
-        for (int v = 0; v < 3; ++v) out[v] = (fmaf(S_r, l.f[v], -S_l * r.f[v]) + srsl * (r.q[v] - l.q[v])) * inv;
+        for (int v = 0; v < 3; ++v) out[v] = fmaf(srsl, r.q[v] - l.q[v], fmaf(S_r, l.f[v], -S_l * r.f[v])) * inv;
     }
 }
 
@@ -177,7 +188,7 @@ __device__ __forceinline__ void swe_muscl_hancock(const float qm[3], const float
     float D[3];
     D[0] = W[1] - E[1];
     D[1] = fmaf(W[1], uw, half_g * W[0] * W[0]) - fmaf(E[1], ue, half_g * E[0] * E[0]);
-    D[2] = W[2] * uw - E[2] * ue;
+    D[2] = fmaf(W[2], uw, -E[2] * ue);
     w = swe_face(fmaf(k2, D[0], W[0]), fmaf(k2, D[1], W[1]), fmaf(k2, D[2], W[2]), g, half_g);
     e = swe_face(fmaf(k2, D[0], E[0]), fmaf(k2, D[1], E[1]), fmaf(k2, D[2], E[2]), g, half_g);
 }
@@ -199,7 +210,7 @@ __device__ __forceinline__ EulerFace euler_face(float rho, float ru, float rv, f
     s.q[2] = rv;
     s.q[3] = E;
     const float rr = 1.0f / rho;
-    const float P = (gamma - 1.0f) * (E - 0.5f * (ru * ru + rv * rv) * rr);
+    const float P = (gamma - 1.0f) * fmaf(-0.5f * fmaf(ru, ru, rv * rv), rr, E);
     s.u = ru * rr;
     s.f[0] = ru;
     s.f[1] = fmaf(ru, s.u, P);
@@ -216,7 +227,7 @@ __device__ __forceinline__ void euler_central_upwind(const EulerFace& m, const E
     const float inv = 1.0f / (ap - am);
     const float apam = ap * am;
 #pragma unroll
-    for (int v = 0; v < 4; ++v) out[v] = (fmaf(ap, m.f[v], -am * p.f[v]) + apam * (p.q[v] - m.q[v])) * inv;
+    for (int v = 0; v < 4; ++v) out[v] = fmaf(apam, p.q[v] - m.q[v], fmaf(ap, m.f[v], -am * p.f[v])) * inv;
 }
 
 // GPUSimulators/cuda/EulerCommon.h:117-160
@@ -226,8 +237,8 @@ __device__ __forceinline__ void euler_hll(const EulerFace& l, const EulerFace& r
     const float h_dag = 0.5f * hsum - 0.25f * (r.u - l.u) * hsum / (l.c + r.c);
     const float q_l = (h_dag > h_l) ? sqrtf(0.5f * ((h_dag + h_l) * h_dag / (h_l * h_l))) : 1.0f;
     const float q_r = (h_dag > h_r) ? sqrtf(0.5f * ((h_dag + h_r) * h_dag / (h_r * h_r))) : 1.0f;
-    const float S_l = l.u - l.c * q_l;
-    const float S_r = r.u + r.c * q_r;
+    const float S_l = fmaf(-l.c, q_l, l.u);
+    const float S_r = fmaf(r.c, q_r, r.u);
     if (S_l >= 0.0f) {
 #pragma unroll
         for (int v = 0; v < 4; ++v) out[v] = l.f[v];
@@ -238,7 +249,7 @@ __device__ __forceinline__ void euler_hll(const EulerFace& l, const EulerFace& r
         const float inv = 1.0f / (S_r - S_l);
         const float srsl = S_r * S_l;
 #pragma unroll
-        for (int v = 0; v < 4; ++v) out[v] = (fmaf(S_r, l.f[v], -S_l * r.f[v]) + srsl * (r.q[v] - l.q[v])) * inv;
+        for (int v = 0; v < 4; ++v) out[v] = fmaf(srsl, r.q[v] - l.q[v], fmaf(S_r, l.f[v], -S_l * r.f[v])) * inv;
     }
 }
 
@@ -261,8 +272,8 @@ __device__ __forceinline__ void euler_muscl_hancock(const float qm[4], const flo
     float D[4];
     D[0] = W[1] - E[1];
     D[1] = fmaf(W[1], uw, gamma) - fmaf(E[1], ue, gamma);
-    D[2] = W[2] * uw - E[2] * ue;
-    D[3] = uw * (W[3] + gamma) - ue * (E[3] + gamma);
+    D[2] = fmaf(W[2], uw, -E[2] * ue);
+    D[3] = fmaf(uw, W[3] + gamma, -ue * (E[3] + gamma));
     w = euler_face(fmaf(k2, D[0], W[0]), fmaf(k2, D[1], W[1]), fmaf(k2, D[2], W[2]), fmaf(k2, D[3], W[3]), gamma);
     e = euler_face(fmaf(k2, D[0], E[0]), fmaf(k2, D[1], E[1]), fmaf(k2, D[2], E[2]), fmaf(k2, D[3], E[3]), gamma);
 }
@@ -306,8 +317,8 @@ __device__ __forceinline__ void waf_flux(const WafCell& l2, const WafCell& l1, c
     const float h_l = l1.q[0], h_r = r1.q[0];
     const float q_l = (hd > h_l) ? sqrtf(0.5f * ((hd + h_l) * hd)) / h_l : 1.0f;
     const float q_r = (hd > h_r) ? sqrtf(0.5f * ((hd + h_r) * hd)) / h_r : 1.0f;
-    const float S_l = l1.u - l1.c * q_l;
-    const float S_r = r1.u + r1.c * q_r;
+    const float S_l = fmaf(-l1.c, q_l, l1.u);
+    const float S_r = fmaf(r1.c, q_r, r1.u);
     const float a_r = h_r * (r1.u - S_r);
     const float a_l = h_l * (l1.u - S_l);
     const float S_star = (S_l * a_r - S_r * a_l) / (a_r - a_l);
@@ -331,7 +342,8 @@ __device__ __forceinline__ void waf_flux(const WafCell& l2, const WafCell& l1, c
         const float F1 = l1.f[v], F4 = r1.f[v];
         const float F2 = fmaf(S_l, Qsl[v] - l1.q[v], F1);
         const float F3 = fmaf(S_r, Qsr[v] - r1.q[v], F4);
-        out[v] = 0.5f * (F1 + F4) - 0.5f * (A_1 * (F2 - F1) + A_2 * (F3 - F2) + A_3 * (F4 - F3));
+        const float wsum = fmaf(A_3, F4 - F3, fmaf(A_2, F3 - F2, A_1 * (F2 - F1)));
+        out[v] = fmaf(-0.5f, wsum, 0.5f * (F1 + F4));
     }
 }
 
@@ -363,8 +375,8 @@ __device__ __forceinline__ void swe_lxf_2d(const SweFace& l, const SweFace& r, f
 __device__ __forceinline__ float cell_cfl(float h, float hu, float hv, float dx, float dy, float gg) {
     const float rh = 1.0f / h;
     const float c = sqrtf(gg * h);
-    const float max_u = dx / (fabsf(hu * rh) + c);
-    const float max_v = dy / (fabsf(hv * rh) + c);
+    const float max_u = dx / fmaf(fabsf(hu), fabsf(rh), c);
+    const float max_v = dy / fmaf(fabsf(hv), fabsf(rh), c);
     return fminf(max_u, max_v);
 }
 

@@ -93,14 +93,15 @@ struct StepCtl {
 // dt of the current step: float32(min(dt, t_end - t)) (GPUSimulators/Simulator.py:199),
 // with Python's min() tie and NaN behaviour; a step runs while t < t_end and
 // dt > 0 (Simulator.py:192, :202).
-__device__ __forceinline__ StepCtl read_step(const StageArgs& A) {
-    const volatile SimCtl* c = A.ctl;
+__device__ __forceinline__ StepCtl read_step(const SimCtl* ctl, bool explicit_dt, float dt_step, bool force_cfl,
+                                             bool is_last) {
+    const volatile SimCtl* c = ctl;
     StepCtl s;
     s.cur = c->cur;
     const double t = c->t;
     const double t_end = c->t_end;
-    if (A.explicit_dt) {
-        s.dt = A.dt_step;
+    if (explicit_dt) {
+        s.dt = dt_step;
         s.active = true;
     } else {
         const double rem = t_end - t;
@@ -111,8 +112,12 @@ __device__ __forceinline__ StepCtl read_step(const StageArgs& A) {
     s.t_new = t + (double)s.dt;
     const long long nt = c->nt;
     const bool sched = c->update_dt && ((nt + 1) % 100 == 0);
-    s.do_cfl = A.force_cfl || (A.is_last && !A.explicit_dt && (sched || !(s.t_new < t_end)));
+    s.do_cfl = force_cfl || (is_last && !explicit_dt && (sched || !(s.t_new < t_end)));
     return s;
+}
+
+__device__ __forceinline__ StepCtl read_step(const StageArgs& A) {
+    return read_step(A.ctl, A.explicit_dt != 0, A.dt_step, A.force_cfl != 0, A.is_last != 0);
 }
 
 template <int NT>
@@ -143,40 +148,40 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
     return r;
 }
 
-// CTA epilogue: per-CTA CFL minimum and FP64 sums, arrival count, and (last
-// CTA) the reduction over all CTAs in fixed order plus the control-block update
+// Tile epilogue: per-tile CFL minimum and FP64 sums, arrival count on the
+// simulation's control block, and (last tile of the simulation in this launch)
+// the reduction over all its tiles in fixed order plus the control-block update
 // of Simulator.step / simulate (GPUSimulators/Simulator.py:195-196, :227-228).
 template <int NT, int NV>
-__device__ void stage_epilogue(const StageArgs& A, const StepCtl& s, float my_cfl, const double (&my_sums)[NV],
-                               bool sums) {
+__device__ void tile_epilogue(SimCtl* ctl, float* block_cfl, double* block_sums, int tile, int ntiles, bool is_last,
+                              bool explicit_dt, const StepCtl& s, float my_cfl, const double (&my_sums)[NV],
+                              bool sums) {
     __shared__ float red_f[NT / 32];
     __shared__ double red_d[NT / 32];
     __shared__ int am_last;
-    const int nblocks = gridDim.x * gridDim.y;
-    const int bid = blockIdx.y * gridDim.x + blockIdx.x;
     if (s.do_cfl) {
         const float m = block_min<NT>(my_cfl, red_f);
-        if (threadIdx.x == 0) A.block_cfl[bid] = m;
+        if (threadIdx.x == 0) block_cfl[tile] = m;
     }
     if (sums) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             const double t = block_sum<NT>(my_sums[v], red_d);
-            if (threadIdx.x == 0) A.block_sums[(size_t)bid * 4 + v] = t;
+            if (threadIdx.x == 0) block_sums[(size_t)tile * 4 + v] = t;
         }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
-        const unsigned prev = atomicAdd(&A.ctl->arrive, 1u);
-        am_last = (prev == (unsigned)nblocks - 1u);
+        const unsigned prev = atomicAdd(&ctl->arrive, 1u);
+        am_last = (prev == (unsigned)ntiles - 1u);
     }
     __syncthreads();
     if (!am_last) return;
     __threadfence();
     float m = __int_as_float(0x7f800000);
     if (s.do_cfl) {
-        for (int i = threadIdx.x; i < nblocks; i += NT) m = fminf(m, __ldcg(&A.block_cfl[i]));
+        for (int i = threadIdx.x; i < ntiles; i += NT) m = fminf(m, __ldcg(&block_cfl[i]));
         m = block_min<NT>(m, red_f);
     }
     double tot[NV];
@@ -185,48 +190,77 @@ __device__ void stage_epilogue(const StageArgs& A, const StepCtl& s, float my_cf
         for (int v = 0; v < NV; ++v) {
             // fixed per-thread striding and tree: deterministic for a given grid
             double acc = 0.0;
-            for (int i = threadIdx.x; i < nblocks; i += NT) acc += __ldcg(&A.block_sums[(size_t)i * 4 + v]);
+            for (int i = threadIdx.x; i < ntiles; i += NT) acc += __ldcg(&block_sums[(size_t)i * 4 + v]);
             tot[v] = block_sum<NT>(acc, red_d);
         }
     }
     if (threadIdx.x == 0) {
-        SimCtl* c = A.ctl;
+        SimCtl* c = ctl;
         c->cur = s.cur ^ 1;
         if (s.do_cfl) c->cfl_min = m;
         if (sums) {
 #pragma unroll
             for (int v = 0; v < NV; ++v) c->sums[v] = tot[v];
         }
-        if (A.is_last) {
+        if (is_last) {
             c->t = s.t_new;
             c->nt = c->nt + 1;
-            if (!A.explicit_dt && c->update_dt && (c->nt % 100 == 0)) c->dt = (c->cfl_min * c->factor) * c->cfl_scale;
+            if (!explicit_dt && c->update_dt && (c->nt % 100 == 0)) c->dt = (c->cfl_min * c->factor) * c->cfl_scale;
         }
         c->arrive = 0u;
         __threadfence();
     }
+    __syncthreads();  // am_last and the reduction scratch are reused by the next tile of a persistent CTA
+}
+
+template <int NT, int NV>
+__device__ __forceinline__ void stage_epilogue(const StageArgs& A, const StepCtl& s, float my_cfl,
+                                               const double (&my_sums)[NV], bool sums) {
+    tile_epilogue<NT, NV>(A.ctl, A.block_cfl, A.block_sums, blockIdx.y * gridDim.x + blockIdx.x,
+                          gridDim.x * gridDim.y, A.is_last != 0, A.explicit_dt != 0, s, my_cfl, my_sums, sums);
 }
 
 // ------------------------------------------------------------------ tile load + ghost cells
 
+// One tile of one simulation: where its input comes from and where it goes.
+struct TileJob {
+    const CUtensorMap* tmap;  // NV tensor maps of the input planes (parameter or global memory)
+    float* const* in;         // NV input planes
+    float* const* out;        // NV output planes
+    int nx, ny, pitch, bc;
+    int x0, y0;               // first interior cell of the tile
+};
+
 // Issues the TMA loads of the tile (thread 0) and waits for them with a bounded
-// wait.  Returns false (uniformly across the CTA) if the wait gave up.
-template <int NV, int SP, int TR>
-__device__ __forceinline__ bool load_tile(float* Qs, const StageArgs& A, int cur, int x0, int y0, uint64_t* bar) {
+// wait on `phase` of the mbarrier (initialised here when `init`).  Returns false
+// (uniformly across the CTA) if the wait gave up; *err is then set.
+template <int NV, int SP, int TR, bool GLOBAL_TMAP = false>
+__device__ __forceinline__ bool load_tile(float* Qs, const CUtensorMap* tmap, int x0, int y0, uint64_t* bar,
+                                          uint32_t phase, bool init, int* err) {
     constexpr int PS = SP * TR;
     if (threadIdx.x == 0) {
-        mbar_init(bar, 1);
-        fence_barrier_init();
+        if (GLOBAL_TMAP) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) fence_tmap_acquire(tmap + v);
+        }
+        if (init) {
+            mbar_init(bar, 1);
+            fence_barrier_init();
+        }
+        // The CTA's generic-proxy reads and writes of the previous tile in this
+        // buffer (ordered before this point by the last barrier) must precede
+        // the async-proxy writes of the new load.
+        fence_proxy_async_shared();
         mbar_arrive_expect_tx(bar, NV * PS * (uint32_t)sizeof(float));
 #pragma unroll
-        for (int v = 0; v < NV; ++v) tma_load_2d(Qs + v * PS, &A.tmap[cur][v], x0, y0, bar);
+        for (int v = 0; v < NV; ++v) tma_load_2d(Qs + v * PS, tmap + v, x0, y0, bar);
     }
     __syncthreads();
-    const bool ok = mbar_wait_bounded(bar, 0, kWaitPolls);
+    const bool ok = mbar_wait_bounded(bar, phase, kWaitPolls);
     const int failed = __syncthreads_or(ok ? 0 : 1);
     if (failed) {
-        if (threadIdx.x == 0) atomicExch(&A.ctl->error, 1);
-        mbar_wait_bounded(bar, 0, kWaitPolls);  // let copies in flight land before the CTA exits
+        if (threadIdx.x == 0) atomicExch(err, 1);
+        mbar_wait_bounded(bar, phase, kWaitPolls);  // let copies in flight land before the CTA moves on
         return false;
     }
     return true;
@@ -241,9 +275,9 @@ __device__ __forceinline__ float sign_y(int v) { return v == 2 ? -1.0f : 1.0f; }
 // with the normal momentum negated, north, south, east, west in turn.
 // Dirichlet ghosts keep the stored values the TMA load brought in.
 template <int NV, int W, int H, int NT>
-__device__ void apply_boundary(float* Qs, const StageArgs& A, int cur, int x0, int y0) {
+__device__ void apply_boundary(float* Qs, const TileJob& J) {
     constexpr int SP = W + 8, TR = H + 4, PS = SP * TR;
-    const int nx = A.nx, ny = A.ny, bc = A.bc;
+    const int nx = J.nx, ny = J.ny, bc = J.bc, x0 = J.x0, y0 = J.y0;
     const bool pw = bc_west(bc) == BC_PERIODIC, pe = bc_east(bc) == BC_PERIODIC;
     const bool ps = bc_south(bc) == BC_PERIODIC, pn = bc_north(bc) == BC_PERIODIC;
     if (pw || pe || ps || pn) {
@@ -257,9 +291,9 @@ __device__ void apply_boundary(float* Qs, const StageArgs& A, int cur, int x0, i
             if (y < 0 && ps) ys = y + ny;
             else if (y >= ny && pn) ys = y - ny;
             if (xs == x && ys == y) continue;
-            const long long gi = cell_index(ys, xs, A.pitch);
+            const long long gi = cell_index(ys, xs, J.pitch);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) Qs[v * PS + i] = __ldg(A.buf[cur][v] + gi);
+            for (int v = 0; v < NV; ++v) Qs[v * PS + i] = __ldg(J.in[v] + gi);
         }
         __syncthreads();
     }
@@ -581,14 +615,110 @@ __device__ __forceinline__ void sweep_y(float* Qs, int s0, int s1, const SweepPa
 
 // ------------------------------------------------------------------ split-scheme stage kernel
 
-template <int SCHEME, int W, int H, int NT>
-__global__ void __launch_bounds__(NT) dimsplit_stage_kernel(const __grid_constant__ StageArgs A) {
+// Scheme constants of a split-scheme tile.
+struct SplitPar {
+    float dx, dy, g, gamma, theta;
+    float kdt;  // kernel dt of this substep
+    int substep;
+};
+
+// Load, ghost cells, both sweeps and copy-out of one tile of a split scheme
+// (FORCE, HLL, HLL2, WAF, KP07_dimsplit, EE2D).  Accumulates the tile's CFL
+// minimum and FP64 sums into the per-thread values.  Returns false if the tile
+// load gave up (nothing was written).
+template <int SCHEME, int W, int H, int NT, bool GLOBAL_TMAP = false>
+__device__ bool process_tile_dimsplit(float* Qs, uint64_t* bar, uint32_t phase, bool init_bar, const TileJob& J,
+                                      const SplitPar& P, bool do_cfl, bool sums, int* err, float& my_cfl,
+                                      double (&my_sums)[(SCHEME == EE2D) ? 4 : 3]) {
     constexpr int NV = (SCHEME == EE2D) ? 4 : 3;
     constexpr int G = (SCHEME == FORCE || SCHEME == HLL) ? 1 : 2;
     constexpr int SP = W + 8, TR = H + 4, PS = SP * TR;
     static_assert(W % 4 == 0 && (W / 4) % 2 == 1, "row segments must be odd for conflict-free x sweeps");
     static_assert(TR * 4 <= NT, "one x-sweep segment per thread");
     static_assert(NT % (W + 4) == 0 && H % (NT / (W + 4)) == 0, "y-sweep segments must tile the block");
+    if (!load_tile<NV, SP, TR, GLOBAL_TMAP>(Qs, J.tmap, J.x0, J.y0, bar, phase, init_bar, err)) return false;
+    const int x0 = J.x0, y0 = J.y0;
+    if (x0 == 0 || x0 + W + 2 > J.nx || y0 == 0 || y0 + H + 2 > J.ny) apply_boundary<NV, W, H, NT>(Qs, J);
+
+    SweepPar p;
+    p.theta = P.theta;
+    p.g = P.g;
+    p.half_g = 0.5f * P.g;
+    p.inv_g = 1.0f / P.g;
+    p.gamma = P.gamma;
+    p.kdt = P.kdt;
+    const bool x_first = (SCHEME == FORCE || SCHEME == HLL) ? true : (P.substep == 0);
+    if (x_first) {
+        p.dxx = P.dx;
+        sweep_x<SCHEME, NV, W, H, NT>(Qs, 2 - G, H + 2 + G, p);
+        p.dxx = P.dy;
+        sweep_y<SCHEME, NV, W, H, NT>(Qs, 4, W + 4, p);
+    } else {
+        p.dxx = P.dy;
+        sweep_y<SCHEME, NV, W, H, NT>(Qs, 4 - G, W + 4 + G, p);
+        p.dxx = P.dx;
+        sweep_x<SCHEME, NV, W, H, NT>(Qs, 2, H + 2, p);
+    }
+
+    // copy-out of the interior (+ gravity source, CFL, sums)
+    constexpr int QW = W / 4;
+    const float gg = (SCHEME == EE2D) ? P.gamma : P.g;
+    for (int i = threadIdx.x; i < H * QW; i += NT) {
+        const int r = i / QW, q = i - r * QW;
+        const int y = y0 + r, x = x0 + 4 * q;
+        if (y >= J.ny || x >= J.nx) continue;
+        float4 val[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) val[v] = *reinterpret_cast<const float4*>(Qs + v * PS + (r + 2) * SP + 4 + 4 * q);
+        if (SCHEME == EE2D) {
+            if (P.g > 0.0f) {
+                // gravity source (GPUSimulators/cuda/EE2D_KP07_dimsplit.cu:197-205)
+                const float gsrc = P.g;
+                float* r0 = &val[0].x;
+                float* r2 = &val[2].x;
+                float* r3 = &val[3].x;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const float rho_v = r2[j];
+                    r2[j] = r2[j] - gsrc * r0[j] * P.kdt;
+                    r3[j] = r3[j] - gsrc * rho_v * P.kdt;
+                }
+            }
+        }
+        const long long gi = cell_index(y, x, J.pitch);
+        const int nvalid = min(4, J.nx - x);
+        if (nvalid == 4) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) *reinterpret_cast<float4*>(J.out[v] + gi) = val[v];
+        } else {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                const float* e = &val[v].x;
+                for (int j = 0; j < nvalid; ++j) J.out[v][gi + j] = e[j];
+            }
+        }
+        if (do_cfl || sums) {
+            const float* h = &val[0].x;
+            const float* hu = &val[1].x;
+            const float* hv = &val[2].x;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (j < nvalid) {
+                    if (do_cfl) my_cfl = fminf(my_cfl, cell_cfl(h[j], hu[j], hv[j], P.dx, P.dy, gg));
+                    if (sums) {
+#pragma unroll
+                        for (int v = 0; v < NV; ++v) my_sums[v] += (double)(&val[v].x)[j];
+                    }
+                }
+            }
+        }
+    }
+    return true;
+}
+
+template <int SCHEME, int W, int H, int NT>
+__global__ void __launch_bounds__(NT) dimsplit_stage_kernel(const __grid_constant__ StageArgs A) {
+    constexpr int NV = (SCHEME == EE2D) ? 4 : 3;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     float* Qs = reinterpret_cast<float*>(smem_raw);
     __shared__ __align__(8) uint64_t bar;
@@ -596,94 +726,97 @@ __global__ void __launch_bounds__(NT) dimsplit_stage_kernel(const __grid_constan
     StepCtl sc = read_step(A);
     if (!sc.active) return;
     if (SCHEME == WAF) sc.do_cfl = false;  // WAFKernel has no CFL output (GPUSimulators/cuda/SWE2D_WAF.cu:103-119)
-    const int x0 = blockIdx.x * W, y0 = blockIdx.y * H;
     float my_cfl = __int_as_float(0x7f800000);
     double my_sums[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) my_sums[v] = 0.0;
     const bool sums = A.want_sums && A.is_last;
 
-    if (load_tile<NV, SP, TR>(Qs, A, sc.cur, x0, y0, &bar)) {
-        if (x0 == 0 || x0 + W + 2 > A.nx || y0 == 0 || y0 + H + 2 > A.ny)
-            apply_boundary<NV, W, H, NT>(Qs, A, sc.cur, x0, y0);
-
-        SweepPar p;
-        p.theta = A.theta;
-        p.g = A.g;
-        p.half_g = 0.5f * A.g;
-        p.inv_g = 1.0f / A.g;
-        p.gamma = A.gamma;
-        p.kdt = sc.dt * A.dt_scale;
-        const bool x_first = (SCHEME == FORCE || SCHEME == HLL) ? true : (A.substep == 0);
-        if (x_first) {
-            p.dxx = A.dx;
-            sweep_x<SCHEME, NV, W, H, NT>(Qs, 2 - G, H + 2 + G, p);
-            p.dxx = A.dy;
-            sweep_y<SCHEME, NV, W, H, NT>(Qs, 4, W + 4, p);
-        } else {
-            p.dxx = A.dy;
-            sweep_y<SCHEME, NV, W, H, NT>(Qs, 4 - G, W + 4 + G, p);
-            p.dxx = A.dx;
-            sweep_x<SCHEME, NV, W, H, NT>(Qs, 2, H + 2, p);
-        }
-
-        // copy-out of the interior (+ gravity source, CFL, sums)
-        constexpr int QW = W / 4;
-        const float gg = (SCHEME == EE2D) ? A.gamma : A.g;
-        const int out = sc.cur ^ 1;
-        for (int i = threadIdx.x; i < H * QW; i += NT) {
-            const int r = i / QW, q = i - r * QW;
-            const int y = y0 + r, x = x0 + 4 * q;
-            if (y >= A.ny || x >= A.nx) continue;
-            float4 val[NV];
-#pragma unroll
-            for (int v = 0; v < NV; ++v)
-                val[v] = *reinterpret_cast<const float4*>(Qs + v * PS + (r + 2) * SP + 4 + 4 * q);
-            if (SCHEME == EE2D) {
-                if (A.g > 0.0f) {
-                    // gravity source (GPUSimulators/cuda/EE2D_KP07_dimsplit.cu:197-205)
-                    const float gdt = A.g;
-                    float* r0 = &val[0].x;
-                    float* r2 = &val[2].x;
-                    float* r3 = &val[3].x;
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const float rho_v = r2[j];
-                        r2[j] = r2[j] - gdt * r0[j] * p.kdt;
-                        r3[j] = r3[j] - gdt * rho_v * p.kdt;
-                    }
-                }
-            }
-            const long long gi = cell_index(y, x, A.pitch);
-            const int nvalid = min(4, A.nx - x);
-            if (nvalid == 4) {
-#pragma unroll
-                for (int v = 0; v < NV; ++v) *reinterpret_cast<float4*>(A.buf[out][v] + gi) = val[v];
-            } else {
-#pragma unroll
-                for (int v = 0; v < NV; ++v) {
-                    const float* e = &val[v].x;
-                    for (int j = 0; j < nvalid; ++j) A.buf[out][v][gi + j] = e[j];
-                }
-            }
-            if (sc.do_cfl || sums) {
-                const float* h = &val[0].x;
-                const float* hu = &val[1].x;
-                const float* hv = &val[2].x;
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    if (j < nvalid) {
-                        if (sc.do_cfl) my_cfl = fminf(my_cfl, cell_cfl(h[j], hu[j], hv[j], A.dx, A.dy, gg));
-                        if (sums) {
-#pragma unroll
-                            for (int v = 0; v < NV; ++v) my_sums[v] += (double)(&val[v].x)[j];
-                        }
-                    }
-                }
-            }
-        }
-    }
+    TileJob J;
+    J.tmap = &A.tmap[sc.cur][0];
+    J.in = A.buf[sc.cur];
+    J.out = A.buf[sc.cur ^ 1];
+    J.nx = A.nx;
+    J.ny = A.ny;
+    J.pitch = A.pitch;
+    J.bc = A.bc;
+    J.x0 = blockIdx.x * W;
+    J.y0 = blockIdx.y * H;
+    SplitPar P{A.dx, A.dy, A.g, A.gamma, A.theta, sc.dt * A.dt_scale, A.substep};
+    process_tile_dimsplit<SCHEME, W, H, NT>(Qs, &bar, 0, true, J, P, sc.do_cfl, sums, &A.ctl->error, my_cfl, my_sums);
     stage_epilogue<NT, NV>(A, sc, my_cfl, my_sums, sums);
+}
+
+// ------------------------------------------------------------------ batched persistent stage kernel
+
+// One simulation of a batch, resident in device memory (64-byte aligned for
+// its tensor maps).
+struct alignas(64) BatchInstance {
+    CUtensorMap tmap[2][4];
+    float* buf[2][4];
+    SimCtl* ctl;
+    float* block_cfl;    // one float per tile of this simulation
+    double* block_sums;  // 4 doubles per tile
+    int nx, ny, pitch, bc;
+    int tiles_x, ntiles;
+    float dx, dy, g, gamma, theta, dt_scale;
+};
+
+struct BatchArgs {
+    const BatchInstance* inst;
+    const int2* work;     // (instance, tile within instance) per work item
+    const int* nwork;     // number of work items (device scalar, updated between graph replays)
+    int substep;
+    int is_last;
+    int want_sums;
+    int* err;
+};
+
+// Persistent split-scheme stage: the CTAs walk the work list of all tiles of
+// all simulations of the batch; each simulation keeps its own t, dt (its own
+// CFL every 100 of its steps) and t_end, and its last tile finalises its
+// control block exactly as the single-simulation kernel does.  Simulations
+// that reached t_end are skipped.  The work list lives in device memory, so
+// one captured CUDA graph serves any batch composition.
+template <int SCHEME, int W, int H, int NT>
+__global__ void __launch_bounds__(NT) batched_stage_kernel(const __grid_constant__ BatchArgs B) {
+    constexpr int NV = (SCHEME == EE2D) ? 4 : 3;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    float* Qs = reinterpret_cast<float*>(smem_raw);
+    __shared__ __align__(8) uint64_t bar;
+    const int n = *B.nwork;
+    uint32_t phase = 0;
+    bool init = true;
+    for (int w = blockIdx.x; w < n; w += gridDim.x) {
+        const int2 job = B.work[w];
+        const BatchInstance& I = B.inst[job.x];
+        StepCtl sc = read_step(I.ctl, false, 0.0f, false, B.is_last != 0);
+        if (!sc.active) continue;  // uniform across the CTA
+        if (SCHEME == WAF) sc.do_cfl = false;
+        float my_cfl = __int_as_float(0x7f800000);
+        double my_sums[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) my_sums[v] = 0.0;
+        const bool sums = B.want_sums && B.is_last;
+        TileJob J;
+        J.tmap = &I.tmap[sc.cur][0];
+        J.in = I.buf[sc.cur];
+        J.out = I.buf[sc.cur ^ 1];
+        J.nx = I.nx;
+        J.ny = I.ny;
+        J.pitch = I.pitch;
+        J.bc = I.bc;
+        const int ty = job.y / I.tiles_x;
+        J.x0 = (job.y - ty * I.tiles_x) * W;
+        J.y0 = ty * H;
+        SplitPar P{I.dx, I.dy, I.g, I.gamma, I.theta, sc.dt * I.dt_scale, B.substep};
+        process_tile_dimsplit<SCHEME, W, H, NT, true>(Qs, &bar, phase, init, J, P, sc.do_cfl, sums, B.err, my_cfl,
+                                                      my_sums);
+        init = false;
+        phase ^= 1u;
+        tile_epilogue<NT, NV>(I.ctl, I.block_cfl, I.block_sums, job.y, I.ntiles, B.is_last != 0, false, sc, my_cfl,
+                              my_sums, sums);
+    }
 }
 
 // ------------------------------------------------------------------ unsplit stage kernel (LxF, KP07)
@@ -710,9 +843,18 @@ __global__ void __launch_bounds__(NT) unsplit_stage_kernel(const __grid_constant
     double my_sums[3] = {0.0, 0.0, 0.0};
     const bool sums = A.want_sums && A.is_last;
 
-    if (load_tile<3, SP, TR>(Qs, A, sc.cur, x0, y0, &bar)) {
-        if (x0 == 0 || x0 + W + 2 > A.nx || y0 == 0 || y0 + H + 2 > A.ny)
-            apply_boundary<3, W, H, NT>(Qs, A, sc.cur, x0, y0);
+    TileJob J;
+    J.tmap = &A.tmap[sc.cur][0];
+    J.in = A.buf[sc.cur];
+    J.out = A.buf[sc.cur ^ 1];
+    J.nx = A.nx;
+    J.ny = A.ny;
+    J.pitch = A.pitch;
+    J.bc = A.bc;
+    J.x0 = x0;
+    J.y0 = y0;
+    if (load_tile<3, SP, TR>(Qs, J.tmap, x0, y0, &bar, 0, true, &A.ctl->error)) {
+        if (x0 == 0 || x0 + W + 2 > A.nx || y0 == 0 || y0 + H + 2 > A.ny) apply_boundary<3, W, H, NT>(Qs, J);
         const float kdt = sc.dt * A.dt_scale;
         const float g = A.g, half_g = 0.5f * g, theta = A.theta;
         const float k4x = A.dx / (4.0f * kdt), k4y = A.dy / (4.0f * kdt);
@@ -810,7 +952,7 @@ __global__ void __launch_bounds__(NT) unsplit_stage_kernel(const __grid_constant
                     for (int v = 0; v < 3; ++v) {
                         const float q = Qs[v * PS + t * SP + s];
                         const float Fw = Fs[(v * H + r) * FW + i], Fe = Fs[(v * H + r) * FW + i + 1];
-                        qn[v] = q + ((Fw - Fe) * kdx + (Gs[v] - Gn[v]) * kdy);
+                        qn[v] = q + fmaf(Fw - Fe, kdx, (Gs[v] - Gn[v]) * kdy);
                     }
 #pragma unroll
                     for (int v = 0; v < 3; ++v) {

@@ -1,0 +1,147 @@
+"""Serving scenarios with continuous batching.
+
+A request is one scenario: scheme, grid, initial state and t_end.  The server
+keeps the state of every admitted scenario resident in HBM inside one Batch
+per scheme, advances all of them a few steps at a time (each batch on its own
+stream, so the schemes overlap on the GPU), returns each scenario as soon as
+it reaches its t_end, and admits waiting requests whenever their arrival time
+has passed and the device-memory budget has room.  Requests that arrive
+while others run join the running batches at the next chunk boundary.
+
+Each scenario follows the reference's simulate(t_end) semantics on its own
+(see batch.py), so its result does not depend on what else is in the batch.
+"""
+
+from __future__ import annotations
+
+import collections
+import dataclasses
+import time
+from typing import Dict, List, Optional
+
+import numpy as np
+
+from .batch import Batch
+from .Simulator import BoundaryCondition
+
+SCHEME_PARAMS = {
+    "KP07_dimsplit": dict(g=9.81),
+    "HLL": dict(g=9.81),
+    "EE2D_KP07_dimsplit": dict(g=0.0, gamma=1.4),
+}
+
+
+@dataclasses.dataclass
+class Request:
+    rid: int
+    scheme: str
+    variables: list
+    nx: int
+    ny: int
+    dx: float
+    dy: float
+    t_end: float
+    arrival: float = 0.0  # seconds after the start of serve()
+    boundary_conditions: Optional[BoundaryCondition] = None
+
+
+@dataclasses.dataclass
+class Result:
+    rid: int
+    scheme: str
+    state: list
+    steps: int
+    t: float
+    arrival: float
+    admitted: float
+    finished: float
+
+    @property
+    def latency(self):
+        return self.finished - self.arrival
+
+
+def state_bytes(scheme, nx, ny, tile_w=60, tile_h=28):
+    """Device bytes one scenario holds (two state buffers plus tile scratch)."""
+    nv = 4 if scheme == "EE2D_KP07_dimsplit" else 3
+    pitch = (nx + 8 + 31) // 32 * 32
+    tiles = -(-nx // tile_w) * -(-ny // tile_h)
+    return 2 * nv * (ny + 4) * pitch * 4 + tiles * 36 + 512
+
+
+class Server(object):
+    def __init__(self, context, budget_bytes=120e9, chunk_steps=8, max_instances=4096, schemes=None,
+                 cfl_scale=0.9):
+        self.context = context
+        self.budget = float(budget_bytes)
+        self.chunk = int(chunk_steps)
+        schemes = schemes or list(SCHEME_PARAMS)
+        self.batches: Dict[str, Batch] = {
+            s: Batch(context, s, cfl_scale=cfl_scale, max_instances=max_instances, **SCHEME_PARAMS[s])
+            for s in schemes
+        }
+        self.used = 0.0
+
+    def serve(self, requests: List[Request], clock=time.perf_counter):
+        pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
+        running = {}  # (scheme, slot) -> (request, admitted, bytes)
+        results: List[Result] = []
+        t0 = clock()
+        busy_since = None
+        cells = 0
+        while pending or running:
+            now = clock() - t0
+            # admission: arrived requests, in arrival order, while the budget allows
+            while pending and pending[0].arrival <= now:
+                r = pending[0]
+                need = state_bytes(r.scheme, r.nx, r.ny)
+                if self.used + need > self.budget:
+                    break
+                try:
+                    slot = self.batches[r.scheme].add(r.variables, r.nx, r.ny, r.dx, r.dy, r.t_end,
+                                                      r.boundary_conditions)
+                except MemoryError:
+                    break
+                pending.popleft()
+                self.used += need
+                running[(r.scheme, slot)] = (r, clock() - t0, need)
+            if not running:
+                if pending:
+                    wait = pending[0].arrival - (clock() - t0)
+                    if wait > 0:
+                        time.sleep(min(wait, 0.01))
+                continue
+            if busy_since is None:
+                busy_since = clock() - t0
+            active = {s for (s, _) in running}
+            for s in active:
+                self.batches[s].run(self.chunk)
+            for s in active:
+                self.batches[s].sync()
+            done = []
+            for key, (r, admitted, need) in running.items():
+                s, slot = key
+                st = self.batches[s].status(slot)
+                if st["done"]:
+                    state = self.batches[s].download(slot)
+                    fin = clock() - t0
+                    results.append(Result(r.rid, s, state, st["nt"], st["t"], r.arrival, admitted, fin))
+                    cells += r.nx * r.ny * st["nt"]
+                    done.append(key)
+            for key in done:
+                s, slot = key
+                self.batches[s].remove(slot)
+                self.used -= running[key][2]
+                del running[key]
+        elapsed = clock() - t0
+        lat = np.array([r.latency for r in results]) if results else np.zeros(1)
+        stats = {
+            "requests": len(results),
+            "elapsed_s": elapsed,
+            "cell_updates": cells,
+            "cell_updates_per_s": cells / max(elapsed - (busy_since or 0.0), 1e-9),
+            "p50_latency_s": float(np.percentile(lat, 50)),
+            "p99_latency_s": float(np.percentile(lat, 99)),
+            "mean_latency_s": float(lat.mean()),
+        }
+        return results, stats

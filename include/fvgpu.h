@@ -143,6 +143,36 @@ FV_API int fv_sim_info(fv_sim* sim, int* tile_w, int* tile_h, int* threads, int*
  * call, measured with CUDA events on the simulation's stream (0 if unknown). */
 FV_API int fv_sim_last_advance_ms(fv_sim* sim, double* ms);
 
+/* ---- Batches: many simulations of one split scheme advanced together.
+ * No counterpart in the reference (it runs one simulation per class instance);
+ * each simulation in a batch follows exactly the reference's simulate(t_end)
+ * semantics (own CFL dt every 100 of its own steps, last step shortened to
+ * t_end), so its result equals a plain fv_sim_simulate of the same scenario. */
+typedef struct fv_batch fv_batch;
+
+/* Scheme: FV_FORCE, FV_HLL, FV_HLL2, FV_WAF, FV_KP07_DIMSPLIT or
+ * FV_EE2D_KP07_DIMSPLIT; params->tile selects the batched kernel's tile shape. */
+FV_API int fv_batch_create(fv_context* ctx, int scheme, const fv_params* params, int max_instances, fv_batch** out);
+FV_API int fv_batch_destroy(fv_batch* batch);
+/* Admits one simulation (initial state as for fv_sim_create) that runs until
+ * its time reaches t_end; returns its slot. */
+FV_API int fv_batch_add(fv_batch* batch, int nx, int ny, float dx, float dy, int bc, const float* const* host_vars,
+                        int host_rows, int host_cols, double t_end, int* slot);
+FV_API int fv_batch_remove(fv_batch* batch, int slot);
+/* Queues n_steps steps for every simulation of the batch (CUDA graphs of the
+ * persistent kernel); simulations that reached t_end do nothing. Asynchronous. */
+FV_API int fv_batch_run(fv_batch* batch, int n_steps);
+/* Waits for queued work and refreshes the host view of every simulation. */
+FV_API int fv_batch_sync(fv_batch* batch);
+/* t, nt, dt and whether the simulation reached t_end, as of the last sync. */
+FV_API int fv_batch_status(fv_batch* batch, int slot, double* t, long long* nt, float* dt, int* done);
+FV_API int fv_batch_download(fv_batch* batch, int slot, int var, float* host, int host_pitch);
+/* Device bytes held, simulations in the batch, work-list length, device time
+ * of the last fv_batch_run (ms, valid after fv_batch_sync). */
+FV_API int fv_batch_info(fv_batch* batch, size_t* device_bytes, int* active, int* work_items, double* last_run_ms);
+/* Tile shape, threads per CTA and persistent grid size of the batch's kernel. */
+FV_API int fv_batch_tile(fv_batch* batch, int* tile_w, int* tile_h, int* threads, int* grid);
+
 /* One KP07_dimsplit substep (GPUSimulators/cuda/SWE2D_KP07_dimsplit.cu semantics)
  * that allocates no memory: for callers that may not call cudaMalloc, such as
  * applications that own all device memory through their own pool, or loops

@@ -1,0 +1,139 @@
+"""Batched and served simulations give the same results as plain ones.
+
+Each simulation in a batch keeps its own CFL time step and t_end, so its
+result must equal a plain simulator's simulate(t_end) of the same scenario,
+alone or mixed with other simulations, whatever joins or leaves the batch in
+between.  The product kernels are the same code in both paths, so the results
+are compared exactly (tolerance 0), plus against the CPU oracle.
+"""
+
+import numpy as np
+import pytest
+
+from conftest import bump, dam_break, kelvin_helmholtz, rel_linf
+
+import finitevolumegpu_b200 as fv
+from finitevolumegpu_b200.batch import Batch
+from finitevolumegpu_b200.server import Request, Server
+from oracle.oracle import OracleSim
+
+pytestmark = pytest.mark.gpu
+
+PERIODIC = fv.BoundaryCondition(fv.BoundaryCondition.getTypes(0x02020202))
+
+
+def scenario(scheme, nx, ny, kind, seed):
+    rng = np.random.default_rng(seed)
+    if scheme == "EE2D_KP07_dimsplit":
+        return kelvin_helmholtz(nx, ny, phase=rng.uniform(0, 6.28)), 1.0 / nx, 1.0 / ny, 0.02 + 0.03 * rng.random()
+    if kind == "bump":
+        q = bump(nx, ny, amp=rng.uniform(0.1, 0.5), cx=rng.uniform(0.3, 0.7) * nx, cy=rng.uniform(0.3, 0.7) * ny,
+                 sigma=min(20.0, min(nx, ny) / 4))
+    else:
+        q = dam_break(nx, ny, radius_frac=rng.uniform(0.1, 0.3))
+    return list(q), 1.0, 1.0, float(rng.uniform(2.0, 8.0))
+
+
+def plain(ctx, scheme, q, nx, ny, dx, dy, t_end, bc=None):
+    cls = fv.SCHEMES[scheme]
+    kw = {} if bc is None else {"boundary_conditions": bc}
+    if scheme == "EE2D_KP07_dimsplit":
+        sim = cls(ctx, *q, nx, ny, dx, dy, 0.0, 1.4, **kw)
+    else:
+        sim = cls(ctx, *q, nx, ny, dx, dy, 9.81, **kw)
+    sim.simulate(t_end)
+    return sim.download(), sim.simSteps(), sim.simTime()
+
+
+SIZES = [(64, 64), (97, 150), (300, 70), (130, 131), (33, 200), (250, 250)]
+
+
+@pytest.mark.parametrize("scheme", ["KP07_dimsplit", "HLL", "EE2D_KP07_dimsplit", "HLL2", "WAF", "FORCE"])
+def test_batch_equals_plain(ctx, scheme):
+    b = Batch(ctx, scheme, g=0.0 if scheme == "EE2D_KP07_dimsplit" else 9.81, max_instances=16)
+    bc = PERIODIC if scheme == "EE2D_KP07_dimsplit" else None
+    cases = {}
+    for k, (nx, ny) in enumerate(SIZES):
+        q, dx, dy, t_end = scenario(scheme, nx, ny, "bump" if k % 2 else "dam", k)
+        slot = b.add(q, nx, ny, dx, dy, t_end, bc)
+        cases[slot] = (q, nx, ny, dx, dy, t_end)
+    b.run_to_completion()
+    for slot, (q, nx, ny, dx, dy, t_end) in cases.items():
+        st = b.status(slot)
+        got = b.download(slot)
+        want, nt, t = plain(ctx, scheme, q, nx, ny, dx, dy, t_end, bc)
+        assert st["nt"] == nt and st["t"] == t, (slot, st, nt, t)
+        for a, w in zip(got, want):
+            assert np.array_equal(a, w), (scheme, slot, rel_linf(a, w))
+
+
+def test_batch_matches_oracle(ctx):
+    b = Batch(ctx, "KP07_dimsplit", max_instances=4)
+    q, dx, dy, t_end = scenario("KP07_dimsplit", 90, 70, "bump", 7)
+    slot = b.add(q, 90, 70, dx, dy, t_end)
+    b.run_to_completion()
+    ref = OracleSim("KP07_dimsplit", q, 90, 70, dx, dy, 9.81)
+    ref.simulate(t_end)
+    assert b.status(slot)["nt"] == ref.nt
+    for a, w in zip(b.download(slot), ref.download()):
+        assert rel_linf(a, w) < 2e-5
+
+
+def test_batch_join_and_leave(ctx):
+    """Simulations join and leave between chunks without disturbing the others."""
+    b = Batch(ctx, "KP07_dimsplit", max_instances=8)
+    cases = {}
+    for k, (nx, ny) in enumerate(SIZES[:3]):
+        q, dx, dy, t_end = scenario("KP07_dimsplit", nx, ny, "bump", 10 + k)
+        cases[b.add(q, nx, ny, dx, dy, t_end)] = (q, nx, ny, dx, dy, t_end)
+    b.run(5)
+    b.sync()
+    victim = next(iter(cases))
+    b.remove(victim)
+    del cases[victim]
+    for k, (nx, ny) in enumerate(SIZES[3:]):
+        q, dx, dy, t_end = scenario("KP07_dimsplit", nx, ny, "dam", 20 + k)
+        cases[b.add(q, nx, ny, dx, dy, t_end)] = (q, nx, ny, dx, dy, t_end)
+    b.run_to_completion()
+    for slot, (q, nx, ny, dx, dy, t_end) in cases.items():
+        want, nt, _ = plain(ctx, "KP07_dimsplit", q, nx, ny, dx, dy, t_end)
+        assert b.status(slot)["nt"] == nt
+        for a, w in zip(b.download(slot), want):
+            assert np.array_equal(a, w)
+
+
+def test_server_same_alone_and_in_mix(ctx):
+    """Requests arriving over time, three schemes mixed, each result equal to a solo run."""
+    rng = np.random.default_rng(3)
+    reqs = []
+    schemes = ["KP07_dimsplit", "HLL", "EE2D_KP07_dimsplit"]
+    for i in range(18):
+        s = schemes[i % 3]
+        nx, ny = int(rng.integers(40, 200)), int(rng.integers(40, 200))
+        q, dx, dy, t_end = scenario(s, nx, ny, "bump" if i % 2 else "dam", 100 + i)
+        bc = PERIODIC if s == "EE2D_KP07_dimsplit" else None
+        reqs.append(Request(i, s, q, nx, ny, dx, dy, t_end, arrival=0.002 * i, boundary_conditions=bc))
+    server = Server(ctx, budget_bytes=2e9, chunk_steps=4, max_instances=64)
+    results, stats = server.serve(reqs)
+    assert stats["requests"] == len(reqs)
+    assert stats["p99_latency_s"] >= stats["p50_latency_s"] > 0
+    by_id = {r.rid: r for r in results}
+    for r in reqs:
+        res = by_id[r.rid]
+        want, nt, t = plain(ctx, r.scheme, r.variables, r.nx, r.ny, r.dx, r.dy, r.t_end, r.boundary_conditions)
+        assert res.steps == nt and res.t == t
+        for a, w in zip(res.state, want):
+            assert np.array_equal(a, w), (r.rid, r.scheme, rel_linf(a, w))
+
+
+def test_server_respects_memory_budget(ctx):
+    """With a budget for about two scenarios at a time, all requests still complete."""
+    reqs = []
+    for i in range(6):
+        q, dx, dy, t_end = scenario("KP07_dimsplit", 256, 256, "bump", 200 + i)
+        reqs.append(Request(i, "KP07_dimsplit", q, 256, 256, dx, dy, t_end, arrival=0.0))
+    server = Server(ctx, budget_bytes=2.5 * 2 * 3 * 260 * 288 * 4, chunk_steps=8, schemes=["KP07_dimsplit"])
+    results, stats = server.serve(reqs)
+    assert stats["requests"] == 6
+    admitted = sorted(r.admitted for r in results)
+    assert admitted[-1] > admitted[0]  # later requests waited for memory

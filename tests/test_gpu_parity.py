@@ -145,7 +145,10 @@ def test_dirichlet_ghost_semantics(ctx, scheme):
     The upload fills u0's ghost cells; u1 starts as zeros and no kernel writes
     ghost cells (GPUSimulators/cuda/common.h:376), so every other substep sees
     zero depth at the boundary and produces NaN there, in the reference as here.
-    The NaN pattern and the finite values must both match the oracle.
+    The NaN pattern must match the CPU oracle and the reference kernels; the
+    finite values are compared with the reference kernels, because cells next
+    to a NaN front depend on the sign bit of NaN (positive on the GPU, negative
+    on x86), which the minmod sign test reads.
     """
     nx, ny = 77, 45
     gc = 1 if scheme in ("LxF", "FORCE", "HLL") else 2
@@ -159,24 +162,19 @@ def test_dirichlet_ghost_semantics(ctx, scheme):
         kw = dict(dx=1.0, dy=1.0, g=9.81)
         okw = {}
     sim = make_sim(ctx, scheme, q, nx, ny, bc=DIRICHLET, cfl_scale=0.45, **kw)
-
-    def run(qq):
-        o = OracleSim(scheme, qq, nx, ny, kw["dx"], kw["dy"], kw["g"], cfl_scale=0.45, bc=DIRICHLET, **okw)
-        for _ in range(2):
-            o.step(np.float32(o.computeDt() * np.float32(0.45)))
-        return o.download()
-
+    ref = ref_kernels.RefKernelSim(scheme, q, nx, ny, kw["dx"], kw["dy"], kw["g"], cfl_scale=0.45, bc=DIRICHLET,
+                                   **okw)
+    orc = OracleSim(scheme, q, nx, ny, kw["dx"], kw["dy"], kw["g"], cfl_scale=0.45, bc=DIRICHLET, **okw)
     for _ in range(2):
         sim.step(sim.computeDt() * np.float32(0.45))
-    want = run(q)
-    # Cells next to zero-depth ghosts are ill-conditioned (u = hu/h with h -> 0):
-    # the bound is the larger of 2e-5 and four times the oracle's one-ulp spread.
-    sens = ulp_sensitivity(run, q)
-    for a, b, (sinf, _) in zip(sim.download(), want, sens):
-        assert np.array_equal(np.isnan(a), np.isnan(b))
-        m = np.isfinite(b)
+        for o in (ref, orc):
+            o.step(np.float32(o.computeDt() * np.float32(0.45)))
+    for a, r, o in zip(sim.download(), ref.download(), orc.download()):
+        assert np.array_equal(np.isnan(a), np.isnan(o))
+        assert np.array_equal(np.isnan(a), np.isnan(r))
+        m = np.isfinite(r)
         assert m.any()
-        assert rel_linf(a[m], b[m]) <= max(2e-5, 4.0 * sinf), (rel_linf(a[m], b[m]), sinf)
+        assert rel_linf(a[m], r[m]) <= 2e-5, rel_linf(a[m], r[m])
 
 
 def test_mass_conservation(ctx):
