@@ -347,15 +347,39 @@ def run_served(ctx, n_req=400, rate=300.0, seed=5, plain_sample=60):
     return stats
 
 
+# Algorithmic HBM bytes per cell per stage launch, averaged over the launches of
+# one step: state read + written (3 or 4 FP32 variables); KP07's second RK
+# stage also reads u^n, so its two launches average (24 + 36) / 2.
+BYTES_PER_CELL_LAUNCH = {"LxF": 24, "FORCE": 24, "HLL": 24, "HLL2": 24, "WAF": 24, "KP07": 30,
+                         "KP07_dimsplit": 24, "EE2D_KP07_dimsplit": 32}
+
+
+def make_scheme_sim(ctx, scheme, seed):
+    """The benchmark workload of one scheme: a seeded circular dam break on NX x NY (SWE), or the
+    Kelvin-Helmholtz problem on NX x NX/2 with periodic boundaries (Euler)."""
+    from finitevolumegpu_b200 import SCHEMES, BoundaryCondition
+
+    if scheme == "EE2D_KP07_dimsplit":
+        nx, ny = NX, NX // 2
+        q = kh_ic(nx, ny, np.random.default_rng(seed))
+        bc = BoundaryCondition(BoundaryCondition.getTypes(0x02020202))
+        sim = SCHEMES[scheme](ctx, q[0], q[1], q[2], q[3], nx, ny, 1.0 / nx, 1.0 / ny, 0.0, 1.4,
+                              boundary_conditions=bc)
+        return sim, nx, ny, q, "Kelvin-Helmholtz %dx%d, periodic" % (nx, ny)
+    h, hu, hv, R = dam_break_4096(seed=seed)
+    sim = SCHEMES[scheme](ctx, h, hu, hv, NX, NY, 1.0, 1.0, 9.81)
+    return sim, NX, NY, [h, hu, hv], "circular dam break %dx%d (R=%.0f cells), reflective walls" % (NX, NY, R)
+
+
 def run_mine(args, rank, world, local_rank):
     import torch
 
-    from finitevolumegpu_b200 import CudaContext, KP07_dimsplit, _lib
+    from finitevolumegpu_b200 import CudaContext, SCHEMES, _lib
 
     dist = world > 1
     ctx = CudaContext.CudaContext(device=local_rank, autotuning=True)
-    h, hu, hv, R = dam_break_4096(seed=rank)
-    sim = KP07_dimsplit.KP07_dimsplit(ctx, h, hu, hv, NX, NY, 1.0, 1.0, 9.81)
+    scheme = args.scheme
+    sim, nx, ny, q0, desc = make_scheme_sim(ctx, scheme, rank)
     sim.advance(args.warmup)
     info = sim.tile_info()
 
@@ -377,20 +401,21 @@ def run_mine(args, rank, world, local_rank):
         t = torch.tensor([T], dtype=torch.float64, device="cuda:%d" % local_rank)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         T = float(t.item())
-    cells = NX * NY
+    cells = nx * ny
     value = world * cells * args.steps / T
     launches = args.steps * info["launches_per_step"]
 
     # roofline of the dominant kernel (the stage kernel)
     pk, pk_kind = peaks()
     launch_s = T / launches
-    alg_bytes = BYTES_PER_CELL_SUBSTEP * cells
+    alg_bytes = BYTES_PER_CELL_LAUNCH[scheme] * cells
     achieved = alg_bytes / launch_s / 1e9
-    prof = load_profile()
+    prof = load_profile() if scheme == SCHEME and NX == 4096 else {}
     traffic = prof.get("dram_bytes_per_launch")
     roof = {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / pk["hbm_gbs"], "traffic": traffic, "peak_kind": pk_kind,
-            "kernel": "dimsplit_stage_kernel<KP07_DIMSPLIT,%d,%d,%d>" % (info["tile_w"], info["tile_h"], info["threads"]),
+            "kernel": "%s stage kernel, tile %dx%d, %d threads" % (scheme, info["tile_w"], info["tile_h"],
+                                                                    info["threads"]),
             "algorithmic_bytes_per_launch": alg_bytes}
     if prof.get("fp32_flop_per_launch"):
         clk = clocks.summary().get("sm_mhz") or 1965.0
@@ -406,10 +431,11 @@ def run_mine(args, rank, world, local_rank):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": T / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": "KP07_dimsplit 4096x4096 circular dam break (R=%.0f cells), reflective walls, "
-                                   "simulate() dt schedule, cfl_scale 0.9" % R,
-                       "scheme": SCHEME, "nx": NX, "ny": NY, "parallelism": "replicas" if world > 1 else "single",
-                       "tile": info, "l2": "state 403 MB > 126 MB L2; no flush"},
+            "config": {"workload": "%s %s, simulate() dt schedule, cfl_scale 0.9" % (scheme, desc),
+                       "scheme": scheme, "nx": nx, "ny": ny, "parallelism": "replicas" if world > 1 else "single",
+                       "tile": info,
+                       "l2": "state %.0f MB (two buffers) > 126 MB L2; no flush" % (
+                           2 * (4 if scheme == "EE2D_KP07_dimsplit" else 3) * cells * 4 / 1e6)},
             "roofline": roof,
             "gpu_launches": launches,
             "clocks": clocks.summary(),
@@ -417,7 +443,8 @@ def run_mine(args, rank, world, local_rank):
         }
     # end-to-end through the public API: pinned upload, K steps, download
     e2e = None
-    if rank == 0 and not args.no_e2e:
+    if rank == 0 and not args.no_e2e and scheme == SCHEME:
+        h, hu, hv = q0
         nbytes = cells * 4
         L = _lib.lib()
         bufs = []
@@ -436,7 +463,7 @@ def run_mine(args, rank, world, local_rank):
         hout = [pinned((NY, NX)) for _ in range(3)]
         torch.cuda.synchronize(local_rank)
         t0 = time.perf_counter()
-        s2 = KP07_dimsplit.KP07_dimsplit(ctx, hin[0], hin[1], hin[2], NX, NY, 1.0, 1.0, 9.81)
+        s2 = SCHEMES[SCHEME](ctx, hin[0], hin[1], hin[2], NX, NY, 1.0, 1.0, 9.81)
         s2.advance(args.steps)
         for v in range(3):
             s2._download_var(v, hout[v])
@@ -448,11 +475,11 @@ def run_mine(args, rank, world, local_rank):
                "h2d_bytes_per_step": 3 * nbytes / args.steps, "d2h_bytes_per_step": 3 * nbytes / args.steps,
                "what": "constructor with pinned host upload + %d steps + download of the final state" % args.steps}
         result["e2e"] = e2e
-    if rank == 0 and world == 1 and not args.no_batched:
+    if rank == 0 and world == 1 and not args.no_batched and scheme == SCHEME:
         result["batched"] = run_batched(ctx)
-    if rank == 0 and world == 1 and not args.no_served:
+    if rank == 0 and world == 1 and not args.no_served and scheme == SCHEME:
         result["served"] = run_served(ctx, n_req=args.served_requests, rate=args.served_rate)
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and scheme == SCHEME:
         result["cpu_baseline"] = cpu_baseline_leg()
     return result
 
@@ -470,6 +497,7 @@ def main():
     ap.add_argument("--served-requests", type=int, default=400)
     ap.add_argument("--served-rate", type=float, default=300.0, help="Poisson arrival rate (requests/s)")
     ap.add_argument("--size", type=int, default=4096, help="grid side (the benchmark workload is 4096)")
+    ap.add_argument("--scheme", default=SCHEME, help="scheme of the single-simulation timing (default KP07_dimsplit)")
     args = ap.parse_args()
     global NX, NY
     NX = NY = args.size
