@@ -698,11 +698,18 @@ struct fv_batch {
     SimCtl* d_ctl = nullptr;              // device, one control block per slot
     SimCtl* h_ctl = nullptr;              // pinned host view
     int2* d_work = nullptr;
-    int2* h_work = nullptr;
+    int2* h_work[2] = {nullptr, nullptr};  // pinned staging, alternated between publishes
+    int* h_nwork[2] = {nullptr, nullptr};
+    cudaEvent_t ev_work[2] = {nullptr, nullptr};
+    int work_buf = 0;
     int work_cap = 0;
+    int nwork = 0;
     int* d_nwork = nullptr;
-    int* h_nwork = nullptr;
     int* d_err = nullptr;
+    cudaStream_t copy_stream = nullptr;  // uploads/downloads, concurrent with the kernels
+    cudaEvent_t ev_up = nullptr, ev_compute = nullptr;
+    std::vector<int> done_at_sync;        // slot finished as of the last fv_batch_sync
+    bool dirty = false;                   // work list changed since the last publish
     std::vector<int> used;               // slot in use
     std::vector<void*> slot_mem;          // per-slot device allocation (planes + tile scratch)
     std::vector<size_t> slot_bytes;
@@ -755,8 +762,10 @@ int batch_build_graph(fv_batch* b, int nsteps, cudaGraphExec_t* out) {
     return FV_OK;
 }
 
-// Rebuilds the work list from the slots in use and queues its upload.  The
-// caller has synchronised the stream (the pinned staging buffers are free).
+// Rebuilds the work list from the slots in use and queues its upload on the
+// compute stream, so the kernels enqueued before it still see the old list and
+// the ones after it the new one.  The two pinned staging buffers alternate;
+// a buffer is rewritten only after its previous copy has completed.
 int batch_publish(fv_batch* b) {
     int n = 0;
     for (int s = 0; s < b->max_inst; ++s)
@@ -764,24 +773,32 @@ int batch_publish(fv_batch* b) {
     if (n > b->work_cap) {
         int cap = b->work_cap;
         while (cap < n) cap *= 2;
-        if (b->d_work) cudaFreeAsync(b->d_work, b->stream);
-        if (b->h_work) cudaFreeHost(b->h_work);
+        FV_CK(cudaStreamSynchronize(b->stream));  // the old list may still be read by queued kernels
+        cudaFree(b->d_work);
         b->d_work = nullptr;
-        b->h_work = nullptr;
-        FV_CK(cudaMallocAsync(reinterpret_cast<void**>(&b->d_work), (size_t)cap * sizeof(int2), b->stream));
-        FV_CK(cudaMallocHost(reinterpret_cast<void**>(&b->h_work), (size_t)cap * sizeof(int2)));
+        for (int k = 0; k < 2; ++k) {
+            cudaFreeHost(b->h_work[k]);
+            b->h_work[k] = nullptr;
+        }
+        FV_CK(cudaMalloc(reinterpret_cast<void**>(&b->d_work), (size_t)cap * sizeof(int2)));
+        for (int k = 0; k < 2; ++k) FV_CK(cudaMallocHost(reinterpret_cast<void**>(&b->h_work[k]), (size_t)cap * sizeof(int2)));
         b->work_cap = cap;
         batch_drop_graphs(b);  // the graphs captured the old work-list pointer
     }
-    int k = 0;
+    const int k = b->work_buf ^ 1;
+    FV_CK(cudaEventSynchronize(b->ev_work[k]));
+    int i = 0;
     for (int s = 0; s < b->max_inst; ++s) {
         if (!b->used[s]) continue;
-        for (int t = 0; t < b->h_inst[s].ntiles; ++t) b->h_work[k++] = make_int2(s, t);
+        for (int t = 0; t < b->h_inst[s].ntiles; ++t) b->h_work[k][i++] = make_int2(s, t);
     }
-    *b->h_nwork = n;
-    if (n > 0) FV_CK(cudaMemcpyAsync(b->d_work, b->h_work, (size_t)n * sizeof(int2), cudaMemcpyHostToDevice, b->stream));
-    FV_CK(cudaMemcpyAsync(b->d_nwork, b->h_nwork, sizeof(int), cudaMemcpyHostToDevice, b->stream));
-    FV_CK(cudaStreamSynchronize(b->stream));
+    *b->h_nwork[k] = n;
+    if (n > 0)
+        FV_CK(cudaMemcpyAsync(b->d_work, b->h_work[k], (size_t)n * sizeof(int2), cudaMemcpyHostToDevice, b->stream));
+    FV_CK(cudaMemcpyAsync(b->d_nwork, b->h_nwork[k], sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    FV_CK(cudaEventRecord(b->ev_work[k], b->stream));
+    b->work_buf = k;
+    b->nwork = n;
     return FV_OK;
 }
 
@@ -828,21 +845,29 @@ int fv_batch_create(fv_context* ctx, int scheme, const fv_params* params, int ma
         return rc;
     };
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess)
+        cudaStreamCreateWithFlags(&b->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_up, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_compute, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_work[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_work[1], cudaEventDisableTiming) != cudaSuccess)
         return bail(fail(FV_ERR_CUDA, "stream/event creation failed"));
+    b->done_at_sync.assign(max_instances, 0);
     b->work_cap = 4096;
     if (cudaMalloc(&b->d_inst, (size_t)max_instances * sizeof(fv::BatchInstance)) != cudaSuccess ||
         cudaMallocHost(&b->h_inst, (size_t)max_instances * sizeof(fv::BatchInstance)) != cudaSuccess ||
         cudaMalloc(&b->d_ctl, (size_t)max_instances * sizeof(SimCtl)) != cudaSuccess ||
         cudaMallocHost(&b->h_ctl, (size_t)max_instances * sizeof(SimCtl)) != cudaSuccess ||
         cudaMalloc(&b->d_work, (size_t)b->work_cap * sizeof(int2)) != cudaSuccess ||
-        cudaMallocHost(&b->h_work, (size_t)b->work_cap * sizeof(int2)) != cudaSuccess ||
-        cudaMalloc(&b->d_nwork, sizeof(int)) != cudaSuccess || cudaMallocHost(&b->h_nwork, sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&b->d_err, sizeof(int)) != cudaSuccess)
+        cudaMallocHost(&b->h_work[0], (size_t)b->work_cap * sizeof(int2)) != cudaSuccess ||
+        cudaMallocHost(&b->h_work[1], (size_t)b->work_cap * sizeof(int2)) != cudaSuccess ||
+        cudaMalloc(&b->d_nwork, sizeof(int)) != cudaSuccess ||
+        cudaMallocHost(&b->h_nwork[0], sizeof(int)) != cudaSuccess ||
+        cudaMallocHost(&b->h_nwork[1], sizeof(int)) != cudaSuccess || cudaMalloc(&b->d_err, sizeof(int)) != cudaSuccess)
         return bail(fail(FV_ERR_NOMEM, "out of memory creating the batch"));
     memset(b->h_inst, 0, (size_t)max_instances * sizeof(fv::BatchInstance));
     memset(b->h_ctl, 0, (size_t)max_instances * sizeof(SimCtl));
-    *b->h_nwork = 0;
+    *b->h_nwork[0] = *b->h_nwork[1] = 0;
     if (cudaMemsetAsync(b->d_ctl, 0, (size_t)max_instances * sizeof(SimCtl), b->stream) != cudaSuccess ||
         cudaMemsetAsync(b->d_err, 0, sizeof(int), b->stream) != cudaSuccess ||
         cudaMemsetAsync(b->d_nwork, 0, sizeof(int), b->stream) != cudaSuccess ||
@@ -866,12 +891,21 @@ int fv_batch_destroy(fv_batch* b) {
     if (b->d_ctl) cudaFree(b->d_ctl);
     if (b->h_ctl) cudaFreeHost(b->h_ctl);
     if (b->d_work) cudaFree(b->d_work);
-    if (b->h_work) cudaFreeHost(b->h_work);
     if (b->d_nwork) cudaFree(b->d_nwork);
-    if (b->h_nwork) cudaFreeHost(b->h_nwork);
+    for (int k = 0; k < 2; ++k) {
+        if (b->h_work[k]) cudaFreeHost(b->h_work[k]);
+        if (b->h_nwork[k]) cudaFreeHost(b->h_nwork[k]);
+        if (b->ev_work[k]) cudaEventDestroy(b->ev_work[k]);
+    }
     if (b->d_err) cudaFree(b->d_err);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->ev_up) cudaEventDestroy(b->ev_up);
+    if (b->ev_compute) cudaEventDestroy(b->ev_compute);
+    if (b->copy_stream) {
+        cudaStreamSynchronize(b->copy_stream);
+        cudaStreamDestroy(b->copy_stream);
+    }
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return FV_OK;
@@ -897,7 +931,6 @@ int fv_batch_add(fv_batch* b, int nx, int ny, float dx, float dy, int bc, const 
             break;
         }
     if (s < 0) return fail(FV_ERR_NOMEM, "batch is full (%d simulations)", b->max_inst);
-    FV_CK(cudaStreamSynchronize(b->stream));  // staging buffers are free once the stream is idle
 
     const int W = b->be->W, H = b->be->H;
     const int pitch = ((nx + 8) + 31) / 32 * 32;
@@ -905,12 +938,14 @@ int fv_batch_add(fv_batch* b, int nx, int ny, float dx, float dy, int bc, const 
     const size_t plane = (size_t)(ny + 4) * pitch * sizeof(float);
     const size_t scratch = (size_t)ntiles * (sizeof(float) + 4 * sizeof(double));
     const size_t total = 2 * b->nv * plane + scratch + 256;
+    // The new simulation's memory is prepared on the copy stream, concurrently
+    // with kernels already queued for the other simulations.
     void* mem = nullptr;
-    if (cudaMallocAsync(&mem, total, b->stream) != cudaSuccess) {
+    if (cudaMallocAsync(&mem, total, b->copy_stream) != cudaSuccess) {
         cudaGetLastError();
         return fail(FV_ERR_NOMEM, "out of device memory for a %d x %d simulation", nx, ny);
     }
-    FV_CK(cudaMemsetAsync(mem, 0, total, b->stream));
+    FV_CK(cudaMemsetAsync(mem, 0, total, b->copy_stream));
     fv::BatchInstance& I = b->h_inst[s];
     memset(&I, 0, sizeof(I));
     char* base = static_cast<char*>(mem);
@@ -942,7 +977,7 @@ int fv_batch_add(fv_batch* b, int nx, int ny, float dx, float dy, int bc, const 
                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
             if (r != CUDA_SUCCESS) {
-                cudaFreeAsync(mem, b->stream);
+                cudaFreeAsync(mem, b->copy_stream);
                 return fail(FV_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
             }
         }
@@ -950,7 +985,9 @@ int fv_batch_add(fv_batch* b, int nx, int ny, float dx, float dy, int bc, const 
     for (int v = 0; v < b->nv; ++v)
         FV_CK(cudaMemcpy2DAsync(I.buf[0][v] + fv::cell_index(-off, -off, pitch), pitch * sizeof(float), host_vars[v],
                                 host_cols * sizeof(float), host_cols * sizeof(float), host_rows, cudaMemcpyHostToDevice,
-                                b->stream));
+                                b->copy_stream));
+    FV_CK(cudaEventRecord(b->ev_up, b->copy_stream));
+    FV_CK(cudaStreamWaitEvent(b->stream, b->ev_up, 0));  // later kernels see the uploaded state
     SimCtl& c = b->h_ctl[s];
     memset(&c, 0, sizeof(c));
     const float c2 = (b->scheme == FV_EE2D_KP07_DIMSPLIT) ? b->p.gamma : b->p.g;
@@ -961,13 +998,15 @@ int fv_batch_add(fv_batch* b, int nx, int ny, float dx, float dy, int bc, const 
     c.cfl_scale = b->p.cfl_scale;
     c.update_dt = 1;
     c.dt = (cfl0 * c.factor) * c.cfl_scale;  // simulate() computes dt at step 0
+    // From pinned staging (h_ctl, h_inst): asynchronous, ordered before the next kernels.
     FV_CK(cudaMemcpyAsync(b->d_ctl + s, &c, sizeof(SimCtl), cudaMemcpyHostToDevice, b->stream));
     FV_CK(cudaMemcpyAsync(b->d_inst + s, &I, sizeof(fv::BatchInstance), cudaMemcpyHostToDevice, b->stream));
     b->used[s] = 1;
+    b->done_at_sync[s] = 0;
     b->slot_mem[s] = mem;
     b->slot_bytes[s] = total;
     b->bytes += total;
-    FV_TRY(batch_publish(b));
+    b->dirty = true;  // joins the work list at the next fv_batch_run
     *slot = s;
     return FV_OK;
 }
@@ -975,9 +1014,9 @@ int fv_batch_add(fv_batch* b, int nx, int ny, float dx, float dy, int bc, const 
 int fv_batch_remove(fv_batch* b, int slot) {
     FV_TRY(check_batch(b));
     if (slot < 0 || slot >= b->max_inst || !b->used[slot]) return fail(FV_ERR_INVALID, "slot %d is not in use", slot);
-    FV_CK(cudaStreamSynchronize(b->stream));
     b->used[slot] = 0;
-    FV_TRY(batch_publish(b));
+    b->dirty = true;  // leaves the work list at the next fv_batch_run
+    // Freed in stream order, after every kernel already queued that may read it.
     FV_CK(cudaFreeAsync(b->slot_mem[slot], b->stream));
     b->slot_mem[slot] = nullptr;
     b->bytes -= b->slot_bytes[slot];
@@ -988,6 +1027,10 @@ int fv_batch_remove(fv_batch* b, int slot) {
 int fv_batch_run(fv_batch* b, int n_steps) {
     FV_TRY(check_batch(b));
     if (n_steps < 0) return fail(FV_ERR_INVALID, "negative step count");
+    if (b->dirty) {
+        FV_TRY(batch_publish(b));
+        b->dirty = false;
+    }
     if (!b->graph1) FV_TRY(batch_build_graph(b, 1, &b->graph1));
     if (!b->graph16) FV_TRY(batch_build_graph(b, 16, &b->graph16));
     FV_CK(cudaEventRecord(b->ev0, b->stream));
@@ -1009,9 +1052,15 @@ int fv_batch_sync(fv_batch* b) {
     FV_CK(cudaMemcpyAsync(b->h_ctl, b->d_ctl, (size_t)b->max_inst * sizeof(SimCtl), cudaMemcpyDeviceToHost,
                           b->stream));
     int err = 0;
-    FV_CK(cudaMemcpyAsync(b->h_nwork, b->d_nwork, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
     FV_CK(cudaStreamSynchronize(b->stream));
     FV_CK(cudaMemcpy(&err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    for (int s = 0; s < b->max_inst; ++s) {
+        if (!b->used[s]) continue;
+        const SimCtl& c = b->h_ctl[s];
+        const double rem = c.t_end - c.t;
+        const float cur = (float)((rem < (double)c.dt) ? rem : (double)c.dt);
+        b->done_at_sync[s] = (!(c.t < c.t_end) || cur <= 0.0f) ? 1 : 0;
+    }
     float ms = 0.0f;
     if (cudaEventElapsedTime(&ms, b->ev0, b->ev1) == cudaSuccess) b->last_ms = ms;
     cudaGetLastError();
@@ -1039,11 +1088,19 @@ int fv_batch_download(fv_batch* b, int slot, int var, float* host, int host_pitc
         return fail(FV_ERR_INVALID, "bad download argument");
     const fv::BatchInstance& I = b->h_inst[slot];
     if (host_pitch < I.nx) return fail(FV_ERR_INVALID, "host pitch too small");
+    if (!b->done_at_sync[slot]) {
+        // still running at the last sync: include every kernel queued since
+        FV_CK(cudaStreamSynchronize(b->stream));
+        FV_CK(cudaMemcpyAsync(b->h_ctl + slot, b->d_ctl + slot, sizeof(SimCtl), cudaMemcpyDeviceToHost, b->stream));
+        FV_CK(cudaStreamSynchronize(b->stream));
+    }
+    // A simulation that had reached t_end at the last sync is skipped by the
+    // kernels queued since, so its state can be read while they run.
     const int cur = b->h_ctl[slot].cur;
     FV_CK(cudaMemcpy2DAsync(host, (size_t)host_pitch * sizeof(float), I.buf[cur][var] + fv::cell_index(0, 0, I.pitch),
                             (size_t)I.pitch * sizeof(float), (size_t)I.nx * sizeof(float), I.ny, cudaMemcpyDeviceToHost,
-                            b->stream));
-    FV_CK(cudaStreamSynchronize(b->stream));
+                            b->copy_stream));
+    FV_CK(cudaStreamSynchronize(b->copy_stream));
     return FV_OK;
 }
 
@@ -1055,7 +1112,7 @@ int fv_batch_info(fv_batch* b, size_t* device_bytes, int* active, int* work_item
         for (int s = 0; s < b->max_inst; ++s) n += b->used[s];
         *active = n;
     }
-    if (work_items) *work_items = *b->h_nwork;
+    if (work_items) *work_items = b->nwork;
     if (last_run_ms) *last_run_ms = b->last_ms;
     return FV_OK;
 }

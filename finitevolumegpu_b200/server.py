@@ -83,15 +83,37 @@ class Server(object):
         self.used = 0.0
 
     def serve(self, requests: List[Request], clock=time.perf_counter):
+        """Serve `requests` (arrival times relative to the call) until all are done.
+
+        Each iteration first queues the next chunk of steps for every batch
+        with running scenarios, then, while the GPU works, admits arrived
+        requests (their uploads run on a copy stream and they join the chunk
+        after) and downloads the scenarios that had finished at the previous
+        synchronisation (their state is final, so it is read while the chunk
+        runs); finally it waits for the chunk and looks for newly finished
+        scenarios.
+        """
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         running = {}  # (scheme, slot) -> (request, admitted, bytes)
+        finished = []  # keys that had reached t_end at the last synchronisation
         results: List[Result] = []
         t0 = clock()
         busy_since = None
         cells = 0
+        timers = collections.Counter()
         while pending or running:
-            now = clock() - t0
-            # admission: arrived requests, in arrival order, while the budget allows
+            # 1. queue the next chunk
+            done_set = set(finished)
+            active = {s for key in running if key not in done_set for s in (key[0],)}
+            ta = clock()
+            for s in active:
+                self.batches[s].run(self.chunk)
+            timers["queue"] += clock() - ta
+            if active and busy_since is None:
+                busy_since = ta - t0
+            # 2. admit arrived requests while the budget allows
+            ta = clock()
+            now = ta - t0
             while pending and pending[0].arrival <= now:
                 r = pending[0]
                 need = state_bytes(r.scheme, r.nx, r.ny)
@@ -105,34 +127,32 @@ class Server(object):
                 pending.popleft()
                 self.used += need
                 running[(r.scheme, slot)] = (r, clock() - t0, need)
-            if not running:
-                if pending:
-                    wait = pending[0].arrival - (clock() - t0)
-                    if wait > 0:
-                        time.sleep(min(wait, 0.01))
-                continue
-            if busy_since is None:
-                busy_since = clock() - t0
-            active = {s for (s, _) in running}
-            for s in active:
-                self.batches[s].run(self.chunk)
+            timers["admit"] += clock() - ta
+            # 3. return the scenarios that finished at the last synchronisation
+            ta = clock()
+            for key in finished:
+                s, slot = key
+                r, admitted, need = running.pop(key)
+                st = self.batches[s].status(slot)
+                state = self.batches[s].download(slot)
+                self.batches[s].remove(slot)
+                self.used -= need
+                results.append(Result(r.rid, s, state, st["nt"], st["t"], r.arrival, admitted, clock() - t0))
+                cells += r.nx * r.ny * st["nt"]
+            finished = []
+            timers["return"] += clock() - ta
+            # 4. wait for the chunk and find the scenarios that are done
+            ta = clock()
             for s in active:
                 self.batches[s].sync()
-            done = []
-            for key, (r, admitted, need) in running.items():
-                s, slot = key
-                st = self.batches[s].status(slot)
-                if st["done"]:
-                    state = self.batches[s].download(slot)
-                    fin = clock() - t0
-                    results.append(Result(r.rid, s, state, st["nt"], st["t"], r.arrival, admitted, fin))
-                    cells += r.nx * r.ny * st["nt"]
-                    done.append(key)
-            for key in done:
-                s, slot = key
-                self.batches[s].remove(slot)
-                self.used -= running[key][2]
-                del running[key]
+            for key in running:
+                if key[0] in active and self.batches[key[0]].status(key[1])["done"]:
+                    finished.append(key)
+            timers["wait"] += clock() - ta
+            if not active and not finished and pending and not running:
+                wait = pending[0].arrival - (clock() - t0)
+                if wait > 0:
+                    time.sleep(min(wait, 0.005))
         elapsed = clock() - t0
         lat = np.array([r.latency for r in results]) if results else np.zeros(1)
         stats = {
@@ -143,5 +163,6 @@ class Server(object):
             "p50_latency_s": float(np.percentile(lat, 50)),
             "p99_latency_s": float(np.percentile(lat, 99)),
             "mean_latency_s": float(lat.mean()),
+            "host_seconds": {k: round(v, 4) for k, v in timers.items()},
         }
         return results, stats
