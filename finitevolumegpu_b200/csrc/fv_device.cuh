@@ -84,20 +84,51 @@ __device__ __forceinline__ void prefetch_tmap(const void* tmap) {
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(tmap)) : "memory");
 }
 
+// ------------------------------------------------------------------ explicit FP32 operations
+
+// Round-to-nearest FP32 add/sub/mul/fma (flush to zero, as in fast-math code)
+// written as PTX, so each one is exactly the operation the formula states:
+// the compiler can neither contract nor rewrite them (fast-math code may turn
+// x * (1/y) into x / y, for instance, which costs more reciprocals).  Division
+// and square root stay C operators (fast-math approximations).
+__device__ __forceinline__ float fadd(float a, float b) {
+    float d;
+    asm("add.rn.ftz.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+    return d;
+}
+__device__ __forceinline__ float fsub(float a, float b) {
+    float d;
+    asm("sub.rn.ftz.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+    return d;
+}
+__device__ __forceinline__ float fmul(float a, float b) {
+    float d;
+    asm("mul.rn.ftz.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+    return d;
+}
+__device__ __forceinline__ float ffma(float a, float b, float c) {
+    float d;
+    asm("fma.rn.ftz.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+
 // ------------------------------------------------------------------ limiters
 
 // Generalised minmod slope (GPUSimulators/cuda/limiters.h:31-41).  The
 // reference's sign product 0.25*s(b)*(s(b)+s(c))*(s(c)+s(f)) is +-1 when the
 // three differences share a sign and 0 otherwise, so the slope is the smallest
 // magnitude with b's sign, or zero.
-__device__ __forceinline__ float minmod_slope(float left, float center, float right, float theta) {
-    const float b = (center - left) * theta;
-    const float c = (right - left) * 0.5f;
-    const float f = (right - center) * theta;
+// minmod3 takes the scaled differences b = theta*(center - left),
+// c = (right - left)/2 and f = theta*(right - center).
+__device__ __forceinline__ float minmod3(float b, float c, float f) {
     const float mag = fminf(fminf(fabsf(b), fabsf(c)), fabsf(f));
     const uint32_t sb = __float_as_uint(b), sc = __float_as_uint(c), sf = __float_as_uint(f);
     const bool same = (((sb ^ sc) | (sc ^ sf)) & 0x80000000u) == 0u;
     return same ? copysignf(mag, b) : 0.0f;
+}
+
+__device__ __forceinline__ float minmod_slope(float left, float center, float right, float theta) {
+    return minmod3(fmul(fsub(center, left), theta), fmul(fsub(right, left), 0.5f), fmul(fsub(right, center), theta));
 }
 
 // GPUSimulators/cuda/limiters.h:100-102
@@ -126,34 +157,35 @@ __device__ __forceinline__ SweFace swe_face(float h, float hu, float hv, float g
     s.q[1] = hu;
     s.q[2] = hv;
     const float rh = 1.0f / h;
-    s.u = hu * rh;
+    s.u = fmul(hu, rh);
     s.f[0] = hu;
-    s.f[1] = fmaf(hu, s.u, half_g * h * h);
-    s.f[2] = hv * s.u;
-    s.c = sqrtf(g * h);
+    s.f[1] = ffma(hu, s.u, fmul(fmul(half_g, h), h));
+    s.f[2] = fmul(hv, s.u);
+    s.c = sqrtf(fmul(g, h));
     return s;
 }
 
 // Central-upwind flux (GPUSimulators/cuda/SWECommon.h:228-241); m is the left
 // (minus) state, p the right (plus) state.
 __device__ __forceinline__ void swe_central_upwind(const SweFace& m, const SweFace& p, float out[3]) {
-    const float am = fminf(fminf(m.u - m.c, p.u - p.c), 0.0f);
-    const float ap = fmaxf(fmaxf(m.u + m.c, p.u + p.c), 0.0f);
-    const float inv = 1.0f / (ap - am);
-    const float apam = ap * am;
+    const float am = fminf(fminf(fsub(m.u, m.c), fsub(p.u, p.c)), 0.0f);
+    const float ap = fmaxf(fmaxf(fadd(m.u, m.c), fadd(p.u, p.c)), 0.0f);
+    const float inv = 1.0f / fsub(ap, am);
+    const float apam = fmul(ap, am);
 #pragma unroll
-    for (int v = 0; v < 3; ++v) out[v] = fmaf(apam, p.q[v] - m.q[v], fmaf(ap, m.f[v], -am * p.f[v])) * inv;
+    for (int v = 0; v < 3; ++v)
+        out[v] = fmul(ffma(apam, fsub(p.q[v], m.q[v]), ffma(ap, m.f[v], fmul(-am, p.f[v]))), inv);
 }
 
 // HLL flux (GPUSimulators/cuda/SWECommon.h:274-313).
 __device__ __forceinline__ void swe_hll(const SweFace& l, const SweFace& r, float out[3]) {
     const float h_l = l.q[0], h_r = r.q[0];
-    const float hsum = h_l + h_r;
-    const float h_dag = 0.5f * hsum - 0.25f * (r.u - l.u) * hsum / (l.c + r.c);
-    const float q_l = (h_dag > h_l) ? sqrtf(0.5f * ((h_dag + h_l) * h_dag / (h_l * h_l))) : 1.0f;
-    const float q_r = (h_dag > h_r) ? sqrtf(0.5f * ((h_dag + h_r) * h_dag / (h_r * h_r))) : 1.0f;
-    const float S_l = fmaf(-l.c, q_l, l.u);
-    const float S_r = fmaf(r.c, q_r, r.u);
+    const float hsum = fadd(h_l, h_r);
+    const float h_dag = fsub(fmul(0.5f, hsum), fmul(fmul(0.25f, fsub(r.u, l.u)), hsum) / fadd(l.c, r.c));
+    const float q_l = (h_dag > h_l) ? sqrtf(fmul(0.5f, fmul(fadd(h_dag, h_l), h_dag) / fmul(h_l, h_l))) : 1.0f;
+    const float q_r = (h_dag > h_r) ? sqrtf(fmul(0.5f, fmul(fadd(h_dag, h_r), h_dag) / fmul(h_r, h_r))) : 1.0f;
+    const float S_l = ffma(-l.c, q_l, l.u);
+    const float S_r = ffma(r.c, q_r, r.u);
     if (S_l >= 0.0f) {
 #pragma unroll
         for (int v = 0; v < 3; ++v) out[v] = l.f[v];
@@ -161,10 +193,11 @@ __device__ __forceinline__ void swe_hll(const SweFace& l, const SweFace& r, floa
 #pragma unroll
         for (int v = 0; v < 3; ++v) out[v] = r.f[v];
     } else {
-        const float inv = 1.0f / (S_r - S_l);
-        const float srsl = S_r * S_l;
+        const float inv = 1.0f / fsub(S_r, S_l);
+        const float srsl = fmul(S_r, S_l);
 #pragma unroll
-        for (int v = 0; v < 3; ++v) out[v] = fmaf(srsl, r.q[v] - l.q[v], fmaf(S_r, l.f[v], -S_l * r.f[v])) * inv;
+        for (int v = 0; v < 3; ++v)
+            out[v] = fmul(ffma(srsl, fsub(r.q[v], l.q[v]), ffma(S_r, l.f[v], fmul(-S_l, r.f[v]))), inv);
     }
 }
 
@@ -173,24 +206,29 @@ __device__ __forceinline__ void swe_hll(const SweFace& l, const SweFace& r, floa
 // minmod slope, face values Q -+ slope/2, and the half-step predictor
 // Q_face + dt/(2dx) * (F(Q_west) - F(Q_east)), which is the same flux
 // difference for both faces of the cell.  w/e: predicted west/east face states.
-__device__ __forceinline__ void swe_muscl_hancock(const float qm[3], const float q0[3], const float qp[3],
-                                                  float theta, float g, float half_g, float k2, SweFace& w,
-                                                  SweFace& e) {
+// bd holds theta*(q0 - qm) on entry and theta*(qp - q0) on return: a cell's
+// forward difference is the backward difference of the next one, so a line
+// walker computes each difference once.
+__device__ __forceinline__ void swe_muscl_hancock(const float (&qm)[3], const float (&q0)[3], const float (&qp)[3],
+                                                  float (&bd)[3], float theta, float g, float half_g, float k2,
+                                                  SweFace& w, SweFace& e) {
     float W[3], E[3];
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
-        const float s = minmod_slope(qm[v], q0[v], qp[v], theta);
-        W[v] = fmaf(-0.5f, s, q0[v]);
-        E[v] = fmaf(0.5f, s, q0[v]);
+        const float f = fmul(fsub(qp[v], q0[v]), theta);
+        const float s = minmod3(bd[v], fmul(fsub(qp[v], qm[v]), 0.5f), f);
+        bd[v] = f;
+        W[v] = ffma(-0.5f, s, q0[v]);
+        E[v] = ffma(0.5f, s, q0[v]);
     }
     const float uw = W[1] / W[0];
     const float ue = E[1] / E[0];
     float D[3];
-    D[0] = W[1] - E[1];
-    D[1] = fmaf(W[1], uw, half_g * W[0] * W[0]) - fmaf(E[1], ue, half_g * E[0] * E[0]);
-    D[2] = fmaf(W[2], uw, -E[2] * ue);
-    w = swe_face(fmaf(k2, D[0], W[0]), fmaf(k2, D[1], W[1]), fmaf(k2, D[2], W[2]), g, half_g);
-    e = swe_face(fmaf(k2, D[0], E[0]), fmaf(k2, D[1], E[1]), fmaf(k2, D[2], E[2]), g, half_g);
+    D[0] = fsub(W[1], E[1]);
+    D[1] = fsub(ffma(W[1], uw, fmul(fmul(half_g, W[0]), W[0])), ffma(E[1], ue, fmul(fmul(half_g, E[0]), E[0])));
+    D[2] = ffma(W[2], uw, fmul(-E[2], ue));
+    w = swe_face(ffma(k2, D[0], W[0]), ffma(k2, D[1], W[1]), ffma(k2, D[2], W[2]), g, half_g);
+    e = swe_face(ffma(k2, D[0], E[0]), ffma(k2, D[1], E[1]), ffma(k2, D[2], E[2]), g, half_g);
 }
 
 // ------------------------------------------------------------------ Euler
@@ -210,35 +248,36 @@ __device__ __forceinline__ EulerFace euler_face(float rho, float ru, float rv, f
     s.q[2] = rv;
     s.q[3] = E;
     const float rr = 1.0f / rho;
-    const float P = (gamma - 1.0f) * fmaf(-0.5f * fmaf(ru, ru, rv * rv), rr, E);
-    s.u = ru * rr;
+    const float P = fmul(gamma - 1.0f, ffma(fmul(-0.5f, ffma(ru, ru, fmul(rv, rv))), rr, E));
+    s.u = fmul(ru, rr);
     s.f[0] = ru;
-    s.f[1] = fmaf(ru, s.u, P);
-    s.f[2] = rv * s.u;
-    s.f[3] = s.u * (E + P);
-    s.c = sqrtf(gamma * P * rr);
+    s.f[1] = ffma(ru, s.u, P);
+    s.f[2] = fmul(rv, s.u);
+    s.f[3] = fmul(s.u, fadd(E, P));
+    s.c = sqrtf(fmul(fmul(gamma, P), rr));
     return s;
 }
 
 // GPUSimulators/cuda/EulerCommon.h:171-187
 __device__ __forceinline__ void euler_central_upwind(const EulerFace& m, const EulerFace& p, float out[4]) {
-    const float am = fminf(fminf(m.u - m.c, p.u - p.c), 0.0f);
-    const float ap = fmaxf(fmaxf(m.u + m.c, p.u + p.c), 0.0f);
-    const float inv = 1.0f / (ap - am);
-    const float apam = ap * am;
+    const float am = fminf(fminf(fsub(m.u, m.c), fsub(p.u, p.c)), 0.0f);
+    const float ap = fmaxf(fmaxf(fadd(m.u, m.c), fadd(p.u, p.c)), 0.0f);
+    const float inv = 1.0f / fsub(ap, am);
+    const float apam = fmul(ap, am);
 #pragma unroll
-    for (int v = 0; v < 4; ++v) out[v] = fmaf(apam, p.q[v] - m.q[v], fmaf(ap, m.f[v], -am * p.f[v])) * inv;
+    for (int v = 0; v < 4; ++v)
+        out[v] = fmul(ffma(apam, fsub(p.q[v], m.q[v]), ffma(ap, m.f[v], fmul(-am, p.f[v]))), inv);
 }
 
 // GPUSimulators/cuda/EulerCommon.h:117-160
 __device__ __forceinline__ void euler_hll(const EulerFace& l, const EulerFace& r, float out[4]) {
     const float h_l = l.q[0], h_r = r.q[0];
-    const float hsum = h_l + h_r;
-    const float h_dag = 0.5f * hsum - 0.25f * (r.u - l.u) * hsum / (l.c + r.c);
-    const float q_l = (h_dag > h_l) ? sqrtf(0.5f * ((h_dag + h_l) * h_dag / (h_l * h_l))) : 1.0f;
-    const float q_r = (h_dag > h_r) ? sqrtf(0.5f * ((h_dag + h_r) * h_dag / (h_r * h_r))) : 1.0f;
-    const float S_l = fmaf(-l.c, q_l, l.u);
-    const float S_r = fmaf(r.c, q_r, r.u);
+    const float hsum = fadd(h_l, h_r);
+    const float h_dag = fsub(fmul(0.5f, hsum), fmul(fmul(0.25f, fsub(r.u, l.u)), hsum) / fadd(l.c, r.c));
+    const float q_l = (h_dag > h_l) ? sqrtf(fmul(0.5f, fmul(fadd(h_dag, h_l), h_dag) / fmul(h_l, h_l))) : 1.0f;
+    const float q_r = (h_dag > h_r) ? sqrtf(fmul(0.5f, fmul(fadd(h_dag, h_r), h_dag) / fmul(h_r, h_r))) : 1.0f;
+    const float S_l = ffma(-l.c, q_l, l.u);
+    const float S_r = ffma(r.c, q_r, r.u);
     if (S_l >= 0.0f) {
 #pragma unroll
         for (int v = 0; v < 4; ++v) out[v] = l.f[v];
@@ -246,10 +285,11 @@ __device__ __forceinline__ void euler_hll(const EulerFace& l, const EulerFace& r
 #pragma unroll
         for (int v = 0; v < 4; ++v) out[v] = r.f[v];
     } else {
-        const float inv = 1.0f / (S_r - S_l);
-        const float srsl = S_r * S_l;
+        const float inv = 1.0f / fsub(S_r, S_l);
+        const float srsl = fmul(S_r, S_l);
 #pragma unroll
-        for (int v = 0; v < 4; ++v) out[v] = fmaf(srsl, r.q[v] - l.q[v], fmaf(S_r, l.f[v], -S_l * r.f[v])) * inv;
+        for (int v = 0; v < 4; ++v)
+            out[v] = fmul(ffma(srsl, fsub(r.q[v], l.q[v]), ffma(S_r, l.f[v], fmul(-S_l, r.f[v]))), inv);
     }
 }
 
@@ -257,25 +297,28 @@ __device__ __forceinline__ void euler_hll(const EulerFace& l, const EulerFace& r
 // (GPUSimulators/cuda/EE2D_KP07_dimsplit.cu:33-58 and :78-103).  The reference's
 // predictor calls F_func(Q, gamma_), whose second argument is the pressure, so
 // the predictor flux uses gamma in place of P; that is reproduced here.
-__device__ __forceinline__ void euler_muscl_hancock(const float qm[4], const float q0[4], const float qp[4],
-                                                    float theta, float gamma, float k2, EulerFace& w,
+// bd: theta*(q0 - qm) on entry, theta*(qp - q0) on return (as in swe_muscl_hancock).
+__device__ __forceinline__ void euler_muscl_hancock(const float (&qm)[4], const float (&q0)[4], const float (&qp)[4],
+                                                    float (&bd)[4], float theta, float gamma, float k2, EulerFace& w,
                                                     EulerFace& e) {
     float W[4], E[4];
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-        const float s = minmod_slope(qm[v], q0[v], qp[v], theta);
-        W[v] = fmaf(-0.5f, s, q0[v]);
-        E[v] = fmaf(0.5f, s, q0[v]);
+        const float f = fmul(fsub(qp[v], q0[v]), theta);
+        const float s = minmod3(bd[v], fmul(fsub(qp[v], qm[v]), 0.5f), f);
+        bd[v] = f;
+        W[v] = ffma(-0.5f, s, q0[v]);
+        E[v] = ffma(0.5f, s, q0[v]);
     }
     const float uw = W[1] / W[0];
     const float ue = E[1] / E[0];
     float D[4];
-    D[0] = W[1] - E[1];
-    D[1] = fmaf(W[1], uw, gamma) - fmaf(E[1], ue, gamma);
-    D[2] = fmaf(W[2], uw, -E[2] * ue);
-    D[3] = fmaf(uw, W[3] + gamma, -ue * (E[3] + gamma));
-    w = euler_face(fmaf(k2, D[0], W[0]), fmaf(k2, D[1], W[1]), fmaf(k2, D[2], W[2]), fmaf(k2, D[3], W[3]), gamma);
-    e = euler_face(fmaf(k2, D[0], E[0]), fmaf(k2, D[1], E[1]), fmaf(k2, D[2], E[2]), fmaf(k2, D[3], E[3]), gamma);
+    D[0] = fsub(W[1], E[1]);
+    D[1] = fsub(ffma(W[1], uw, gamma), ffma(E[1], ue, gamma));
+    D[2] = ffma(W[2], uw, fmul(-E[2], ue));
+    D[3] = ffma(uw, fadd(W[3], gamma), fmul(-ue, fadd(E[3], gamma)));
+    w = euler_face(ffma(k2, D[0], W[0]), ffma(k2, D[1], W[1]), ffma(k2, D[2], W[2]), ffma(k2, D[3], W[3]), gamma);
+    e = euler_face(ffma(k2, D[0], E[0]), ffma(k2, D[1], E[1]), ffma(k2, D[2], E[2]), ffma(k2, D[3], E[3]), gamma);
 }
 
 // ------------------------------------------------------------------ WAF

@@ -371,9 +371,9 @@ struct SwePhys {
     static constexpr int NV = 3;
     using Face = SweFace;
     float theta, g, half_g, k2;
-    __device__ __forceinline__ void recon(const float (&qm)[3], const float (&q0)[3], const float (&qp)[3], Face& w,
-                                          Face& e) const {
-        swe_muscl_hancock(qm, q0, qp, theta, g, half_g, k2, w, e);
+    __device__ __forceinline__ void recon(const float (&qm)[3], const float (&q0)[3], const float (&qp)[3],
+                                          float (&bd)[3], Face& w, Face& e) const {
+        swe_muscl_hancock(qm, q0, qp, bd, theta, g, half_g, k2, w, e);
     }
     template <bool HLLF> __device__ __forceinline__ static void flux(const Face& l, const Face& r, float (&F)[3]) {
         if (HLLF) swe_hll(l, r, F);
@@ -385,9 +385,9 @@ struct EulerPhys {
     static constexpr int NV = 4;
     using Face = EulerFace;
     float theta, gamma, k2;
-    __device__ __forceinline__ void recon(const float (&qm)[4], const float (&q0)[4], const float (&qp)[4], Face& w,
-                                          Face& e) const {
-        euler_muscl_hancock(qm, q0, qp, theta, gamma, k2, w, e);
+    __device__ __forceinline__ void recon(const float (&qm)[4], const float (&q0)[4], const float (&qp)[4],
+                                          float (&bd)[4], Face& w, Face& e) const {
+        euler_muscl_hancock(qm, q0, qp, bd, theta, gamma, k2, w, e);
     }
     template <bool HLLF> __device__ __forceinline__ static void flux(const Face& l, const Face& r, float (&F)[4]) {
         if (HLLF) euler_hll(l, r, F);
@@ -399,7 +399,7 @@ struct EulerPhys {
 // flux at c-1/2, update cell c-1 (GPUSimulators/cuda/common.h:444-475).
 template <class Phys, bool HLLF, bool SWAP, int PS>
 __device__ __forceinline__ void mh_step(float* line, int step, int c, float (&qm)[Phys::NV], float (&q0)[Phys::NV],
-                                        float (&qp)[Phys::NV], const float (&qn)[Phys::NV],
+                                        float (&qp)[Phys::NV], const float (&qn)[Phys::NV], float (&bd)[Phys::NV],
                                         typename Phys::Face& eL, float (&Fprev)[Phys::NV], const Phys& P,
                                         float kdx, bool update) {
     constexpr int NV = Phys::NV;
@@ -410,13 +410,13 @@ __device__ __forceinline__ void mh_step(float* line, int step, int c, float (&qm
         qp[v] = qn[v];
     }
     typename Phys::Face w, e;
-    P.recon(qm, q0, qp, w, e);
+    P.recon(qm, q0, qp, bd, w, e);
     float F[NV];
     Phys::template flux<HLLF>(eL, w, F);
     if (update) {
         float out[NV];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) out[v] = fmaf(Fprev[v] - F[v], kdx, qm[v]);
+        for (int v = 0; v < NV; ++v) out[v] = ffma(fsub(Fprev[v], F[v]), kdx, qm[v]);
         st_cell<NV, SWAP, PS>(line, c - 1, step, out);
     }
 #pragma unroll
@@ -429,7 +429,7 @@ template <class Phys, bool HLLF, bool SWAP, int PS>
 __device__ __forceinline__ void walk_mh(float* line, int step, int a, int b, const float (&pre)[4][Phys::NV],
                                         const Phys& P, float kdx) {
     constexpr int NV = Phys::NV;
-    float qm[NV], q0[NV], qp[NV], qn[NV], Fprev[NV];
+    float qm[NV], q0[NV], qp[NV], qn[NV], Fprev[NV], bd[NV];
     typename Phys::Face eL;
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
@@ -445,19 +445,20 @@ __device__ __forceinline__ void walk_mh(float* line, int step, int a, int b, con
             qm[v] = q0[v];
             q0[v] = qp[v];
             qp[v] = qn[v];
+            bd[v] = fmul(fsub(q0[v], qm[v]), P.theta);
         }
         typename Phys::Face w;
-        P.recon(qm, q0, qp, w, eL);
+        P.recon(qm, q0, qp, bd, w, eL);
     }
     // c = a: first face, no update
     ld_cell<NV, SWAP, PS>(line, a + 1, step, qn);
-    mh_step<Phys, HLLF, SWAP, PS>(line, step, a, qm, q0, qp, qn, eL, Fprev, P, kdx, false);
+    mh_step<Phys, HLLF, SWAP, PS>(line, step, a, qm, q0, qp, qn, bd, eL, Fprev, P, kdx, false);
     for (int c = a + 1; c < b - 1; ++c) {
         ld_cell<NV, SWAP, PS>(line, c + 1, step, qn);
-        mh_step<Phys, HLLF, SWAP, PS>(line, step, c, qm, q0, qp, qn, eL, Fprev, P, kdx, true);
+        mh_step<Phys, HLLF, SWAP, PS>(line, step, c, qm, q0, qp, qn, bd, eL, Fprev, P, kdx, true);
     }
-    mh_step<Phys, HLLF, SWAP, PS>(line, step, b - 1, qm, q0, qp, pre[2], eL, Fprev, P, kdx, true);
-    mh_step<Phys, HLLF, SWAP, PS>(line, step, b, qm, q0, qp, pre[3], eL, Fprev, P, kdx, true);
+    mh_step<Phys, HLLF, SWAP, PS>(line, step, b - 1, qm, q0, qp, pre[2], bd, eL, Fprev, P, kdx, true);
+    mh_step<Phys, HLLF, SWAP, PS>(line, step, b, qm, q0, qp, pre[3], bd, eL, Fprev, P, kdx, true);
 }
 
 // Two-point flux walker (FORCE, HLL: GPUSimulators/cuda/SWE2D_FORCE.cu:29-81,
