@@ -35,10 +35,23 @@ NX = NY = 4096  # may be overridden by --size (profiling captures use a smaller 
 SCHEME = "KP07_dimsplit"
 BYTES_PER_CELL_SUBSTEP = 24  # 3 FP32 variables read + written per stage launch
 SUBSTEPS = 2
-# FP32 operations per cell-substep of the algorithm (count of the restated
-# formulas for KP07_dimsplit: reconstruction, predictor, central-upwind flux and
-# update along both axes; see profiles/kp07_dimsplit_flops.md).
-ALG_FLOP_PER_CELL_SUBSTEP = None
+# Algorithmic floating-point operations per cell and stage launch (averaged
+# over the launches of a step) of each scheme as the reference formulates it:
+# +, -, *, /, sqrt, min, max counted once each ("flops"), of which divisions and
+# square roots ("mufu").  Counted by running the CPU restatement with an
+# operation-counting number type (oracle.oracle.ops_per_cell_substep);
+# tests/test_flop_count.py checks these figures against that count.
+ALG_OPS_PER_CELL_LAUNCH = {
+    "LxF": {"flops": 123.0, "mufu": 21.0},
+    "FORCE": {"flops": 184.0, "mufu": 30.0},
+    "HLL": {"flops": 164.0, "mufu": 38.0},
+    "HLL2": {"flops": 484.0, "mufu": 56.0},
+    "WAF": {"flops": 506.0, "mufu": 88.0},
+    "KP07": {"flops": 474.0, "mufu": 39.0},
+    "KP07_dimsplit": {"flops": 450.0, "mufu": 46.0},
+    "EE2D_KP07_dimsplit": {"flops": 585.0, "mufu": 51.0},
+}
+FP32_LANES_PER_SM = 128  # FP32 FMA lanes per Blackwell SM
 PROFILE_JSON = os.path.join(ROOT, "profiles", "kp07_dimsplit_stage_4096.json")
 
 
@@ -417,12 +430,26 @@ def run_mine(args, rank, world, local_rank):
             "kernel": "%s stage kernel, tile %dx%d, %d threads" % (scheme, info["tile_w"], info["tile_h"],
                                                                     info["threads"]),
             "algorithmic_bytes_per_launch": alg_bytes}
-    if prof.get("fp32_flop_per_launch"):
-        clk = clocks.summary().get("sm_mhz") or 1965.0
-        fp32_peak = 148 * 128 * 2 * clk * 1e6 / 1e12
-        ach = prof["fp32_flop_per_launch"] / launch_s / 1e12
-        roof["fp32"] = {"achieved_tflops": ach, "peak_tflops_at_clock": fp32_peak, "frac": ach / fp32_peak,
-                        "note": "executed FP32 ops per launch from ncu; peak = 148 SM x 128 lanes x 2 x SM clock"}
+    # FP32 roofline: algorithmic operations of the reference formulation per
+    # launch against the nominal FP32 peak (an FMA is 2 operations); the
+    # binding roofline is the one with the longer lower-bound time.
+    props = torch.cuda.get_device_properties(local_rank)
+    sm_max_mhz = float(pk.get("sm_max_mhz") or 1965.0)
+    fp32_peak = props.multi_processor_count * FP32_LANES_PER_SM * 2 * sm_max_mhz * 1e6 / 1e12
+    ops = ALG_OPS_PER_CELL_LAUNCH[scheme]
+    alg_flop = ops["flops"] * cells
+    ach_tf = alg_flop / launch_s / 1e12
+    roof_fp32 = {"bound": "fp32", "achieved": ach_tf, "peak": fp32_peak, "unit": "TFLOP/s", "frac": ach_tf / fp32_peak,
+                 "peak_kind": "nominal: %d SMs x %d FP32 lanes x 2 x %.0f MHz" % (
+                     props.multi_processor_count, FP32_LANES_PER_SM, sm_max_mhz),
+                 "algorithmic_flop_per_launch": alg_flop, "flop_per_cell_launch": ops["flops"],
+                 "mufu_per_cell_launch": ops["mufu"]}
+    if prof.get("executed_inst_per_cell_substep"):
+        roof_fp32["executed_inst_per_cell_launch"] = prof["executed_inst_per_cell_substep"]
+    t_hbm = alg_bytes / (pk["hbm_gbs"] * 1e9)
+    t_fp32 = alg_flop / (fp32_peak * 1e12)
+    roof["binding"] = "fp32" if t_fp32 > t_hbm else "hbm"
+    roof["frac_of_binding"] = max(t_hbm, t_fp32) / launch_s
 
     result = None
     if rank == 0:
@@ -437,6 +464,7 @@ def run_mine(args, rank, world, local_rank):
                        "l2": "state %.0f MB (two buffers) > 126 MB L2; no flush" % (
                            2 * (4 if scheme == "EE2D_KP07_dimsplit" else 3) * cells * 4 / 1e6)},
             "roofline": roof,
+            "roofline_fp32": roof_fp32,
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "wall_s_timed_region": wall,

@@ -53,9 +53,45 @@ int ghost_cells(int scheme) {
 }
 int num_vars(int scheme) { return scheme == EE2D_KP07_DIMSPLIT ? 4 : 3; }
 
-template <typename T> inline T sgn1(T x) { return std::copysign(T(1), x); }
+// Math helpers.  Unqualified so that the operation-counting type below can
+// supply its own overloads.
+template <typename T> inline T sqrt_(T x) { return std::sqrt(x); }
+template <typename T> inline T fabs_(T x) { return std::fabs(x); }
+template <typename T> inline T copysign_(T a, T b) { return std::copysign(a, b); }
 template <typename T> inline T fmin_(T a, T b) { return std::fmin(a, b); }
 template <typename T> inline T fmax_(T a, T b) { return std::fmax(a, b); }
+template <typename T> inline T sgn1(T x) { return copysign_(T(1), x); }
+
+// ---------------------------------------------------------------- operation counting
+// A double that counts the floating-point operations applied to it, used to
+// measure the algorithmic cost of one substep of each scheme as the reference
+// formulates it (run single-threaded).  Sign manipulation (fabs, copysign) and
+// comparisons are not counted.
+struct OpCounts {
+    long long add, sub, mul, div, sqrt, minmax;
+};
+OpCounts g_ops;
+
+struct Counted {
+    double v;
+    Counted() : v(0.0) {}
+    Counted(double x) : v(x) {}
+    explicit operator double() const { return v; }
+    Counted operator-() const { return Counted(-v); }
+};
+inline Counted operator+(Counted a, Counted b) { ++g_ops.add; return Counted(a.v + b.v); }
+inline Counted operator-(Counted a, Counted b) { ++g_ops.sub; return Counted(a.v - b.v); }
+inline Counted operator*(Counted a, Counted b) { ++g_ops.mul; return Counted(a.v * b.v); }
+inline Counted operator/(Counted a, Counted b) { ++g_ops.div; return Counted(a.v / b.v); }
+inline bool operator<(Counted a, Counted b) { return a.v < b.v; }
+inline bool operator>(Counted a, Counted b) { return a.v > b.v; }
+inline bool operator<=(Counted a, Counted b) { return a.v <= b.v; }
+inline bool operator>=(Counted a, Counted b) { return a.v >= b.v; }
+template <> inline Counted sqrt_(Counted x) { ++g_ops.sqrt; return Counted(std::sqrt(x.v)); }
+template <> inline Counted fabs_(Counted x) { return Counted(std::fabs(x.v)); }
+template <> inline Counted copysign_(Counted a, Counted b) { return Counted(std::copysign(a.v, b.v)); }
+template <> inline Counted fmin_(Counted a, Counted b) { ++g_ops.minmax; return Counted(std::fmin(a.v, b.v)); }
+template <> inline Counted fmax_(Counted a, Counted b) { ++g_ops.minmax; return Counted(std::fmax(a.v, b.v)); }
 
 template <typename T, int N> struct Vec {
     T c[N];
@@ -70,7 +106,7 @@ inline T minmod_slope(T left, T center, T right, T theta) {
     const T forward = (right - center) * theta;
     return T(0.25) * sgn1(backward) * (sgn1(backward) + sgn1(central)) *
            (sgn1(central) + sgn1(forward)) *
-           fmin_(fmin_(std::fabs(backward), std::fabs(central)), std::fabs(forward));
+           fmin_(fmin_(fabs_(backward), fabs_(central)), fabs_(forward));
 }
 
 // GPUSimulators/cuda/limiters.h:100-102
@@ -80,7 +116,7 @@ template <typename T> inline T generalized_minmod(T r, T theta) {
 
 // GPUSimulators/cuda/common.h:81-83
 template <typename T> inline T desingularize(T x, T eps) {
-    return sgn1(x) * fmax_(std::fabs(x), fmin_(x * x / (T(2) * eps) + T(0.5) * eps, eps));
+    return sgn1(x) * fmax_(fabs_(x), fmin_(x * x / (T(2) * eps) + T(0.5) * eps, eps));
 }
 
 // ---------------------------------------------------------------- shallow water
@@ -97,10 +133,10 @@ template <typename T> inline Vec<T, 3> swe_F(const Vec<T, 3>& Q, T g) {
 template <typename T> inline Vec<T, 3> swe_central_upwind(const Vec<T, 3>& Qm, const Vec<T, 3>& Qp, T g) {
     const Vec<T, 3> Fp = swe_F(Qp, g);
     const T up = Qp.c[1] / Qp.c[0];
-    const T cp = std::sqrt(g * Qp.c[0]);
+    const T cp = sqrt_(g * Qp.c[0]);
     const Vec<T, 3> Fm = swe_F(Qm, g);
     const T um = Qm.c[1] / Qm.c[0];
-    const T cm = std::sqrt(g * Qm.c[0]);
+    const T cm = sqrt_(g * Qm.c[0]);
     const T am = fmin_(fmin_(um - cm, up - cp), T(0));
     const T ap = fmax_(fmax_(um + cm, up + cp), T(0));
     const T apam = ap * am;
@@ -116,11 +152,11 @@ template <typename T> inline Vec<T, 3> swe_hll(const Vec<T, 3>& Ql, const Vec<T,
     const T h_r = Qr.c[0];
     const T u_l = Ql.c[1] / h_l;
     const T u_r = Qr.c[1] / h_r;
-    const T c_l = std::sqrt(g * h_l);
-    const T c_r = std::sqrt(g * h_r);
+    const T c_l = sqrt_(g * h_l);
+    const T c_r = sqrt_(g * h_r);
     const T h_dag = T(0.5) * (h_l + h_r) - T(0.25) * (u_r - u_l) * (h_l + h_r) / (c_l + c_r);
-    const T q_l_tmp = std::sqrt(T(0.5) * ((h_dag + h_l) * h_dag / (h_l * h_l)));
-    const T q_r_tmp = std::sqrt(T(0.5) * ((h_dag + h_r) * h_dag / (h_r * h_r)));
+    const T q_l_tmp = sqrt_(T(0.5) * ((h_dag + h_l) * h_dag / (h_l * h_l)));
+    const T q_r_tmp = sqrt_(T(0.5) * ((h_dag + h_r) * h_dag / (h_r * h_r)));
     const T q_l = (h_dag > h_l) ? q_l_tmp : T(1);
     const T q_r = (h_dag > h_r) ? q_r_tmp : T(1);
     const T S_l = u_l - c_l * q_l;
@@ -137,7 +173,7 @@ template <typename T> inline Vec<T, 3> swe_hll(const Vec<T, 3>& Ql, const Vec<T,
 }
 
 // GPUSimulators/cuda/SWECommon.h:109-111
-template <typename T> inline T limiter_to_waf_limiter(T r, T c) { return T(1) - (T(1) - std::fabs(c)) * r; }
+template <typename T> inline T limiter_to_waf_limiter(T r, T c) { return T(1) - (T(1) - fabs_(c)) * r; }
 
 // GPUSimulators/cuda/SWECommon.h:114-121
 template <typename T> inline T compute_h_star(T h_l, T h_r, T u_l, T u_r, T c_l, T c_r, T g) {
@@ -157,13 +193,13 @@ inline Vec<T, 3> swe_waf(const Vec<T, 3>& Ql2, const Vec<T, 3>& Ql1, const Vec<T
     const T u_l2 = Ql2.c[1] / h_l2, u_r2 = Qr2.c[1] / h_r2;
     const T v_l = Ql1.c[2] / h_l, v_r = Qr1.c[2] / h_r;
     const T v_l2 = Ql2.c[2] / h_l2, v_r2 = Qr2.c[2] / h_r2;
-    const T c_l = std::sqrt(g * h_l), c_r = std::sqrt(g * h_r);
-    const T c_l2 = std::sqrt(g * h_l2), c_r2 = std::sqrt(g * h_r2);
+    const T c_l = sqrt_(g * h_l), c_r = sqrt_(g * h_r);
+    const T c_l2 = sqrt_(g * h_l2), c_r2 = sqrt_(g * h_r2);
     const T h_dag_l = compute_h_star(h_l2, h_l, u_l2, u_l, c_l2, c_l, g);
     const T h_dag = compute_h_star(h_l, h_r, u_l, u_r, c_l, c_r, g);
     const T h_dag_r = compute_h_star(h_r, h_r2, u_r, u_r2, c_r, c_r2, g);
-    const T q_l_tmp = std::sqrt(T(0.5) * ((h_dag + h_l) * h_dag)) / h_l;
-    const T q_r_tmp = std::sqrt(T(0.5) * ((h_dag + h_r) * h_dag)) / h_r;
+    const T q_l_tmp = sqrt_(T(0.5) * ((h_dag + h_l) * h_dag)) / h_l;
+    const T q_r_tmp = sqrt_(T(0.5) * ((h_dag + h_r) * h_dag)) / h_r;
     const T q_l = (h_dag > h_l) ? q_l_tmp : T(1);
     const T q_r = (h_dag > h_r) ? q_r_tmp : T(1);
     const T S_l = u_l - c_l * q_l;
@@ -255,11 +291,11 @@ template <typename T> inline Vec<T, 4> euler_hll(const Vec<T, 4>& Ql, const Vec<
     const T h_l = Ql.c[0], h_r = Qr.c[0];
     const T u_l = Ql.c[1] / h_l, u_r = Qr.c[1] / h_r;
     const T P_l = euler_pressure(Ql, gamma), P_r = euler_pressure(Qr, gamma);
-    const T c_l = std::sqrt(gamma * P_l / Ql.c[0]);
-    const T c_r = std::sqrt(gamma * P_r / Qr.c[0]);
+    const T c_l = sqrt_(gamma * P_l / Ql.c[0]);
+    const T c_r = sqrt_(gamma * P_r / Qr.c[0]);
     const T h_dag = T(0.5) * (h_l + h_r) - T(0.25) * (u_r - u_l) * (h_l + h_r) / (c_l + c_r);
-    const T q_l_tmp = std::sqrt(T(0.5) * ((h_dag + h_l) * h_dag / (h_l * h_l)));
-    const T q_r_tmp = std::sqrt(T(0.5) * ((h_dag + h_r) * h_dag / (h_r * h_r)));
+    const T q_l_tmp = sqrt_(T(0.5) * ((h_dag + h_l) * h_dag / (h_l * h_l)));
+    const T q_r_tmp = sqrt_(T(0.5) * ((h_dag + h_r) * h_dag / (h_r * h_r)));
     const T q_l = (h_dag > h_l) ? q_l_tmp : T(1);
     const T q_r = (h_dag > h_r) ? q_r_tmp : T(1);
     const T S_l = u_l - c_l * q_l;
@@ -279,11 +315,11 @@ template <typename T> inline Vec<T, 4> euler_central_upwind(const Vec<T, 4>& Qm,
     const T Pp = euler_pressure(Qp, gamma);
     const Vec<T, 4> Fp = euler_F(Qp, Pp);
     const T up = Qp.c[1] / Qp.c[0];
-    const T cp = std::sqrt(gamma * Pp / Qp.c[0]);
+    const T cp = sqrt_(gamma * Pp / Qp.c[0]);
     const T Pm = euler_pressure(Qm, gamma);
     const Vec<T, 4> Fm = euler_F(Qm, Pm);
     const T um = Qm.c[1] / Qm.c[0];
-    const T cm = std::sqrt(gamma * Pm / Qm.c[0]);
+    const T cm = sqrt_(gamma * Pm / Qm.c[0]);
     const T am = fmin_(fmin_(um - cm, up - cp), T(0));
     const T ap = fmax_(fmax_(um + cm, up + cp), T(0));
     const T apam = ap * am;
@@ -448,6 +484,16 @@ inline Vec<T, 4> euler_face_flux(const Params<T>& P, const Line<T, 4>& L, int k,
     return euler_central_upwind(Ql_bar, Qr_bar, gamma);         // EE2D_KP07_dimsplit.cu:106
 }
 template <>
+inline Vec<Counted, 3> face_flux<Counted, 3>(const Params<Counted>& P, const Line<Counted, 3>& L, int k, Counted dxx,
+                                             bool) {
+    return swe_face_flux<Counted>(P, L, k, dxx);
+}
+template <>
+inline Vec<Counted, 4> face_flux<Counted, 4>(const Params<Counted>& P, const Line<Counted, 4>& L, int k, Counted dxx,
+                                             bool y) {
+    return euler_face_flux<Counted>(P, L, k, dxx, y);
+}
+template <>
 inline Vec<float, 4> face_flux<float, 4>(const Params<float>& P, const Line<float, 4>& L, int k, float dxx, bool y) {
     return euler_face_flux<float>(P, L, k, dxx, y);
 }
@@ -514,8 +560,8 @@ T cfl_min(const Params<T>& P, const Grid<T>& Q) {
             const T h = Q.at(0, l, k);
             const T u = Q.at(1, l, k) / h;
             const T v = Q.at(2, l, k) / h;
-            const T max_u = P.dx / (std::fabs(u) + std::sqrt(gg * h));
-            const T max_v = P.dy / (std::fabs(v) + std::sqrt(gg * h));
+            const T max_u = P.dx / (fabs_(u) + sqrt_(gg * h));
+            const T max_v = P.dy / (fabs_(v) + sqrt_(gg * h));
             const T c = fmin_(max_u, max_v);
             m = any ? fmin_(m, c) : c;
             any = true;
@@ -669,6 +715,42 @@ int fvo_substep_f64(int scheme, int nx, int ny, const double* const* in, double*
                     int nthreads) {
     return substep_impl<double>(scheme, nx, ny, in, out, dx, dy, dt, g, gamma, theta, step, order, bc, cfl,
                                 nthreads);
+}
+
+// Floating-point operations of one substep as the reference formulates it:
+// runs the substep single-threaded on `in` (nv arrays of (ny+2g) x (nx+2g)
+// values) with the counting type and stores the counts of add, sub, mul, div,
+// sqrt and min/max into counts[0..5].  The state it computes is discarded.
+int fvo_count_ops(int scheme, int nx, int ny, const double* const* in, double dx, double dy, double dt, double g,
+                  double gamma, double theta, int step, int order, int bc, long long* counts) {
+    if (scheme < 0 || scheme > 7 || nx <= 0 || ny <= 0) return 1;
+    const int gh = ghost_cells(scheme), nv = num_vars(scheme);
+    const size_t n = (size_t)(nx + 2 * gh) * (ny + 2 * gh);
+    std::vector<Counted> src[4], dst[4];
+    const Counted* ip[4] = {nullptr, nullptr, nullptr, nullptr};
+    Counted* op[4] = {nullptr, nullptr, nullptr, nullptr};
+    for (int v = 0; v < nv; ++v) {
+        src[v].assign(in[v], in[v] + n);
+        dst[v].assign(n, Counted(0.0));
+        ip[v] = src[v].data();
+        op[v] = dst[v].data();
+    }
+#ifdef _OPENMP
+    const int threads = omp_get_max_threads();
+#endif
+    g_ops = OpCounts{0, 0, 0, 0, 0, 0};
+    const int rc = substep_impl<Counted>(scheme, nx, ny, ip, op, Counted(dx), Counted(dy), Counted(dt), Counted(g),
+                                         Counted(gamma), Counted(theta), step, order, bc, nullptr, 1);
+#ifdef _OPENMP
+    omp_set_num_threads(threads);
+#endif
+    counts[0] = g_ops.add;
+    counts[1] = g_ops.sub;
+    counts[2] = g_ops.mul;
+    counts[3] = g_ops.div;
+    counts[4] = g_ops.sqrt;
+    counts[5] = g_ops.minmax;
+    return rc;
 }
 
 int fvo_ghost_cells(int scheme) { return ghost_cells(scheme); }

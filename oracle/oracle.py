@@ -118,6 +118,73 @@ def oracle_substep(scheme, u_in, u_out, nx, ny, dx, dy, dt, g, gamma, theta, ste
     return dtype.type(cfl.value) if want_cfl else None
 
 
+OP_NAMES = ("add", "sub", "mul", "div", "sqrt", "minmax")
+
+
+def count_ops(scheme, u_in, nx, ny, dx, dy, dt, g, gamma, theta, step, order, bc):
+    """Floating-point operations of one stage kernel of `scheme` as the reference
+    formulates it, on full (ny+2g, nx+2g) float64 arrays: a dict over OP_NAMES."""
+    L = lib()
+    P = ctypes.POINTER(ctypes.c_double)
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in u_in]
+    ins = (P * len(arrs))(*[a.ctypes.data_as(P) for a in arrs])
+    counts = (ctypes.c_longlong * 6)()
+    f = L.fvo_count_ops
+    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(P)] + [ctypes.c_double] * 6 + [
+        ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]
+    f.restype = ctypes.c_int
+    if f(SCHEMES[scheme], nx, ny, ins, dx, dy, dt, g, gamma, theta, step, order, bc, counts) != 0:
+        raise RuntimeError("oracle operation count failed")
+    return dict(zip(OP_NAMES, (int(c) for c in counts)))
+
+
+def ops_per_cell_substep(scheme, order=2):
+    """Algorithmic floating-point operations per interior cell and substep of
+    `scheme`, averaged over the substeps of one step: each count is fitted as
+    a*n^2 + b*n + c over n x n grids (n = 16, 32, 64) so that the ghost-line and
+    extra-face work of a finite grid drops out, and `a` is returned.  Also
+    returns 'flops' (+, -, *, /, sqrt, min, max counted 1 each) and 'mufu'
+    (divisions and square roots, the special-function work).  The state is a
+    smooth bump at rest (a lake with a Gaussian mound; Kelvin-Helmholtz bands
+    for the Euler scheme) with reflective walls, so every face takes the
+    subsonic branch of the HLL-type fluxes."""
+    steps = (0, 1) if (scheme in DIMSPLIT_HALF_DT or (scheme == "KP07" and order == 2)) else (0,)
+    theta = DEFAULT_THETA.get(scheme, 1.3)
+    gc = ghost_cells(scheme)
+    sizes = (16, 32, 64)
+    per_size = []
+    for n in sizes:
+        m = n + 2 * gc
+        y, x = np.mgrid[0:m, 0:m] + 0.5 - gc
+        if scheme == "EE2D_KP07_dimsplit":
+            band = (y >= 0.25 * n) & (y < 0.75 * n)
+            rho = np.where(band, 2.0, 1.0)
+            u = np.where(band, 0.5, -0.5)
+            v = 0.01 * np.sin(4 * np.pi * x / n)
+            q = [rho, rho * u, rho * v, 2.5 / 0.4 + 0.5 * rho * (u * u + v * v)]
+            dx = 1.0 / n
+            g, dt = 0.0, 0.1 * dx
+        else:
+            h = 1.0 + 0.3 * np.exp(-((x - 0.45 * n) ** 2 + (y - 0.55 * n) ** 2) / (2 * (n / 8.0) ** 2))
+            q = [h, np.zeros_like(h), np.zeros_like(h)]
+            dx = 1.0
+            g, dt = 9.81, 0.05
+        tot = dict.fromkeys(OP_NAMES, 0)
+        for st in steps:
+            c = count_ops(scheme, q, n, n, dx, dx, dt, g, 1.4, theta, st, order, 0x03030303)
+            for k in OP_NAMES:
+                tot[k] += c[k]
+        per_size.append({k: tot[k] / len(steps) for k in OP_NAMES})
+    A = np.array([[n * n, n, 1.0] for n in sizes])
+    out = {}
+    for k in OP_NAMES:
+        a, _, _ = np.linalg.solve(A, np.array([c[k] for c in per_size], dtype=np.float64))
+        out[k] = round(float(a), 6)
+    out["flops"] = round(sum(out[k] for k in OP_NAMES), 6)
+    out["mufu"] = round(out["div"] + out["sqrt"], 6)
+    return out
+
+
 class OracleSim:
     """A reference simulator's host semantics, on the CPU oracle."""
 
