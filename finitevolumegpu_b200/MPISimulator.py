@@ -1,0 +1,388 @@
+"""Row-stripe domain decomposition: the counterpart of GPUSimulators/MPISimulator.py.
+
+The reference splits one domain into north-south stripes, one MPI rank (and
+GPU) per stripe (``MPIGrid.getGrid`` keeps ``grid[0] = 1``,
+GPUSimulators/MPISimulator.py:137-143).  Each rank runs an ordinary simulator
+on its stripe whose internal north/south edges are Dirichlet, i.e. whose ghost
+rows hold whatever was last stored there (MPISimulator.py:239-258); after every
+substep the ranks exchange two rows with each neighbour, so those ghost rows
+hold the neighbour's edge rows (``full_exchange``, :371-480), and the time step
+is the minimum over all ranks (``computeDt``, :349-355).
+
+Here the same scheme runs on top of the sm_100a simulators:
+
+* ``StripeGrid`` is the ``MPIGrid`` counterpart over a ``torch.distributed``
+  process group (NCCL between GPUs, gloo on CPU).
+* ``MPISimulator(sim, grid)`` wraps a local simulator like the reference class.
+  The halo rows are zero-copy views of the simulator's device buffers
+  (``BaseSimulator.halo_views``) and the sends and receives are issued on the
+  simulator's own CUDA stream, so they are ordered with the stage kernels
+  without host synchronisation.  Each message is one variable's two full
+  storage rows (ghost columns included), 2 x pitch floats.
+* ``StripedSimulator`` runs all stripes of a domain in one process (on one
+  GPU or several), exchanging the rows with device copies ordered by CUDA
+  events.
+
+East and west edges are not exchanged: every stripe spans the whole width, so
+its own boundary handling (periodic wrap or reflective mirror along x,
+including the corner cells of the exchanged ghost rows) gives the cells the
+reference's self-exchange along x gives.  With the same per-cell arithmetic in
+every tile, a decomposed run reproduces the single-domain run bit for bit.
+
+Any local simulator with this interface can be decomposed: ``nx, ny, dx, dy,
+cfl_scale, num_substeps``, ``substep(dt, step_number)``, ``computeDt()``,
+``download()``, ``synchronize()``, ``getBoundaryConditions()`` /
+``setBoundaryConditions(bc)``, ``halo_views()`` and ``comm_stream()``.
+"""
+
+from __future__ import annotations
+
+import logging
+
+import numpy as np
+
+from .Simulator import BoundaryCondition
+
+GOING_NORTH = 0  # tag of rows sent to the northern neighbour (they fill its south ghost rows)
+GOING_SOUTH = 1  # tag of rows sent to the southern neighbour (they fill its north ghost rows)
+
+
+def stripe_rows(ny, n):
+    """Split ny rows into n stripes, south to north: a list of (first row, rows);
+    sizes differ by at most one row."""
+    ny, n = int(ny), int(n)
+    assert 1 <= n <= ny, "cannot split %d rows into %d stripes" % (ny, n)
+    base, extra = divmod(ny, n)
+    out, y = [], 0
+    for j in range(n):
+        rows = base + (1 if j < extra else 0)
+        out.append((y, rows))
+        y += rows
+    return out
+
+
+def stripe_boundaries(boundary_conditions, j, n):
+    """Boundary conditions of stripe j of n and whether it has a southern and a
+    northern neighbour (MPISimulator.py:239-258): internal edges become
+    Dirichlet, the domain's south (north) edge keeps its condition unless it is
+    periodic, in which case the first and last stripes are neighbours."""
+    bc = boundary_conditions
+    T = BoundaryCondition.Type
+    has_south = not (j == 0 and bc.south != T.Periodic)
+    has_north = not (j == n - 1 and bc.north != T.Periodic)
+    new = BoundaryCondition({
+        "north": T.Dirichlet if has_north else bc.north,
+        "south": T.Dirichlet if has_south else bc.south,
+        "east": bc.east,
+        "west": bc.west,
+    })
+    return new, has_south, has_north
+
+
+class StripeGrid(object):
+    """North-south stripes over a torch.distributed process group: the
+    counterpart of MPIGrid (GPUSimulators/MPISimulator.py:34-203) with its
+    vertical-only partitioning."""
+
+    def __init__(self, group=None, device=None):
+        import torch.distributed as dist
+
+        assert dist.is_initialized(), "torch.distributed must be initialised"
+        self.group = group
+        self.rank = dist.get_rank(group)
+        self.size = dist.get_world_size(group)
+        self.grid = np.array([1, self.size])
+        self.backend = dist.get_backend(group)
+        if device is None:
+            import torch
+
+            device = torch.device("cuda", torch.cuda.current_device()) if self.backend == "nccl" else torch.device("cpu")
+        self.device = device
+
+    def getCoordinate(self, rank=None):
+        rank = self.rank if rank is None else rank
+        return 0, rank
+
+    def getRank(self, i, j):
+        return j
+
+    def getNorth(self):
+        return (self.rank + 1) % self.size
+
+    def getSouth(self):
+        return (self.rank + self.size - 1) % self.size
+
+    def getEast(self):
+        return self.rank
+
+    def getWest(self):
+        return self.rank
+
+    def getLocalRank(self):
+        import os
+
+        return int(os.environ.get("LOCAL_RANK", self.rank))
+
+    def exchange(self, sends, recvs):
+        """Point-to-point messages: sends and recvs are lists of (peer, tensor,
+        tag), posted in list order; returns once all have completed on the
+        current stream."""
+        import torch.distributed as dist
+
+        ops = [dist.P2POp(dist.isend, t, self._global(p), self.group, tag) for p, t, tag in sends]
+        ops += [dist.P2POp(dist.irecv, t, self._global(p), self.group, tag) for p, t, tag in recvs]
+        if ops:
+            for w in dist.batch_isend_irecv(ops):
+                w.wait()
+
+    def allreduce_min(self, value):
+        import torch
+        import torch.distributed as dist
+
+        t = torch.tensor([float(value)], dtype=torch.float32, device=self.device)
+        dist.all_reduce(t, op=dist.ReduceOp.MIN, group=self.group)
+        return np.float32(t.item())
+
+    def gather(self, data, root=0):
+        """Stripes of all ranks stacked on `root` (None elsewhere)."""
+        import torch.distributed as dist
+
+        out = [None] * self.size if self.rank == root else None
+        dist.gather_object(np.asarray(data), out, dst=self._global(root), group=self.group)
+        return out
+
+    def _global(self, rank):
+        import torch.distributed as dist
+
+        return rank if self.group is None else dist.get_global_rank(self.group, rank)
+
+
+def _exchange_plan(views, north, south):
+    """Sends and receives of one halo exchange in an order every rank shares:
+    both sends, then the receive from the south, then from the north, so the
+    k-th message between two ranks is matched by position even when the
+    northern and southern neighbours are the same rank."""
+    sends, recvs = [], []
+    nv = len(views["north_send"])
+    if north is not None:
+        sends += [(north, views["north_send"][v], GOING_NORTH) for v in range(nv)]
+    if south is not None:
+        sends += [(south, views["south_send"][v], GOING_SOUTH) for v in range(nv)]
+    if south is not None:
+        recvs += [(south, views["south_ghost"][v], GOING_NORTH) for v in range(nv)]
+    if north is not None:
+        recvs += [(north, views["north_ghost"][v], GOING_SOUTH) for v in range(nv)]
+    return sends, recvs
+
+
+class MPISimulator(object):
+    """One stripe of a decomposed simulation (GPUSimulators/MPISimulator.py:205-480).
+
+    ``sim`` is this rank's simulator on its stripe (nx x ny_local cells, its
+    own initial state), ``grid`` a ``StripeGrid``.  Time stepping follows
+    BaseSimulator.simulate/step (GPUSimulators/Simulator.py:176-228), with the
+    time step reduced over all ranks."""
+
+    def __init__(self, sim, grid):
+        self.logger = logging.getLogger(__name__)
+        self.sim = sim
+        self.grid = grid
+        self.context = getattr(sim, "context", None)
+        self.nx, self.ny, self.dx, self.dy = sim.nx, sim.ny, sim.dx, sim.dy
+        self.cfl_scale = sim.cfl_scale
+        self.num_substeps = sim.num_substeps
+        self.t, self.nt = 0.0, 0
+        self.dt = None
+        bc = sim.getBoundaryConditions()
+        self.boundary_conditions = bc
+        _, j = grid.getCoordinate()
+        new_bc, has_south, has_north = stripe_boundaries(bc, j, grid.grid[1])
+        self.north = grid.getNorth() if has_north else None
+        self.south = grid.getSouth() if has_south else None
+        self.east = self.west = None
+        sim.setBoundaryConditions(new_bc)
+        self.full_exchange()
+        sim.synchronize()
+
+    # -- Simulator.py:176-217
+    def simulate(self, t, dt=None):
+        t_end = self.t + t
+        update_dt = dt is None
+        if not update_dt:
+            self.dt = np.float32(dt)
+        while self.t < t_end:
+            if update_dt and (self.nt % 100 == 0):
+                self.dt = np.float32(self.computeDt() * np.float32(self.cfl_scale))
+            current_dt = np.float32(min(self.dt, t_end - self.t))
+            if current_dt <= 0.0:
+                break
+            self.step(current_dt)
+        return self.t, self.nt
+
+    # -- Simulator.py:220-228
+    def step(self, dt):
+        for i in range(self.num_substeps):
+            self.substep(dt, i)
+        self.t = float(self.t) + float(np.float32(dt))
+        self.nt += 1
+
+    def substep(self, dt, step_number):
+        self.sim.substep(dt, step_number)
+        self.full_exchange()
+
+    def computeDt(self):
+        return self.grid.allreduce_min(np.float32(self.sim.computeDt()))
+
+    def full_exchange(self):
+        views = self.sim.halo_views()
+        me = self.grid.rank
+        sends, recvs = _exchange_plan(views, self.north, self.south)
+        stream = self.sim.comm_stream()
+        ctx = _stream_context(stream)
+        with ctx:
+            # a stripe that is its own neighbour (periodic, one rank) copies locally
+            nv = len(views["north_send"])
+            if self.south == me:
+                for v in range(nv):
+                    views["south_ghost"][v].copy_(views["north_send"][v])
+            if self.north == me:
+                for v in range(nv):
+                    views["north_ghost"][v].copy_(views["south_send"][v])
+            self.grid.exchange([s for s in sends if s[0] != me], [r for r in recvs if r[0] != me])
+
+    def download(self, variables=None):
+        return self.sim.download(variables) if variables is not None else self.sim.download()
+
+    def getOutput(self):
+        return self.sim.getOutput()
+
+    def synchronize(self):
+        self.sim.synchronize()
+
+    def check(self):
+        return self.sim.check()
+
+    def simTime(self):
+        return self.t
+
+    def simSteps(self):
+        return self.nt
+
+    def getBoundaryConditions(self):
+        return self.boundary_conditions
+
+    def getExtent(self):
+        """[x0, x1, y0, y1] of this rank's stripe (MPISimulator.py:357-369)."""
+        width = self.nx * self.dx
+        height = self.ny * self.dy
+        i, j = self.grid.getCoordinate()
+        x0, y0 = i * width, j * height
+        return [x0, x0 + width, y0, y0 + height]
+
+
+def _stream_context(stream):
+    if stream is None:
+        import contextlib
+
+        return contextlib.nullcontext()
+    import torch
+
+    return torch.cuda.stream(stream)
+
+
+class StripedSimulator(object):
+    """All stripes of one domain in one process (``sims`` ordered south to
+    north, each holding its stripe's initial state): halo rows move by device
+    copies ordered with CUDA events between the stripes' streams (or plain
+    copies for host-memory simulators).  Results equal a single-domain run."""
+
+    def __init__(self, sims, boundary_conditions=None):
+        assert len(sims) >= 1
+        self.sims = list(sims)
+        s0 = self.sims[0]
+        assert all(s.nx == s0.nx for s in self.sims), "stripes must have the same width"
+        self.nx = s0.nx
+        self.ny = sum(int(s.ny) for s in self.sims)
+        self.dx, self.dy = s0.dx, s0.dy
+        self.cfl_scale = s0.cfl_scale
+        self.num_substeps = s0.num_substeps
+        self.t, self.nt, self.dt = 0.0, 0, None
+        bc = boundary_conditions or s0.getBoundaryConditions()
+        self.boundary_conditions = bc
+        n = len(self.sims)
+        self.neighbours = []
+        for j, s in enumerate(self.sims):
+            new_bc, has_south, has_north = stripe_boundaries(bc, j, n)
+            s.setBoundaryConditions(new_bc)
+            self.neighbours.append(((j + n - 1) % n if has_south else None, (j + 1) % n if has_north else None))
+        self.full_exchange()
+        for s in self.sims:
+            s.synchronize()
+
+    def simulate(self, t, dt=None):
+        t_end = self.t + t
+        update_dt = dt is None
+        if not update_dt:
+            self.dt = np.float32(dt)
+        while self.t < t_end:
+            if update_dt and (self.nt % 100 == 0):
+                self.dt = np.float32(self.computeDt() * np.float32(self.cfl_scale))
+            current_dt = np.float32(min(self.dt, t_end - self.t))
+            if current_dt <= 0.0:
+                break
+            self.step(current_dt)
+        return self.t, self.nt
+
+    def step(self, dt):
+        for i in range(self.num_substeps):
+            self.substep(dt, i)
+        self.t = float(self.t) + float(np.float32(dt))
+        self.nt += 1
+
+    def substep(self, dt, step_number):
+        for s in self.sims:
+            s.substep(dt, step_number)
+        self.full_exchange()
+
+    def computeDt(self):
+        return np.float32(min(np.float32(s.computeDt()) for s in self.sims))
+
+    def full_exchange(self):
+        views = [s.halo_views() for s in self.sims]
+        streams = [s.comm_stream() for s in self.sims]
+        events = None
+        if streams[0] is not None:
+            import torch
+
+            events = []
+            for st in streams:
+                ev = torch.cuda.Event()
+                ev.record(st)
+                events.append(ev)
+        for j, (south, north) in enumerate(self.neighbours):
+            dst = views[j]
+            pairs = []
+            if south is not None:
+                pairs.append((south, "south_ghost", "north_send"))
+            if north is not None:
+                pairs.append((north, "north_ghost", "south_send"))
+            with _stream_context(streams[j]):
+                for peer, ghost, send in pairs:
+                    if events is not None:
+                        streams[j].wait_event(events[peer])
+                    for v in range(len(dst[ghost])):
+                        dst[ghost][v].copy_(views[peer][send][v])
+
+    def download(self):
+        parts = [s.download() for s in self.sims]
+        return [np.concatenate([p[v] for p in parts], axis=0) for v in range(len(parts[0]))]
+
+    def synchronize(self):
+        for s in self.sims:
+            s.synchronize()
+
+    def simTime(self):
+        return self.t
+
+    def simSteps(self):
+        return self.nt

@@ -111,6 +111,14 @@ class _StateView(object):
         self._sim.check()
 
 
+class _DeviceRows(object):
+    """A device range of FP32 values seen through the CUDA array interface."""
+
+    def __init__(self, address, count):
+        self.__cuda_array_interface__ = {"shape": (int(count),), "typestr": "<f4", "data": (int(address), False),
+                                         "version": 3, "strides": None}
+
+
 class BaseSimulator(object):
     """Common state and time loop of all schemes (GPUSimulators/Simulator.py:109-266)."""
 
@@ -136,6 +144,8 @@ class BaseSimulator(object):
         self.internal_stream = None
         self._handle = None
         self._nv = 3
+        self._state = None  # (buffer pointers, pitch) for halo views, queried on first use
+        self._cur = None    # buffer holding the current state, tracked across substeps; None = ask the device
 
     # -- construction helper used by the scheme classes
     def _create(self, variables, g=9.81, gamma=1.4, theta=1.3, order=2):
@@ -176,6 +186,7 @@ class BaseSimulator(object):
     # -- time stepping (Simulator.py:176-228)
     def simulate(self, t, dt=None):
         """Advance by t seconds; dt=None recomputes dt = computeDt()*cfl_scale every 100 steps."""
+        self._cur = None
         if dt is None:
             _lib.check(_lib.lib().fv_sim_simulate(self._handle, float(t), 0.0, 0))
         else:
@@ -183,13 +194,55 @@ class BaseSimulator(object):
 
     def step(self, dt):
         _lib.check(_lib.lib().fv_sim_step(self._handle, float(np.float32(dt))))
+        if self._cur is not None:
+            self._cur ^= self.num_substeps & 1
 
     def substep(self, dt, step_number):
         _lib.check(_lib.lib().fv_sim_substep(self._handle, float(np.float32(dt)), int(step_number)))
+        if self._cur is not None:
+            self._cur ^= 1  # every stage launch writes the other buffer
 
     def advance(self, n_steps):
         """Run exactly n_steps steps with simulate()'s dt schedule (benchmark helper)."""
+        self._cur = None
         _lib.check(_lib.lib().fv_sim_advance(self._handle, int(n_steps)))
+
+    # -- device state for row-stripe halo exchange (MPISimulator.py)
+    def halo_views(self):
+        """Zero-copy torch views of the rows a north-south halo exchange moves, in
+        the buffer that holds the current state: a dict with 'south_ghost'
+        (domain rows -2, -1), 'south_send' (rows 0, 1), 'north_send' (rows
+        ny-2, ny-1) and 'north_ghost' (rows ny, ny+1), each a list with one
+        1-D float32 CUDA tensor per variable covering those two full storage
+        rows (ghost columns included).  Work on them must be ordered on
+        comm_stream()."""
+        import torch
+
+        if self._state is None or self._cur is None:
+            ptrs = (_lib._FP * 8)()
+            pitch, cur = ctypes.c_int(), ctypes.c_int()
+            _lib.check(_lib.lib().fv_sim_buffers(self._handle, ptrs, ctypes.byref(pitch), ctypes.byref(cur)))
+            addrs = [ctypes.cast(ptrs[k], ctypes.c_void_p).value for k in range(8)]
+            self._state = (addrs, pitch.value)
+            self._cur = cur.value
+        addrs, pitch = self._state
+        ny = int(self.ny)
+        dev = torch.device("cuda", self.context.device_id)
+
+        def rows(var, r0):
+            base = addrs[self._cur * 4 + var] + r0 * pitch * 4
+            return torch.as_tensor(_DeviceRows(base, 2 * pitch), device=dev)
+
+        views = {"south_ghost": 0, "south_send": 2, "north_send": ny, "north_ghost": ny + 2}
+        return {k: [rows(v, r0) for v in range(self._nv)] for k, r0 in views.items()}
+
+    def comm_stream(self):
+        """The simulation's CUDA stream as a torch stream."""
+        import torch
+
+        p = ctypes.c_void_p()
+        _lib.check(_lib.lib().fv_sim_stream(self._handle, ctypes.byref(p)))
+        return torch.cuda.ExternalStream(p.value or 0, device=torch.device("cuda", self.context.device_id))
 
     def computeDt(self):
         d = ctypes.c_float()

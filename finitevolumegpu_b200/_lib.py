@@ -77,6 +77,8 @@ _SIGNATURES = {
     "fv_sim_check": ([_P, ctypes.POINTER(_I)], _I),
     "fv_sim_synchronize": ([_P], _I),
     "fv_sim_set_boundary_conditions": ([_P, _I], _I),
+    "fv_sim_buffers": ([_P, ctypes.POINTER(_FP), ctypes.POINTER(_I), ctypes.POINTER(_I)], _I),
+    "fv_sim_stream": ([_P, ctypes.POINTER(_P)], _I),
     "fv_sim_info": ([_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)], _I),
     "fv_sim_last_advance_ms": ([_P, ctypes.POINTER(_D)], _I),
     "fv_kp07_dimsplit_substep_noalloc": ([ctypes.POINTER(_FP), ctypes.POINTER(_FP), _I, _I, _I, _F, _F, _F, _F, _F,

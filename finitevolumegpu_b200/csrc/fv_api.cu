@@ -649,6 +649,24 @@ int fv_sim_set_boundary_conditions(fv_sim* s, int bc) {
     return FV_OK;
 }
 
+int fv_sim_buffers(fv_sim* s, float** ptrs, int* pitch, int* cur) {
+    FV_TRY(check_sim(s));
+    if (!ptrs || !pitch || !cur) return fail(FV_ERR_INVALID, "bad argument");
+    FV_TRY(read_ctl(s));
+    for (int b = 0; b < 2; ++b)
+        for (int v = 0; v < 4; ++v) ptrs[b * 4 + v] = (v < s->nv) ? s->buf[b][v] : nullptr;
+    *pitch = s->pitch;
+    *cur = s->ctl_h->cur;
+    return FV_OK;
+}
+
+int fv_sim_stream(fv_sim* s, void** stream) {
+    FV_TRY(check_sim(s));
+    if (!stream) return fail(FV_ERR_INVALID, "stream is null");
+    *stream = static_cast<void*>(s->stream);
+    return FV_OK;
+}
+
 int fv_sim_info(fv_sim* s, int* tile_w, int* tile_h, int* threads, int* launches_per_step) {
     if (!s) return fail(FV_ERR_INVALID, "null simulation");
     if (tile_w) *tile_w = s->ke->W;

@@ -135,6 +135,23 @@ FV_API int fv_sim_synchronize(fv_sim* sim);
 /* setBoundaryConditions (Simulator.py:245-247). */
 FV_API int fv_sim_set_boundary_conditions(fv_sim* sim, int bc);
 
+/* Device state of a simulation for halo exchange between row stripes
+ * (replaces the PyCUDA array access of MPISimulator.full_exchange,
+ * GPUSimulators/MPISimulator.py:371-480).  ptrs[b * 4 + v] receives the base
+ * of buffer b (0, 1) of variable v: storage row 0 is domain row y = -2, every
+ * row holds *pitch floats and domain cell (y, x) is at [(y + 2) * pitch +
+ * x + 4].  *cur is the buffer that holds the current state (this call waits
+ * for the simulation's stream).  Entries for v >= number of variables are
+ * null. */
+FV_API int fv_sim_buffers(fv_sim* sim, float** ptrs, int* pitch, int* cur);
+
+/* The CUDA stream (cudaStream_t) every launch and copy of the simulation is
+ * ordered on, so that a caller can order its own device work (e.g. NCCL halo
+ * sends and receives) with the stage kernels without host synchronisation.
+ * No reference counterpart (the reference's Simulator.stream is a PyCUDA
+ * stream, GPUSimulators/Simulator.py:164). */
+FV_API int fv_sim_stream(fv_sim* sim, void** stream);
+
 /* Device-side launches per step of the graph path, and the tile used
  * (introspection for benchmarks and tests). */
 FV_API int fv_sim_info(fv_sim* sim, int* tile_w, int* tile_h, int* threads, int* launches_per_step);

@@ -1,0 +1,100 @@
+"""Test helpers for the row-stripe decomposition on the CPU.
+
+``OracleStripe`` gives the CPU oracle the local-simulator interface that
+``MPISimulator`` and ``StripedSimulator`` drive (halo rows as torch views of its
+host arrays, no stream), so the decomposition logic and its message plan can
+be checked against a single-domain oracle run with gloo ranks, without a GPU.
+"""
+
+import os
+import socket
+
+import numpy as np
+
+from oracle.oracle import OracleSim
+
+
+class OracleStripe(OracleSim):
+    """OracleSim with the local-simulator interface of the stripe drivers."""
+
+    def getBoundaryConditions(self):
+        from finitevolumegpu_b200.Simulator import BoundaryCondition
+
+        return BoundaryCondition(BoundaryCondition.getTypes(self.bc))
+
+    def setBoundaryConditions(self, bc):
+        self.bc = int(bc.asCodedInt())
+
+    def halo_views(self):
+        import torch
+
+        g, ny = self.gc, self.ny
+
+        def rows(a, r0):
+            return torch.from_numpy(a[r0:r0 + g].reshape(-1))
+
+        return {"south_ghost": [rows(a, 0) for a in self.u0], "south_send": [rows(a, g) for a in self.u0],
+                "north_send": [rows(a, ny) for a in self.u0], "north_ghost": [rows(a, ny + g) for a in self.u0]}
+
+    def comm_stream(self):
+        return None
+
+    def synchronize(self):
+        pass
+
+
+def global_state(scheme, nx, ny, seed=0):
+    rng = np.random.default_rng(seed)
+    y, x = np.mgrid[0:ny, 0:nx] + 0.5
+    if scheme == "EE2D_KP07_dimsplit":
+        band = (y >= 0.25 * ny) & (y < 0.75 * ny)
+        rho = np.where(band, 2.0, 1.0)
+        u = np.where(band, 0.5, -0.5)
+        v = 0.01 * np.sin(4 * np.pi * x / nx + rng.uniform(0, 6.28))
+        q = [rho, rho * u, rho * v, 2.5 / 0.4 + 0.5 * rho * (u * u + v * v)]
+        return [a.astype(np.float32) for a in q], 1.0 / nx, 1.0 / ny, 0.0
+    cx, cy = rng.uniform(0.3, 0.7) * nx, rng.uniform(0.3, 0.7) * ny
+    h = 1.0 + 0.4 * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2 * (min(nx, ny) / 6.0) ** 2))
+    h = np.where(np.hypot(x - 0.7 * nx, y - 0.3 * ny) < 0.1 * min(nx, ny), 1.6, h)  # a small dam as well
+    z = np.zeros_like(h)
+    return [h.astype(np.float32), z.astype(np.float32), z.astype(np.float32)], 1.0, 1.0, 9.81
+
+
+def free_port():
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def gloo_worker(rank, world, port, scheme, nx, ny, bc, t_end, out_path):
+    """One rank of a gloo run: simulate this rank's stripe and gather to rank 0."""
+    import datetime
+
+    import torch.distributed as dist
+
+    from finitevolumegpu_b200.MPISimulator import MPISimulator, StripeGrid, stripe_rows
+
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        q, dx, dy, g = global_state(scheme, nx, ny)
+        y0, rows = stripe_rows(ny, world)[rank]
+        local = [a[y0:y0 + rows] for a in q]
+        sim = OracleStripe(scheme, local, nx, rows, dx, dy, g, cfl_scale=0.45, bc=bc)
+        mpi = MPISimulator(sim, StripeGrid())
+        mpi.simulate(t_end)
+        parts = mpi.grid.gather(np.stack(mpi.download()))
+        if rank == 0:
+            full = np.concatenate(parts, axis=1)
+            np.savez(out_path, state=full, nt=mpi.simSteps(), t=mpi.simTime())
+    finally:
+        dist.destroy_process_group()
+
+
+def run_gloo(world, scheme, nx, ny, bc, t_end, out_path):
+    import torch.multiprocessing as mp
+
+    os.environ.setdefault("GLOO_SOCKET_IFNAME", "lo")
+    mp.start_processes(gloo_worker, args=(world, free_port(), scheme, nx, ny, bc, t_end, out_path), nprocs=world,
+                       join=True, start_method="spawn")
+    return np.load(out_path)
