@@ -307,19 +307,19 @@ def run_batched(ctx, n_inst=512, seed=4, check=4):
     }
 
 
-def run_served(ctx, n_req=400, rate=300.0, seed=5, plain_sample=60):
+def run_served(ctx, n_req=400, rates=(300.0, 3000.0), seed=5, plain_sample=60, warmup_req=16):
     """Config 5: scenario requests with Poisson arrivals, scheme uniform over {KP07_dimsplit, HLL, EE2D},
-    sides log-uniform [128, 2048], t_end ~ U(1, 20), served with continuous batching under a 120 GB budget."""
+    sides log-uniform [128, 2048], t_end ~ U(1, 20), served with continuous batching under a 120 GB budget.
+    The same scenarios are served at each arrival rate of the sweep (the last one saturates the server);
+    a short warm-up serve first pays the one-time costs (memory pool and pinned staging growth)."""
     from finitevolumegpu_b200 import SCHEMES, BoundaryCondition
     from finitevolumegpu_b200.server import Request, Server
 
     rng = np.random.default_rng(seed)
     schemes = ["KP07_dimsplit", "HLL", "EE2D_KP07_dimsplit"]
     periodic = BoundaryCondition(BoundaryCondition.getTypes(0x02020202))
-    reqs = []
-    t = 0.0
+    scen = []
     for i in range(n_req):
-        t += rng.exponential(1.0 / rate)
         s = schemes[int(rng.integers(0, 3))]
         nx = int(round(np.exp(rng.uniform(np.log(128), np.log(2048)))))
         ny = int(round(np.exp(rng.uniform(np.log(128), np.log(2048)))))
@@ -327,31 +327,46 @@ def run_served(ctx, n_req=400, rate=300.0, seed=5, plain_sample=60):
             q, bc = kh_ic(nx, ny, rng), periodic  # unit cells: the Kelvin-Helmholtz family scaled to the grid
         else:
             q, bc = (bump_ic(nx, ny, rng) if rng.random() < 0.5 else dam_ic(nx, ny, rng)), None
-        reqs.append(Request(i, s, q, nx, ny, 1.0, 1.0, float(rng.uniform(1.0, 20.0)), arrival=t,
-                            boundary_conditions=bc))
-    server = Server(ctx, budget_bytes=120e9, chunk_steps=8)
-    results, stats = server.serve(reqs)
+        scen.append((s, q, nx, ny, float(rng.uniform(1.0, 20.0)), bc))
+    gaps = np.random.default_rng(seed + 1).exponential(1.0, n_req)
+
+    def requests(rate, count=n_req):
+        t = np.cumsum(gaps[:count]) / rate
+        return [Request(i, s, q, nx, ny, 1.0, 1.0, te, arrival=float(t[i]), boundary_conditions=bc)
+                for i, (s, q, nx, ny, te, bc) in enumerate(scen[:count])]
+
+    Server(ctx, budget_bytes=120e9, chunk_steps=8).serve(requests(1e9, warmup_req))
+    sweep, results = [], None
+    for rate in rates:
+        results, st = Server(ctx, budget_bytes=120e9, chunk_steps=8).serve(requests(rate))
+        st["arrival_rate_per_s"] = rate
+        sweep.append(st)
+    stats = dict(sweep[-1])
     # plain one-at-a-time path on a sample of the same requests
     by_id = {r.rid: r for r in results}
     t0 = time.perf_counter()
     cells = 0
     same = True
-    for r in reqs[:plain_sample]:
-        cls = SCHEMES[r.scheme]
-        kw = {} if r.boundary_conditions is None else {"boundary_conditions": r.boundary_conditions}
-        if r.scheme == "EE2D_KP07_dimsplit":
-            sim = cls(ctx, *r.variables, r.nx, r.ny, 1.0, 1.0, 0.0, 1.4, **kw)
+    for i, (s, q, nx, ny, te, bc) in enumerate(scen[:plain_sample]):
+        cls = SCHEMES[s]
+        kw = {} if bc is None else {"boundary_conditions": bc}
+        if s == "EE2D_KP07_dimsplit":
+            sim = cls(ctx, *q, nx, ny, 1.0, 1.0, 0.0, 1.4, **kw)
         else:
-            sim = cls(ctx, *r.variables, r.nx, r.ny, 1.0, 1.0, 9.81, **kw)
-        sim.simulate(r.t_end)
+            sim = cls(ctx, *q, nx, ny, 1.0, 1.0, 9.81, **kw)
+        sim.simulate(te)
         out = sim.download()
-        cells += r.nx * r.ny * sim.simSteps()
-        same = same and all(np.array_equal(a, w) for a, w in zip(out, by_id[r.rid].state))
+        cells += nx * ny * sim.simSteps()
+        same = same and all(np.array_equal(a, w) for a, w in zip(out, by_id[i].state))
         del sim
     plain_rate = cells / (time.perf_counter() - t0)
     stats.update({
-        "workload": "%d requests, Poisson arrivals at %.0f/s (seed %d), schemes KP07_dimsplit/HLL/EE2D, sides "
-                    "log-uniform [128,2048], t_end ~ U(1,20), 120 GB budget" % (n_req, rate, seed),
+        "workload": "%d requests, Poisson arrivals (seed %d) swept over %s per s, schemes KP07_dimsplit/HLL/EE2D, "
+                    "sides log-uniform [128,2048], t_end ~ U(1,20), 120 GB budget; top-level figures at the last "
+                    "rate" % (n_req, seed, "/".join("%.0f" % r for r in rates)),
+        "sweep": [{k: v for k, v in st.items() if k in ("arrival_rate_per_s", "cell_updates_per_s", "p50_latency_s",
+                                                        "p99_latency_s", "mean_latency_s", "elapsed_s",
+                                                        "host_seconds")} for st in sweep],
         "plain_one_at_a_time_cell_updates_per_s": plain_rate,
         "plain_sample_requests": plain_sample,
         "speedup_vs_plain": stats["cell_updates_per_s"] / plain_rate,
@@ -506,7 +521,8 @@ def run_mine(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_batched and scheme == SCHEME:
         result["batched"] = run_batched(ctx)
     if rank == 0 and world == 1 and not args.no_served and scheme == SCHEME:
-        result["served"] = run_served(ctx, n_req=args.served_requests, rate=args.served_rate)
+        result["served"] = run_served(ctx, n_req=args.served_requests,
+                                      rates=tuple(float(r) for r in args.served_rates.split(",")))
     if rank == 0 and world == 1 and not args.no_cpu_baseline and scheme == SCHEME:
         result["cpu_baseline"] = cpu_baseline_leg()
     return result
@@ -523,7 +539,9 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the 512-simulation batched workload")
     ap.add_argument("--no-served", action="store_true", help="skip the served request stream")
     ap.add_argument("--served-requests", type=int, default=400)
-    ap.add_argument("--served-rate", type=float, default=300.0, help="Poisson arrival rate (requests/s)")
+    ap.add_argument("--served-rates", default="300,3000",
+                    help="Poisson arrival rates (requests/s) of the served sweep, comma separated; the last one "
+                         "should saturate the server")
     ap.add_argument("--size", type=int, default=4096, help="grid side (the benchmark workload is 4096)")
     ap.add_argument("--scheme", default=SCHEME, help="scheme of the single-simulation timing (default KP07_dimsplit)")
     args = ap.parse_args()

@@ -11,11 +11,14 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/fvgpu.h"
@@ -154,20 +157,105 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 // Host replica of the reference's initial CFL estimate, in float32 with numpy's
 // NaN-propagating np.min (e.g. GPUSimulators/KP07_dimsplit.py:103-105).
-float initial_cfl(const float* const* v, size_t n, float dx, float dy, float c2) {
+
+// Initial CFL estimate of an uploaded state, computed on the device after the
+// upload: the reference's host formula min(dx / (|hu/h| + sqrt(g h)),
+// dy / (|hv/h| + sqrt(g h))) over every uploaded value (e.g.
+// GPUSimulators/KP07_dimsplit.py:102-106; EE2D uses gamma and rho,
+// EE2D_KP07_dimsplit.py:106-108), in IEEE FP32 with denormals kept (explicit
+// round-to-nearest PTX, not the fast-math operators), i.e. exactly what the
+// reference's NumPy float32 code computes.  A NaN anywhere along an axis makes
+// that axis' minimum NaN (NumPy's min); the two axes then combine with
+// Python's min.
+__device__ __forceinline__ float ieee_div(float a, float b) {
+    float d;
+    asm("div.rn.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+    return d;
+}
+__device__ __forceinline__ float ieee_mul(float a, float b) {
+    float d;
+    asm("mul.rn.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+    return d;
+}
+__device__ __forceinline__ float ieee_add(float a, float b) {
+    float d;
+    asm("add.rn.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+    return d;
+}
+__device__ __forceinline__ float ieee_sqrt(float a) {
+    float d;
+    asm("sqrt.rn.f32 %0, %1;" : "=f"(d) : "f"(a));
+    return d;
+}
+
+__global__ void cfl0_partial_kernel(const float* __restrict__ h, const float* __restrict__ hu,
+                                    const float* __restrict__ hv, int rows, int cols, int pitch, float dx, float dy,
+                                    float c2, float2* __restrict__ part) {
+    float mx = INFINITY, my = INFINITY;
+    int nan_x = 0, nan_y = 0;
+    const long long n = (long long)rows * cols;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(i / cols), c = (int)(i - (long long)r * cols);
+        const long long k = (long long)r * pitch + c;
+        const float hh = h[k];
+        const float cc = ieee_sqrt(ieee_mul(c2, hh));
+        const float ax = ieee_div(dx, ieee_add(fabsf(ieee_div(hu[k], hh)), cc));
+        const float ay = ieee_div(dy, ieee_add(fabsf(ieee_div(hv[k], hh)), cc));
+        if (isnan(ax)) nan_x = 1; else if (ax < mx) mx = ax;
+        if (isnan(ay)) nan_y = 1; else if (ay < my) my = ay;
+    }
+    __shared__ float rx[256 / 32], ry[256 / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fminf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        my = fminf(my, __shfl_xor_sync(0xffffffffu, my, o));
+    }
+    nan_x = __syncthreads_or(nan_x);
+    nan_y = __syncthreads_or(nan_y);
+    if ((threadIdx.x & 31) == 0) {
+        rx[threadIdx.x >> 5] = mx;
+        ry[threadIdx.x >> 5] = my;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+            mx = fminf(mx, rx[w]);
+            my = fminf(my, ry[w]);
+        }
+        part[blockIdx.x] = make_float2(nan_x ? NAN : mx, nan_y ? NAN : my);
+    }
+}
+
+// Combines the partial minima and seeds the control block: cfl_min = the
+// estimate, dt = the estimate (a simulator before simulate(),
+// EE2D_KP07_dimsplit.py:107) or dt = estimate * factor * cfl_scale (a batch
+// instance, whose first step is simulate()'s step 0).
+__global__ void cfl0_final_kernel(const float2* __restrict__ part, int n, SimCtl* ctl, int scaled) {
     float mx = INFINITY, my = INFINITY;
     bool nan_x = false, nan_y = false;
-    for (size_t i = 0; i < n; ++i) {
-        const float h = v[0][i];
-        const float c = std::sqrt(c2 * h);
-        const float ax = dx / (std::fabs(v[1][i] / h) + c);
-        const float ay = dy / (std::fabs(v[2][i] / h) + c);
-        if (std::isnan(ax)) nan_x = true; else if (ax < mx) mx = ax;
-        if (std::isnan(ay)) nan_y = true; else if (ay < my) my = ay;
+    for (int i = 0; i < n; ++i) {
+        const float2 p = part[i];
+        if (isnan(p.x)) nan_x = true; else if (p.x < mx) mx = p.x;
+        if (isnan(p.y)) nan_y = true; else if (p.y < my) my = p.y;
     }
     if (nan_x) mx = NAN;
     if (nan_y) my = NAN;
-    return (my < mx) ? my : mx;  // Python min(dt_x, dt_y)
+    const float cfl0 = (my < mx) ? my : mx;
+    ctl->cfl_min = cfl0;
+    ctl->dt = scaled ? ieee_mul(ieee_mul(cfl0, ctl->factor), ctl->cfl_scale) : cfl0;
+}
+
+// Queues the initial-CFL kernels on `st`; `scratch` holds at least
+// `max_parts` float2.
+int launch_initial_cfl(cudaStream_t st, const float* h, const float* hu, const float* hv, int rows, int cols,
+                       int pitch, float dx, float dy, float c2, float2* scratch, int max_parts, SimCtl* ctl,
+                       bool scaled) {
+    const long long n = (long long)rows * cols;
+    const int parts = (int)std::max<long long>(1, std::min<long long>({(n + 255) / 256, (long long)max_parts, 592}));
+    cfl0_partial_kernel<<<parts, 256, 0, st>>>(h, hu, hv, rows, cols, pitch, dx, dy, c2, scratch);
+    cfl0_final_kernel<<<1, 1, 0, st>>>(scratch, parts, ctl, scaled ? 1 : 0);
+    FV_CK(cudaGetLastError());
+    return FV_OK;
 }
 
 __global__ void sum_rows_kernel(const float* __restrict__ a, int nx, int pitch, double* __restrict__ out) {
@@ -198,10 +286,33 @@ __global__ void nan_scan_kernel(const float* __restrict__ a, long long n, int* _
 // Shared with the other translation units of the library (not exported).
 void fv_internal_set_error(const char* msg) { g_err = msg; }
 
+// Pinned host staging for copies between pageable host arrays and the device:
+// a pageable 2-D copy is staged by the driver row by row, while a pinned one is
+// a single DMA.  A ring of slots, each reusable once the copy through it has
+// completed (its event), serves all simulations and batches of a context.
+struct HostStaging {
+    static constexpr int kSlots = 4;
+    void* ptr[kSlots] = {nullptr, nullptr, nullptr, nullptr};
+    size_t cap[kSlots] = {0, 0, 0, 0};
+    cudaEvent_t ev[kSlots] = {nullptr, nullptr, nullptr, nullptr};
+    int next = 0;
+    std::mutex mu;
+    ~HostStaging() {
+        for (int k = 0; k < kSlots; ++k) {
+            if (ev[k]) {
+                cudaEventSynchronize(ev[k]);
+                cudaEventDestroy(ev[k]);
+            }
+            if (ptr[k]) cudaFreeHost(ptr[k]);
+        }
+    }
+};
+
 struct fv_context {
     int device = 0;
     int sm_count = 0;
     char name[256] = {0};
+    HostStaging staging;
 };
 
 struct fv_sim {
@@ -229,6 +340,100 @@ struct fv_sim {
 };
 
 namespace {
+
+bool is_pinned(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// rows x width bytes from src (row stride spitch) to dst (row stride dpitch),
+// split across up to 8 threads (one per 512 KB) for copies of 1 MB and more.
+void copy_rows(char* dst, size_t dpitch, const char* src, size_t spitch, size_t width, size_t rows) {
+    auto work = [=](size_t r0, size_t r1) {
+        if (dpitch == width && spitch == width) {
+            memcpy(dst + r0 * width, src + r0 * width, (r1 - r0) * width);
+        } else {
+            for (size_t r = r0; r < r1; ++r) memcpy(dst + r * dpitch, src + r * spitch, width);
+        }
+    };
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t bytes = width * rows;
+    const size_t nt = (bytes >= (1u << 20)) ? std::min<size_t>({8, hw, rows, bytes >> 19}) : 1;
+    if (nt <= 1) {
+        work(0, rows);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (size_t t = 1; t < nt; ++t) pool.emplace_back(work, rows * t / nt, rows * (t + 1) / nt);
+    work(0, rows / nt);
+    for (auto& th : pool) th.join();
+}
+
+// A staging slot of at least `bytes`, free of earlier copies; ctx->staging.mu must be held.
+int staging_slot(fv_context* ctx, size_t bytes, void** ptr, cudaEvent_t* ev) {
+    HostStaging& H = ctx->staging;
+    const int k = H.next;
+    H.next = (H.next + 1) % HostStaging::kSlots;
+    if (!H.ev[k]) {
+        FV_CK(cudaEventCreateWithFlags(&H.ev[k], cudaEventDisableTiming));
+    } else {
+        FV_CK(cudaEventSynchronize(H.ev[k]));
+    }
+    if (H.cap[k] < bytes) {
+        if (H.ptr[k]) cudaFreeHost(H.ptr[k]);
+        H.ptr[k] = nullptr;
+        H.cap[k] = 0;
+        const size_t cap = std::max<size_t>(bytes, 8u << 20);
+        if (cudaHostAlloc(&H.ptr[k], cap, cudaHostAllocPortable) != cudaSuccess)
+            return fail(FV_ERR_NOMEM, "cannot allocate %zu bytes of pinned staging memory", cap);
+        H.cap[k] = cap;
+    }
+    *ptr = H.ptr[k];
+    *ev = H.ev[k];
+    return FV_OK;
+}
+
+// Host (any memory) -> device 2-D copy queued on `st`; pageable sources go
+// through a staging slot.  Returns once the host array may be reused.
+int copy_h2d(fv_context* ctx, cudaStream_t st, float* dst, size_t dpitch, const float* src, size_t spitch,
+             size_t width, size_t rows) {
+    if (is_pinned(src)) {
+        FV_CK(cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, cudaMemcpyHostToDevice, st));
+        return FV_OK;
+    }
+    std::lock_guard<std::mutex> lock(ctx->staging.mu);
+    void* buf = nullptr;
+    cudaEvent_t ev = nullptr;
+    FV_TRY(staging_slot(ctx, width * rows, &buf, &ev));
+    copy_rows(static_cast<char*>(buf), width, reinterpret_cast<const char*>(src), spitch, width, rows);
+    FV_CK(cudaMemcpy2DAsync(dst, dpitch, buf, width, width, rows, cudaMemcpyHostToDevice, st));
+    FV_CK(cudaEventRecord(ev, st));
+    return FV_OK;
+}
+
+// Device -> host (any memory) 2-D copy ordered after the work queued on `st`;
+// returns when the host array holds the data.
+int copy_d2h(fv_context* ctx, cudaStream_t st, float* dst, size_t dpitch, const float* src, size_t spitch,
+             size_t width, size_t rows) {
+    if (is_pinned(dst)) {
+        FV_CK(cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, cudaMemcpyDeviceToHost, st));
+        FV_CK(cudaStreamSynchronize(st));
+        return FV_OK;
+    }
+    std::lock_guard<std::mutex> lock(ctx->staging.mu);
+    void* buf = nullptr;
+    cudaEvent_t ev = nullptr;
+    FV_TRY(staging_slot(ctx, width * rows, &buf, &ev));
+    FV_CK(cudaMemcpy2DAsync(buf, width, src, spitch, width, rows, cudaMemcpyDeviceToHost, st));
+    FV_CK(cudaEventRecord(ev, st));
+    FV_CK(cudaEventSynchronize(ev));
+    copy_rows(reinterpret_cast<char*>(dst), dpitch, static_cast<const char*>(buf), width, width, rows);
+    return FV_OK;
+}
 
 int read_ctl(fv_sim* s) {
     FV_CK(cudaMemcpyAsync(s->ctl_h, s->ctl, sizeof(SimCtl), cudaMemcpyDeviceToHost, s->stream));
@@ -327,6 +532,19 @@ int fv_context_create(int device, fv_context** out) {
     for (int i = 0; i < kNumEntries; ++i)
         FV_CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(kTable[i].fn),
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)entry_smem(kTable[i])));
+    // Device memory of finished simulations stays in the stream-ordered pool
+    // for the next ones instead of being unmapped at every synchronisation
+    // (the pool is trimmed when the context is destroyed).  Memory freed on
+    // one stream is reused on another only once the free has completed: an
+    // admission queued on a batch's copy stream must not wait for the
+    // compute stream's current chunk.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        int no = 0;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no);
+    }
     fv_context* c = new fv_context;
     c->device = device;
     c->sm_count = prop.multiProcessorCount;
@@ -336,6 +554,10 @@ int fv_context_create(int device, fv_context** out) {
 }
 
 int fv_context_destroy(fv_context* ctx) {
+    if (ctx) {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+    }
     delete ctx;
     return FV_OK;
 }
@@ -399,7 +621,8 @@ int fv_sim_create(fv_context* ctx, int scheme, int nx, int ny, float dx, float d
     const size_t plane = (size_t)(ny + 4) * s->pitch * sizeof(float);
     for (int b = 0; b < 2; ++b)
         for (int v = 0; v < nv; ++v) {
-            if (cudaMalloc(&s->buf[b][v], plane) != cudaSuccess) return cleanup(fail(FV_ERR_NOMEM, "out of device memory"));
+            if (cudaMallocAsync(&s->buf[b][v], plane, s->stream) != cudaSuccess)
+                return cleanup(fail(FV_ERR_NOMEM, "out of device memory"));
             if (cudaMemsetAsync(s->buf[b][v], 0, plane, s->stream) != cudaSuccess)
                 return cleanup(fail(FV_ERR_CUDA, "memset failed"));
         }
@@ -417,26 +640,30 @@ int fv_sim_create(fv_context* ctx, int scheme, int nx, int ny, float dx, float d
     const int off = halo ? gc : 0;
     for (int v = 0; v < nv; ++v) {
         float* dst = s->buf[0][v] + fv::cell_index(-off, -off, s->pitch);
-        if (cudaMemcpy2DAsync(dst, s->pitch * sizeof(float), host_vars[v], host_cols * sizeof(float),
-                              host_cols * sizeof(float), host_rows, cudaMemcpyHostToDevice, s->stream) != cudaSuccess)
-            return cleanup(fail(FV_ERR_CUDA, "upload failed"));
+        if (copy_h2d(ctx, s->stream, dst, s->pitch * sizeof(float), host_vars[v], host_cols * sizeof(float),
+                     host_cols * sizeof(float), host_rows) != FV_OK)
+            return cleanup(FV_ERR_CUDA);
     }
 
     // control block
     SimCtl& c = *s->ctl_h;
     memset(&c, 0, sizeof(SimCtl));
     const float c2 = (scheme == FV_EE2D_KP07_DIMSPLIT) ? params->gamma : params->g;
-    const float cfl0 = initial_cfl(host_vars, (size_t)host_rows * host_cols, dx, dy, c2);
     c.t = 0.0;
     c.t_end = 0.0;
     c.nt = 0;
-    c.dt = cfl0;  // as EE2D_KP07_dimsplit.py:107 (the other classes leave dt unset until simulate())
-    c.cfl_min = cfl0;
     c.factor = s->factor;
     c.cfl_scale = params->cfl_scale;
     c.update_dt = 1;
     c.cur = 0;
     if (write_ctl(s) != FV_OK) return cleanup(FV_ERR_CUDA);
+    // cfl_min and dt = the initial CFL estimate (dt as EE2D_KP07_dimsplit.py:107;
+    // the other classes leave dt unset until simulate())
+    if (launch_initial_cfl(s->stream, s->buf[0][0] + fv::cell_index(-off, -off, s->pitch),
+                           s->buf[0][1] + fv::cell_index(-off, -off, s->pitch),
+                           s->buf[0][2] + fv::cell_index(-off, -off, s->pitch), host_rows, host_cols, s->pitch, dx, dy,
+                           c2, reinterpret_cast<float2*>(s->block_sums), (int)(nblocks * 4), s->ctl, false) != FV_OK)
+        return cleanup(FV_ERR_CUDA);
 
     // kernel arguments and TMA descriptors
     StageArgs& a = s->args;
@@ -480,7 +707,7 @@ int fv_sim_destroy(fv_sim* s) {
     if (s->graph16) cudaGraphExecDestroy(s->graph16);
     for (int b = 0; b < 2; ++b)
         for (int v = 0; v < 4; ++v)
-            if (s->buf[b][v]) cudaFree(s->buf[b][v]);
+            if (s->buf[b][v]) cudaFreeAsync(s->buf[b][v], s->stream);
     if (s->ctl) cudaFree(s->ctl);
     if (s->ctl_h) cudaFreeHost(s->ctl_h);
     if (s->block_cfl) cudaFree(s->block_cfl);
@@ -573,10 +800,8 @@ int fv_sim_download(fv_sim* s, int var, float* host, int host_pitch) {
     if (var < 0 || var >= s->nv || !host || host_pitch < s->nx) return fail(FV_ERR_INVALID, "bad download argument");
     FV_TRY(read_ctl(s));
     const float* src = s->buf[s->ctl_h->cur][var] + fv::cell_index(0, 0, s->pitch);
-    FV_CK(cudaMemcpy2DAsync(host, (size_t)host_pitch * sizeof(float), src, (size_t)s->pitch * sizeof(float),
-                            (size_t)s->nx * sizeof(float), s->ny, cudaMemcpyDeviceToHost, s->stream));
-    FV_CK(cudaStreamSynchronize(s->stream));
-    return FV_OK;
+    return copy_d2h(s->ctx, s->stream, host, (size_t)host_pitch * sizeof(float), src, (size_t)s->pitch * sizeof(float),
+                    (size_t)s->nx * sizeof(float), s->ny);
 }
 
 int fv_sim_upload(fv_sim* s, int var, const float* host, int host_pitch) {
@@ -584,8 +809,8 @@ int fv_sim_upload(fv_sim* s, int var, const float* host, int host_pitch) {
     if (var < 0 || var >= s->nv || !host || host_pitch < s->nx) return fail(FV_ERR_INVALID, "bad upload argument");
     FV_TRY(read_ctl(s));
     float* dst = s->buf[s->ctl_h->cur][var] + fv::cell_index(0, 0, s->pitch);
-    FV_CK(cudaMemcpy2DAsync(dst, (size_t)s->pitch * sizeof(float), host, (size_t)host_pitch * sizeof(float),
-                            (size_t)s->nx * sizeof(float), s->ny, cudaMemcpyHostToDevice, s->stream));
+    FV_TRY(copy_h2d(s->ctx, s->stream, dst, (size_t)s->pitch * sizeof(float), host, (size_t)host_pitch * sizeof(float),
+                    (size_t)s->nx * sizeof(float), s->ny));
     FV_CK(cudaStreamSynchronize(s->stream));
     return FV_OK;
 }
@@ -1001,24 +1226,29 @@ int fv_batch_add(fv_batch* b, int nx, int ny, float dx, float dy, int bc, const 
         }
     const int off = halo ? gc : 0;
     for (int v = 0; v < b->nv; ++v)
-        FV_CK(cudaMemcpy2DAsync(I.buf[0][v] + fv::cell_index(-off, -off, pitch), pitch * sizeof(float), host_vars[v],
-                                host_cols * sizeof(float), host_cols * sizeof(float), host_rows, cudaMemcpyHostToDevice,
-                                b->copy_stream));
+        if (copy_h2d(b->ctx, b->copy_stream, I.buf[0][v] + fv::cell_index(-off, -off, pitch), pitch * sizeof(float),
+                     host_vars[v], host_cols * sizeof(float), host_cols * sizeof(float), host_rows) != FV_OK) {
+            cudaFreeAsync(mem, b->copy_stream);
+            return FV_ERR_CUDA;
+        }
     FV_CK(cudaEventRecord(b->ev_up, b->copy_stream));
     FV_CK(cudaStreamWaitEvent(b->stream, b->ev_up, 0));  // later kernels see the uploaded state
     SimCtl& c = b->h_ctl[s];
     memset(&c, 0, sizeof(c));
     const float c2 = (b->scheme == FV_EE2D_KP07_DIMSPLIT) ? b->p.gamma : b->p.g;
-    const float cfl0 = initial_cfl(host_vars, (size_t)host_rows * host_cols, dx, dy, c2);
     c.t_end = t_end;
-    c.cfl_min = cfl0;
     c.factor = b->factor;
     c.cfl_scale = b->p.cfl_scale;
     c.update_dt = 1;
-    c.dt = (cfl0 * c.factor) * c.cfl_scale;  // simulate() computes dt at step 0
     // From pinned staging (h_ctl, h_inst): asynchronous, ordered before the next kernels.
     FV_CK(cudaMemcpyAsync(b->d_ctl + s, &c, sizeof(SimCtl), cudaMemcpyHostToDevice, b->stream));
     FV_CK(cudaMemcpyAsync(b->d_inst + s, &I, sizeof(fv::BatchInstance), cudaMemcpyHostToDevice, b->stream));
+    // cfl_min = the initial CFL estimate, dt = estimate * factor * cfl_scale
+    // (simulate() computes dt at step 0), on the device once the upload landed
+    FV_TRY(launch_initial_cfl(b->stream, I.buf[0][0] + fv::cell_index(-off, -off, pitch),
+                              I.buf[0][1] + fv::cell_index(-off, -off, pitch),
+                              I.buf[0][2] + fv::cell_index(-off, -off, pitch), host_rows, host_cols, pitch, dx, dy, c2,
+                              reinterpret_cast<float2*>(I.block_sums), ntiles * 4, b->d_ctl + s, true));
     b->used[s] = 1;
     b->done_at_sync[s] = 0;
     b->slot_mem[s] = mem;
@@ -1115,11 +1345,9 @@ int fv_batch_download(fv_batch* b, int slot, int var, float* host, int host_pitc
     // A simulation that had reached t_end at the last sync is skipped by the
     // kernels queued since, so its state can be read while they run.
     const int cur = b->h_ctl[slot].cur;
-    FV_CK(cudaMemcpy2DAsync(host, (size_t)host_pitch * sizeof(float), I.buf[cur][var] + fv::cell_index(0, 0, I.pitch),
-                            (size_t)I.pitch * sizeof(float), (size_t)I.nx * sizeof(float), I.ny, cudaMemcpyDeviceToHost,
-                            b->copy_stream));
-    FV_CK(cudaStreamSynchronize(b->copy_stream));
-    return FV_OK;
+    return copy_d2h(b->ctx, b->copy_stream, host, (size_t)host_pitch * sizeof(float),
+                    I.buf[cur][var] + fv::cell_index(0, 0, I.pitch), (size_t)I.pitch * sizeof(float),
+                    (size_t)I.nx * sizeof(float), I.ny);
 }
 
 int fv_batch_info(fv_batch* b, size_t* device_bytes, int* active, int* work_items, double* last_run_ms) {
