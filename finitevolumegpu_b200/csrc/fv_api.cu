@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <condition_variable>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -288,15 +289,19 @@ void fv_internal_set_error(const char* msg) { g_err = msg; }
 
 // Pinned host staging for copies between pageable host arrays and the device:
 // a pageable 2-D copy is staged by the driver row by row, while a pinned one is
-// a single DMA.  A ring of slots, each reusable once the copy through it has
-// completed (its event), serves all simulations and batches of a context.
+// a single DMA.  A ring of slots serves all simulations and batches of a
+// context; a copy reserves a slot (the lock covers only the reservation, so
+// copies of different threads proceed in parallel), waits for the slot's
+// previous copy (its event) and releases the slot when done.
 struct HostStaging {
     static constexpr int kSlots = 4;
     void* ptr[kSlots] = {nullptr, nullptr, nullptr, nullptr};
     size_t cap[kSlots] = {0, 0, 0, 0};
     cudaEvent_t ev[kSlots] = {nullptr, nullptr, nullptr, nullptr};
+    bool busy[kSlots] = {false, false, false, false};
     int next = 0;
     std::mutex mu;
+    std::condition_variable freed;
     ~HostStaging() {
         for (int k = 0; k < kSlots; ++k) {
             if (ev[k]) {
@@ -373,11 +378,40 @@ void copy_rows(char* dst, size_t dpitch, const char* src, size_t spitch, size_t 
     for (auto& th : pool) th.join();
 }
 
-// A staging slot of at least `bytes`, free of earlier copies; ctx->staging.mu must be held.
-int staging_slot(fv_context* ctx, size_t bytes, void** ptr, cudaEvent_t* ev) {
+// A reserved staging slot of at least `bytes`, free of earlier copies; the
+// slot is released when the object goes out of scope.
+struct StagingSlot {
+    HostStaging* H = nullptr;
+    int k = -1;
+    void* ptr = nullptr;
+    cudaEvent_t ev = nullptr;
+    ~StagingSlot() {
+        if (k >= 0) {
+            std::lock_guard<std::mutex> lock(H->mu);
+            H->busy[k] = false;
+            H->freed.notify_one();
+        }
+    }
+};
+
+int staging_slot(fv_context* ctx, size_t bytes, StagingSlot& out) {
     HostStaging& H = ctx->staging;
-    const int k = H.next;
-    H.next = (H.next + 1) % HostStaging::kSlots;
+    int k = -1;
+    {
+        std::unique_lock<std::mutex> lock(H.mu);
+        for (;;) {
+            for (int i = 0; i < HostStaging::kSlots && k < 0; ++i) {
+                const int c = (H.next + i) % HostStaging::kSlots;
+                if (!H.busy[c]) k = c;
+            }
+            if (k >= 0) break;
+            H.freed.wait(lock);
+        }
+        H.busy[k] = true;
+        H.next = (k + 1) % HostStaging::kSlots;
+    }
+    out.H = &H;
+    out.k = k;
     if (!H.ev[k]) {
         FV_CK(cudaEventCreateWithFlags(&H.ev[k], cudaEventDisableTiming));
     } else {
@@ -392,8 +426,8 @@ int staging_slot(fv_context* ctx, size_t bytes, void** ptr, cudaEvent_t* ev) {
             return fail(FV_ERR_NOMEM, "cannot allocate %zu bytes of pinned staging memory", cap);
         H.cap[k] = cap;
     }
-    *ptr = H.ptr[k];
-    *ev = H.ev[k];
+    out.ptr = H.ptr[k];
+    out.ev = H.ev[k];
     return FV_OK;
 }
 
@@ -405,13 +439,11 @@ int copy_h2d(fv_context* ctx, cudaStream_t st, float* dst, size_t dpitch, const 
         FV_CK(cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, cudaMemcpyHostToDevice, st));
         return FV_OK;
     }
-    std::lock_guard<std::mutex> lock(ctx->staging.mu);
-    void* buf = nullptr;
-    cudaEvent_t ev = nullptr;
-    FV_TRY(staging_slot(ctx, width * rows, &buf, &ev));
-    copy_rows(static_cast<char*>(buf), width, reinterpret_cast<const char*>(src), spitch, width, rows);
-    FV_CK(cudaMemcpy2DAsync(dst, dpitch, buf, width, width, rows, cudaMemcpyHostToDevice, st));
-    FV_CK(cudaEventRecord(ev, st));
+    StagingSlot slot;
+    FV_TRY(staging_slot(ctx, width * rows, slot));
+    copy_rows(static_cast<char*>(slot.ptr), width, reinterpret_cast<const char*>(src), spitch, width, rows);
+    FV_CK(cudaMemcpy2DAsync(dst, dpitch, slot.ptr, width, width, rows, cudaMemcpyHostToDevice, st));
+    FV_CK(cudaEventRecord(slot.ev, st));
     return FV_OK;
 }
 
@@ -424,14 +456,12 @@ int copy_d2h(fv_context* ctx, cudaStream_t st, float* dst, size_t dpitch, const 
         FV_CK(cudaStreamSynchronize(st));
         return FV_OK;
     }
-    std::lock_guard<std::mutex> lock(ctx->staging.mu);
-    void* buf = nullptr;
-    cudaEvent_t ev = nullptr;
-    FV_TRY(staging_slot(ctx, width * rows, &buf, &ev));
-    FV_CK(cudaMemcpy2DAsync(buf, width, src, spitch, width, rows, cudaMemcpyDeviceToHost, st));
-    FV_CK(cudaEventRecord(ev, st));
-    FV_CK(cudaEventSynchronize(ev));
-    copy_rows(reinterpret_cast<char*>(dst), dpitch, static_cast<const char*>(buf), width, width, rows);
+    StagingSlot slot;
+    FV_TRY(staging_slot(ctx, width * rows, slot));
+    FV_CK(cudaMemcpy2DAsync(slot.ptr, width, src, spitch, width, rows, cudaMemcpyDeviceToHost, st));
+    FV_CK(cudaEventRecord(slot.ev, st));
+    FV_CK(cudaEventSynchronize(slot.ev));
+    copy_rows(reinterpret_cast<char*>(dst), dpitch, static_cast<const char*>(slot.ptr), width, width, rows);
     return FV_OK;
 }
 
@@ -961,6 +991,11 @@ struct fv_batch {
     cudaGraphExec_t graph1 = nullptr, graph16 = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0.0;
+    // Guards the slot bookkeeping (used, done_at_sync, slot_mem, bytes, dirty,
+    // h_inst, h_ctl reads) so that one host thread can return finished
+    // simulations (status, download, remove) while another admits and runs.
+    // Held only for short sections: never across copies or stream waits.
+    std::mutex mu;
 };
 
 namespace {
@@ -1168,12 +1203,22 @@ int fv_batch_add(fv_batch* b, int nx, int ny, float dx, float dy, int bc, const 
     for (int v = 0; v < b->nv; ++v)
         if (!host_vars[v]) return fail(FV_ERR_INVALID, "variable %d is null", v);
     int s = -1;
-    for (int i = 0; i < b->max_inst; ++i)
-        if (!b->used[i]) {
-            s = i;
-            break;
-        }
-    if (s < 0) return fail(FV_ERR_NOMEM, "batch is full (%d simulations)", b->max_inst);
+    {
+        std::lock_guard<std::mutex> lock(b->mu);
+        for (int i = 0; i < b->max_inst; ++i)
+            if (!b->used[i]) {
+                s = i;
+                break;
+            }
+        if (s < 0) return fail(FV_ERR_NOMEM, "batch is full (%d simulations)", b->max_inst);
+        b->used[s] = 1;  // reserved; joins the work list only when registered below
+        b->done_at_sync[s] = 0;
+    }
+    auto release = [&](int rc) {
+        std::lock_guard<std::mutex> lock(b->mu);
+        b->used[s] = 0;
+        return rc;
+    };
 
     const int W = b->be->W, H = b->be->H;
     const int pitch = ((nx + 8) + 31) / 32 * 32;
@@ -1186,9 +1231,12 @@ int fv_batch_add(fv_batch* b, int nx, int ny, float dx, float dy, int bc, const 
     void* mem = nullptr;
     if (cudaMallocAsync(&mem, total, b->copy_stream) != cudaSuccess) {
         cudaGetLastError();
-        return fail(FV_ERR_NOMEM, "out of device memory for a %d x %d simulation", nx, ny);
+        return release(fail(FV_ERR_NOMEM, "out of device memory for a %d x %d simulation", nx, ny));
     }
-    FV_CK(cudaMemsetAsync(mem, 0, total, b->copy_stream));
+    if (cudaMemsetAsync(mem, 0, total, b->copy_stream) != cudaSuccess) {
+        cudaFreeAsync(mem, b->copy_stream);
+        return release(fail(FV_ERR_CUDA, "memset failed"));
+    }
     fv::BatchInstance& I = b->h_inst[s];
     memset(&I, 0, sizeof(I));
     char* base = static_cast<char*>(mem);
@@ -1221,7 +1269,7 @@ int fv_batch_add(fv_batch* b, int nx, int ny, float dx, float dy, int bc, const 
                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
             if (r != CUDA_SUCCESS) {
                 cudaFreeAsync(mem, b->copy_stream);
-                return fail(FV_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+                return release(fail(FV_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r));
             }
         }
     const int off = halo ? gc : 0;
@@ -1229,8 +1277,9 @@ int fv_batch_add(fv_batch* b, int nx, int ny, float dx, float dy, int bc, const 
         if (copy_h2d(b->ctx, b->copy_stream, I.buf[0][v] + fv::cell_index(-off, -off, pitch), pitch * sizeof(float),
                      host_vars[v], host_cols * sizeof(float), host_cols * sizeof(float), host_rows) != FV_OK) {
             cudaFreeAsync(mem, b->copy_stream);
-            return FV_ERR_CUDA;
+            return release(FV_ERR_CUDA);
         }
+    std::lock_guard<std::mutex> lock(b->mu);
     FV_CK(cudaEventRecord(b->ev_up, b->copy_stream));
     FV_CK(cudaStreamWaitEvent(b->stream, b->ev_up, 0));  // later kernels see the uploaded state
     SimCtl& c = b->h_ctl[s];
@@ -1249,8 +1298,6 @@ int fv_batch_add(fv_batch* b, int nx, int ny, float dx, float dy, int bc, const 
                               I.buf[0][1] + fv::cell_index(-off, -off, pitch),
                               I.buf[0][2] + fv::cell_index(-off, -off, pitch), host_rows, host_cols, pitch, dx, dy, c2,
                               reinterpret_cast<float2*>(I.block_sums), ntiles * 4, b->d_ctl + s, true));
-    b->used[s] = 1;
-    b->done_at_sync[s] = 0;
     b->slot_mem[s] = mem;
     b->slot_bytes[s] = total;
     b->bytes += total;
@@ -1261,6 +1308,7 @@ int fv_batch_add(fv_batch* b, int nx, int ny, float dx, float dy, int bc, const 
 
 int fv_batch_remove(fv_batch* b, int slot) {
     FV_TRY(check_batch(b));
+    std::lock_guard<std::mutex> lock(b->mu);
     if (slot < 0 || slot >= b->max_inst || !b->used[slot]) return fail(FV_ERR_INVALID, "slot %d is not in use", slot);
     b->used[slot] = 0;
     b->dirty = true;  // leaves the work list at the next fv_batch_run
@@ -1275,6 +1323,7 @@ int fv_batch_remove(fv_batch* b, int slot) {
 int fv_batch_run(fv_batch* b, int n_steps) {
     FV_TRY(check_batch(b));
     if (n_steps < 0) return fail(FV_ERR_INVALID, "negative step count");
+    std::lock_guard<std::mutex> lock(b->mu);
     if (b->dirty) {
         FV_TRY(batch_publish(b));
         b->dirty = false;
@@ -1297,11 +1346,15 @@ int fv_batch_run(fv_batch* b, int n_steps) {
 
 int fv_batch_sync(fv_batch* b) {
     FV_TRY(check_batch(b));
-    FV_CK(cudaMemcpyAsync(b->h_ctl, b->d_ctl, (size_t)b->max_inst * sizeof(SimCtl), cudaMemcpyDeviceToHost,
-                          b->stream));
+    {
+        std::lock_guard<std::mutex> lock(b->mu);
+        FV_CK(cudaMemcpyAsync(b->h_ctl, b->d_ctl, (size_t)b->max_inst * sizeof(SimCtl), cudaMemcpyDeviceToHost,
+                              b->stream));
+    }
     int err = 0;
     FV_CK(cudaStreamSynchronize(b->stream));
     FV_CK(cudaMemcpy(&err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    std::lock_guard<std::mutex> lock(b->mu);
     for (int s = 0; s < b->max_inst; ++s) {
         if (!b->used[s]) continue;
         const SimCtl& c = b->h_ctl[s];
@@ -1317,7 +1370,9 @@ int fv_batch_sync(fv_batch* b) {
 }
 
 int fv_batch_status(fv_batch* b, int slot, double* t, long long* nt, float* dt, int* done) {
-    if (!b || slot < 0 || slot >= b->max_inst || !b->used[slot]) return fail(FV_ERR_INVALID, "slot not in use");
+    if (!b) return fail(FV_ERR_INVALID, "null batch");
+    std::lock_guard<std::mutex> lock(b->mu);
+    if (slot < 0 || slot >= b->max_inst || !b->used[slot]) return fail(FV_ERR_INVALID, "slot not in use");
     const SimCtl& c = b->h_ctl[slot];
     if (t) *t = c.t;
     if (nt) *nt = c.nt;
@@ -1332,26 +1387,40 @@ int fv_batch_status(fv_batch* b, int slot, double* t, long long* nt, float* dt, 
 
 int fv_batch_download(fv_batch* b, int slot, int var, float* host, int host_pitch) {
     FV_TRY(check_batch(b));
-    if (slot < 0 || slot >= b->max_inst || !b->used[slot] || var < 0 || var >= b->nv || !host)
-        return fail(FV_ERR_INVALID, "bad download argument");
-    const fv::BatchInstance& I = b->h_inst[slot];
-    if (host_pitch < I.nx) return fail(FV_ERR_INVALID, "host pitch too small");
-    if (!b->done_at_sync[slot]) {
+    int nx, ny, pitch, done;
+    float* bufs[2];
+    {
+        std::lock_guard<std::mutex> lock(b->mu);
+        if (slot < 0 || slot >= b->max_inst || !b->used[slot] || var < 0 || var >= b->nv || !host)
+            return fail(FV_ERR_INVALID, "bad download argument");
+        const fv::BatchInstance& I = b->h_inst[slot];
+        nx = I.nx;
+        ny = I.ny;
+        pitch = I.pitch;
+        bufs[0] = I.buf[0][var];
+        bufs[1] = I.buf[1][var];
+        done = b->done_at_sync[slot];
+    }
+    if (host_pitch < nx) return fail(FV_ERR_INVALID, "host pitch too small");
+    SimCtl c;
+    if (!done) {
         // still running at the last sync: include every kernel queued since
         FV_CK(cudaStreamSynchronize(b->stream));
-        FV_CK(cudaMemcpyAsync(b->h_ctl + slot, b->d_ctl + slot, sizeof(SimCtl), cudaMemcpyDeviceToHost, b->stream));
-        FV_CK(cudaStreamSynchronize(b->stream));
+        FV_CK(cudaMemcpy(&c, b->d_ctl + slot, sizeof(SimCtl), cudaMemcpyDeviceToHost));
+    } else {
+        // A simulation that had reached t_end at the last sync is skipped by the
+        // kernels queued since, so its state can be read while they run.
+        std::lock_guard<std::mutex> lock(b->mu);
+        c = b->h_ctl[slot];
     }
-    // A simulation that had reached t_end at the last sync is skipped by the
-    // kernels queued since, so its state can be read while they run.
-    const int cur = b->h_ctl[slot].cur;
     return copy_d2h(b->ctx, b->copy_stream, host, (size_t)host_pitch * sizeof(float),
-                    I.buf[cur][var] + fv::cell_index(0, 0, I.pitch), (size_t)I.pitch * sizeof(float),
-                    (size_t)I.nx * sizeof(float), I.ny);
+                    bufs[c.cur] + fv::cell_index(0, 0, pitch), (size_t)pitch * sizeof(float),
+                    (size_t)nx * sizeof(float), ny);
 }
 
 int fv_batch_info(fv_batch* b, size_t* device_bytes, int* active, int* work_items, double* last_run_ms) {
     if (!b) return fail(FV_ERR_INVALID, "null batch");
+    std::lock_guard<std::mutex> lock(b->mu);
     if (device_bytes) *device_bytes = b->bytes;
     if (active) {
         int n = 0;

@@ -10,12 +10,17 @@ while others run join the running batches at the next chunk boundary.
 
 Each scenario follows the reference's simulate(t_end) semantics on its own
 (see batch.py), so its result does not depend on what else is in the batch.
+Finished scenarios are downloaded and released by return threads, so
+host-to-device uploads of new requests and device-to-host reads of results
+overlap.
 """
 
 from __future__ import annotations
 
 import collections
 import dataclasses
+import queue
+import threading
 import time
 from typing import Dict, List, Optional
 
@@ -71,8 +76,9 @@ def state_bytes(scheme, nx, ny, tile_w=60, tile_h=28):
 
 class Server(object):
     def __init__(self, context, budget_bytes=120e9, chunk_steps=8, max_instances=4096, schemes=None,
-                 cfl_scale=0.9):
+                 cfl_scale=0.9, return_threads=3):
         self.context = context
+        self.return_threads = max(1, int(return_threads))
         self.budget = float(budget_bytes)
         self.chunk = int(chunk_steps)
         schemes = schemes or list(SCHEME_PARAMS)
@@ -85,74 +91,112 @@ class Server(object):
     def serve(self, requests: List[Request], clock=time.perf_counter):
         """Serve `requests` (arrival times relative to the call) until all are done.
 
-        Each iteration first queues the next chunk of steps for every batch
-        with running scenarios, then, while the GPU works, admits arrived
-        requests (their uploads run on a copy stream and they join the chunk
-        after) and downloads the scenarios that had finished at the previous
-        synchronisation (their state is final, so it is read while the chunk
-        runs); finally it waits for the chunk and looks for newly finished
-        scenarios.
+        The calling thread queues the next chunk of steps for every batch with
+        running scenarios, admits arrived requests while the budget allows
+        (their uploads run on each batch's copy stream and they join the chunk
+        after), then waits for the chunk and hands the scenarios that reached
+        t_end to the return threads.  These download and release them while the
+        calling thread queues and admits the next chunk: their state is final
+        (later chunks skip them), and their memory returns to the budget once
+        released.  Several return threads copy results out in parallel.
         """
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
-        running = {}  # (scheme, slot) -> (request, admitted, bytes)
-        finished = []  # keys that had reached t_end at the last synchronisation
+        running = {}  # (scheme, slot) -> (request, admitted, bytes): on the GPU, not yet at t_end
         results: List[Result] = []
-        t0 = clock()
-        busy_since = None
-        cells = 0
+        lock = threading.Lock()
+        returns = queue.Queue()
+        shared = {"cells": 0, "outstanding": 0, "error": None}
         timers = collections.Counter()
-        while pending or running:
-            # 1. queue the next chunk
-            done_set = set(finished)
-            active = {s for key in running if key not in done_set for s in (key[0],)}
-            ta = clock()
-            for s in active:
-                self.batches[s].run(self.chunk)
-            timers["queue"] += clock() - ta
-            if active and busy_since is None:
-                busy_since = ta - t0
-            # 2. admit arrived requests while the budget allows
-            ta = clock()
-            now = ta - t0
-            while pending and pending[0].arrival <= now:
-                r = pending[0]
-                need = state_bytes(r.scheme, r.nx, r.ny)
-                if self.used + need > self.budget:
-                    break
+        t0 = clock()
+
+        def return_finished():
+            while True:
+                item = returns.get()
+                if item is None:
+                    return
+                (s, slot), r, admitted, need = item
+                ta = clock()
                 try:
-                    slot = self.batches[r.scheme].add(r.variables, r.nx, r.ny, r.dx, r.dy, r.t_end,
-                                                      r.boundary_conditions)
-                except MemoryError:
+                    b = self.batches[s]
+                    st = b.status(slot)
+                    state = b.download(slot)
+                    b.remove(slot)
+                except Exception as e:  # reported by serve()
+                    with lock:
+                        shared["error"] = e
+                        shared["outstanding"] -= 1
+                    continue
+                done = clock() - t0
+                with lock:
+                    self.used -= need
+                    results.append(Result(r.rid, s, state, st["nt"], st["t"], r.arrival, admitted, done))
+                    shared["cells"] += r.nx * r.ny * st["nt"]
+                    shared["outstanding"] -= 1
+                    timers["return"] += clock() - ta
+
+        workers = [threading.Thread(target=return_finished, name="fvgpu-return-%d" % k, daemon=True)
+                   for k in range(self.return_threads)]
+        for w in workers:
+            w.start()
+        busy_since = None
+        try:
+            while True:
+                with lock:
+                    outstanding = shared["outstanding"]
+                    if shared["error"] is not None:
+                        raise shared["error"]
+                if not (pending or running or outstanding):
                     break
-                pending.popleft()
-                self.used += need
-                running[(r.scheme, slot)] = (r, clock() - t0, need)
-            timers["admit"] += clock() - ta
-            # 3. return the scenarios that finished at the last synchronisation
-            ta = clock()
-            for key in finished:
-                s, slot = key
-                r, admitted, need = running.pop(key)
-                st = self.batches[s].status(slot)
-                state = self.batches[s].download(slot)
-                self.batches[s].remove(slot)
-                self.used -= need
-                results.append(Result(r.rid, s, state, st["nt"], st["t"], r.arrival, admitted, clock() - t0))
-                cells += r.nx * r.ny * st["nt"]
-            finished = []
-            timers["return"] += clock() - ta
-            # 4. wait for the chunk and find the scenarios that are done
-            ta = clock()
-            for s in active:
-                self.batches[s].sync()
-            for key in running:
-                if key[0] in active and self.batches[key[0]].status(key[1])["done"]:
-                    finished.append(key)
-            timers["wait"] += clock() - ta
-            if not active and not finished and pending and not running:
-                wait = pending[0].arrival - (clock() - t0)
-                if wait > 0:
-                    time.sleep(min(wait, 0.005))
+                # 1. queue the next chunk
+                active = {key[0] for key in running}
+                ta = clock()
+                for s in active:
+                    self.batches[s].run(self.chunk)
+                timers["queue"] += clock() - ta
+                if active and busy_since is None:
+                    busy_since = ta - t0
+                # 2. admit arrived requests while the budget allows
+                ta = clock()
+                now = ta - t0
+                while pending and pending[0].arrival <= now:
+                    r = pending[0]
+                    need = state_bytes(r.scheme, r.nx, r.ny)
+                    with lock:
+                        if self.used + need > self.budget:
+                            break
+                    try:
+                        slot = self.batches[r.scheme].add(r.variables, r.nx, r.ny, r.dx, r.dy, r.t_end,
+                                                          r.boundary_conditions)
+                    except MemoryError:
+                        break
+                    pending.popleft()
+                    with lock:
+                        self.used += need
+                    running[(r.scheme, slot)] = (r, clock() - t0, need)
+                timers["admit"] += clock() - ta
+                # 3. wait for the chunk; hand the scenarios at t_end to the return thread
+                ta = clock()
+                for s in active:
+                    self.batches[s].sync()
+                for key in [k for k in running if k[0] in active]:
+                    if self.batches[key[0]].status(key[1])["done"]:
+                        r, admitted, need = running.pop(key)
+                        with lock:
+                            shared["outstanding"] += 1
+                        returns.put((key, r, admitted, need))
+                timers["wait"] += clock() - ta
+                if not active:
+                    # nothing on the GPU: wait for the next arrival or for returns to free memory
+                    wait = (pending[0].arrival - (clock() - t0)) if pending else 0.001
+                    time.sleep(min(max(wait, 0.0005), 0.005))
+        finally:
+            for _ in workers:
+                returns.put(None)
+            for w in workers:
+                w.join()
+        if shared["error"] is not None:
+            raise shared["error"]
+        cells = shared["cells"]
         elapsed = clock() - t0
         lat = np.array([r.latency for r in results]) if results else np.zeros(1)
         stats = {
