@@ -31,8 +31,8 @@ TILE_CONFIGS = {
     "FORCE": 2,
     "HLL": 3,
     "EE2D_KP07_dimsplit": 3,
-    "LxF": 2,
-    "KP07": 2,
+    "LxF": 3,
+    "KP07": 3,
 }
 # Tile configurations of the batched (persistent) kernels per scheme.
 BATCH_TILE_CONFIGS = {

@@ -83,10 +83,12 @@ const KEntry kTable[] = {
     {FV_EE2D_KP07_DIMSPLIT, 124, 28, 128, true, fv::dimsplit_stage_kernel<fv::EE2D, 124, 28, 128>},
     {FV_EE2D_KP07_DIMSPLIT, 124, 60, 256, true, fv::dimsplit_stage_kernel<fv::EE2D, 124, 60, 256>},
     {FV_EE2D_KP07_DIMSPLIT, 60, 28, 128, true, fv::dimsplit_stage_kernel<fv::EE2D, 60, 28, 128>},
-    {FV_LXF, 124, 28, 256, false, fv::unsplit_stage_kernel<fv::LXF, 124, 28, 256>},
-    {FV_LXF, 124, 12, 256, false, fv::unsplit_stage_kernel<fv::LXF, 124, 12, 256>},
-    {FV_KP07, 124, 28, 256, false, fv::unsplit_stage_kernel<fv::KP07, 124, 28, 256>},
-    {FV_KP07, 124, 12, 256, false, fv::unsplit_stage_kernel<fv::KP07, 124, 12, 256>},
+    {FV_LXF, 120, 60, 256, false, fv::unsplit_stage_kernel<fv::LXF, 120, 60, 256>},
+    {FV_LXF, 120, 28, 128, false, fv::unsplit_stage_kernel<fv::LXF, 120, 28, 128>},
+    {FV_LXF, 120, 60, 128, false, fv::unsplit_stage_kernel<fv::LXF, 120, 60, 128>},
+    {FV_KP07, 120, 28, 128, false, fv::unsplit_stage_kernel<fv::KP07, 120, 28, 128>},
+    {FV_KP07, 120, 60, 128, false, fv::unsplit_stage_kernel<fv::KP07, 120, 60, 128>},
+    {FV_KP07, 120, 60, 256, false, fv::unsplit_stage_kernel<fv::KP07, 120, 60, 256>},
 };
 constexpr int kNumEntries = sizeof(kTable) / sizeof(kTable[0]);
 
@@ -130,8 +132,7 @@ const BEntry* find_batch_entry(int scheme, int cfg) {
 
 size_t entry_smem(const KEntry& e) {
     const size_t tile = (size_t)(e.W + 8) * (e.H + 4) * sizeof(float);
-    if (e.split) return scheme_nv(e.scheme) * tile;
-    return 3 * tile + 3 * (size_t)e.H * (e.W + 1) * sizeof(float);
+    return scheme_nv(e.scheme) * tile;
 }
 
 const KEntry* find_entry(int scheme, int cfg) {

@@ -822,19 +822,37 @@ __global__ void __launch_bounds__(NT) batched_stage_kernel(const __grid_constant
 
 // ------------------------------------------------------------------ unsplit stage kernel (LxF, KP07)
 
-// Phase 1 computes the x-face fluxes of the interior rows into shared memory
-// (lanes along x); phase 2 walks columns, computes the y-face fluxes on the fly
-// and writes the updated cells straight to global memory
-// (GPUSimulators/cuda/SWE2D_LxF.cu:137-153, SWE2D_KP07.cu:187-225).
+__device__ __forceinline__ SweFace shfl_up_face(const SweFace& f, int d) {
+    SweFace r;
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+        r.q[v] = __shfl_up_sync(0xffffffffu, f.q[v], d);
+        r.f[v] = __shfl_up_sync(0xffffffffu, f.f[v], d);
+    }
+    r.u = __shfl_up_sync(0xffffffffu, f.u, d);
+    r.c = __shfl_up_sync(0xffffffffu, f.c, d);
+    return r;
+}
+
+// One pass over the tile, as column walkers (GPUSimulators/cuda/SWE2D_LxF.cu:102-165,
+// SWE2D_KP07.cu:136-232).  Lanes run along x: warp column wx of a row segment
+// covers tile columns 3+30wx .. 34+30wx; lanes 1..30 update interior columns
+// 30wx .. 30wx+29, lanes 0 and 31 supply the states of the columns beside
+// them.  At each row a lane builds the west and east face states of its cell;
+// the flux at its west face takes the east state of the lane to its left
+// (warp shuffle), and its east-face flux is the west-face flux of the lane
+// to its right, so each x face is computed once.  Along y each lane keeps a
+// sliding window: the north face state of the row above and the flux at the
+// south face carry over from the previous row.  The updated cells (KP07
+// stage 2 blended with the old output) go straight to global memory.
 template <int SCHEME, int W, int H, int NT>
 __global__ void __launch_bounds__(NT) unsplit_stage_kernel(const __grid_constant__ StageArgs A) {
     constexpr int SP = W + 8, TR = H + 4, PS = SP * TR;
-    constexpr int FW = W + 1;            // faces per row
-    constexpr int NSEG = NT / W, R = H / NSEG;
-    static_assert(NSEG >= 1 && H % NSEG == 0, "column segments must tile the block");
+    constexpr int WX = W / 30, NSEG = NT / (32 * WX), R = H / NSEG;
+    static_assert(W % 30 == 0 && NT % (32 * WX) == 0 && NSEG >= 1 && H % NSEG == 0,
+                  "warps of 30 updated columns must tile the block");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     float* Qs = reinterpret_cast<float*>(smem_raw);
-    float* Fs = Qs + 3 * PS;  // [3][H][FW]
     __shared__ __align__(8) uint64_t bar;
 
     const StepCtl sc = read_step(A);
@@ -859,116 +877,126 @@ __global__ void __launch_bounds__(NT) unsplit_stage_kernel(const __grid_constant
         const float kdt = sc.dt * A.dt_scale;
         const float g = A.g, half_g = 0.5f * g, theta = A.theta;
         const float k4x = A.dx / (4.0f * kdt), k4y = A.dy / (4.0f * kdt);
-
-        // phase 1: x faces; face f of row r lies between tile columns 3+f and 4+f.
-        for (int i = threadIdx.x; i < H * FW; i += NT) {
-            const int r = i / FW, f = i - r * FW;
-            const float* row = Qs + (r + 2) * SP;
-            float F[3];
-            if (SCHEME == LXF) {
-                const SweFace l = swe_face(row[3 + f], row[PS + 3 + f], row[2 * PS + 3 + f], g, half_g);
-                const SweFace rr = swe_face(row[4 + f], row[PS + 4 + f], row[2 * PS + 4 + f], g, half_g);
-                swe_lxf_2d(l, rr, k4x, F);
-            } else {
-                float qm[3], qp[3];
-#pragma unroll
-                for (int v = 0; v < 3; ++v) {
-                    const float* c = row + v * PS + 3 + f;
-                    qm[v] = fmaf(0.5f, minmod_slope(c[-1], c[0], c[1], theta), c[0]);
-                    qp[v] = fmaf(-0.5f, minmod_slope(c[0], c[1], c[2], theta), c[1]);
-                }
-                const SweFace l = swe_face(qm[0], qm[1], qm[2], g, half_g);
-                const SweFace rr = swe_face(qp[0], qp[1], qp[2], g, half_g);
-                swe_central_upwind(l, rr, F);
-            }
-#pragma unroll
-            for (int v = 0; v < 3; ++v) Fs[(v * H + r) * FW + f] = F[v];
-        }
-        __syncthreads();
-
-        // phase 2: one column segment per thread
+        const float kdx = kdt / A.dx, kdy = kdt / A.dy;
         const int out = sc.cur ^ 1;
         const bool blend = (SCHEME == KP07) && A.order == 2 && A.substep == 1;
-        const int item = threadIdx.x;
-        if (item < W * NSEG) {
-            const int i = item % W, seg = item / W;
-            const int x = x0 + i;
-            const int s = 4 + i;
-            const int a = 2 + seg * R, b = a + R;  // tile rows updated
-            const float kdx = kdt / A.dx, kdy = kdt / A.dy;
-            // y-face state of row m toward north (n) and toward south (s), swapped (h, hv, hu)
-            auto qcell = [&](int t, float (&q)[3]) {
-                q[0] = Qs[t * SP + s];
-                q[1] = Qs[2 * PS + t * SP + s];
-                q[2] = Qs[PS + t * SP + s];
-            };
-            SweFace north_prev;  // north face state of row m-1
-            auto face_states = [&](int t, SweFace& sface, SweFace& nface) {
+
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int wx = warp % WX, seg = warp / WX;
+        const int s = 3 + 30 * wx + lane;  // tile column of this lane
+        const int x = x0 + s - 4;          // domain column
+        const bool owner = lane >= 1 && lane <= 30;
+        const int a = 2 + seg * R, b = a + R;  // tile rows updated by this segment
+
+        // q of tile cell (t, c), components in (h, hu, hv) order
+        auto qat = [&](int t, int c, float (&q)[3]) {
+#pragma unroll
+            for (int v = 0; v < 3; ++v) q[v] = Qs[v * PS + t * SP + c];
+        };
+        // y-face states of row t (south, north) from rows t-1, t, t+1 of this
+        // column, components swapped to (h, hv, hu) as computeFluxG does
+        // (GPUSimulators/cuda/SWE2D_KP07.cu:117-131)
+        auto ystates = [&](const float (&qm)[3], const float (&q0)[3], const float (&qp)[3], SweFace& sf,
+                           SweFace& nf) {
+            float sv[3], nv[3];
+#pragma unroll
+            for (int v = 0; v < 3; ++v) {
+                const int k = (v == 0) ? 0 : 3 - v;  // (h, hv, hu)
                 if (SCHEME == LXF) {
-                    float q[3];
-                    qcell(t, q);
-                    sface = nface = swe_face(q[0], q[1], q[2], g, half_g);
+                    sv[v] = nv[v] = q0[k];
                 } else {
-                    float qm[3], q0[3], qp[3], sv[3], nv[3];
-                    qcell(t - 1, qm);
-                    qcell(t, q0);
-                    qcell(t + 1, qp);
-#pragma unroll
-                    for (int v = 0; v < 3; ++v) {
-                        const float sl = minmod_slope(qm[v], q0[v], qp[v], theta);
-                        sv[v] = fmaf(-0.5f, sl, q0[v]);
-                        nv[v] = fmaf(0.5f, sl, q0[v]);
-                    }
-                    sface = swe_face(sv[0], sv[1], sv[2], g, half_g);
-                    nface = swe_face(nv[0], nv[1], nv[2], g, half_g);
+                    const float sl = minmod_slope(qm[k], q0[k], qp[k], theta);
+                    sv[v] = fmaf(-0.5f, sl, q0[k]);
+                    nv[v] = fmaf(0.5f, sl, q0[k]);
                 }
-            };
-            auto yflux = [&](const SweFace& l, const SweFace& r, float (&Gf)[3]) {
-                float tmp[3];
-                if (SCHEME == LXF) swe_lxf_2d(l, r, k4y, tmp);
-                else swe_central_upwind(l, r, tmp);
-                Gf[0] = tmp[0];  // swap back to (h, hu, hv)
-                Gf[1] = tmp[2];
-                Gf[2] = tmp[1];
-            };
-            {
-                SweFace sdummy;
-                face_states(a - 1, sdummy, north_prev);
             }
-            SweFace s_cur, n_cur;
-            face_states(a, s_cur, n_cur);
-            float Gs[3];
-            yflux(north_prev, s_cur, Gs);  // south face of row a
-            for (int t = a; t < b; ++t) {
-                SweFace s_nxt, n_nxt;
-                face_states(t + 1, s_nxt, n_nxt);
-                float Gn[3];
-                yflux(n_cur, s_nxt, Gn);  // north face of row t
-                const int y = y0 + t - 2;
-                const int r = t - 2;
-                if (x < A.nx && y < A.ny) {
-                    float qn[3];
-                    const long long gi = cell_index(y, x, A.pitch);
+            sf = swe_face(sv[0], sv[1], sv[2], g, half_g);
+            nf = (SCHEME == LXF) ? sf : swe_face(nv[0], nv[1], nv[2], g, half_g);
+        };
+        auto yflux = [&](const SweFace& l, const SweFace& r, float (&G)[3]) {
+            float tmp[3];
+            if (SCHEME == LXF) swe_lxf_2d(l, r, k4y, tmp);
+            else swe_central_upwind(l, r, tmp);
+            G[0] = tmp[0];  // back to (h, hu, hv)
+            G[1] = tmp[2];
+            G[2] = tmp[1];
+        };
+
+        // window: rows a-1, a, a+1 of this column
+        float qm[3], q0[3], qp[3];
+        qat(a - 1, s, qm);
+        qat(a, s, q0);
+        qat(a + 1, s, qp);
+        SweFace s_cur, n_cur, n_prev;
+        {
+            float qmm[3];
+            qat(a - 2, s, qmm);
+            SweFace sd;
+            ystates(qmm, qm, q0, sd, n_prev);  // row a-1
+        }
+        ystates(qm, q0, qp, s_cur, n_cur);  // row a
+        float Gs[3];
+        yflux(n_prev, s_cur, Gs);  // south face of row a
+        for (int t = a; t < b; ++t) {
+            const int y = y0 + t - 2;
+            const bool store = owner && x < A.nx && y < A.ny;
+            const long long gi = cell_index(y, x, A.pitch);
+            float old[3] = {0.0f, 0.0f, 0.0f};
+            if (blend && store) {
 #pragma unroll
-                    for (int v = 0; v < 3; ++v) {
-                        const float q = Qs[v * PS + t * SP + s];
-                        const float Fw = Fs[(v * H + r) * FW + i], Fe = Fs[(v * H + r) * FW + i + 1];
-                        qn[v] = q + fmaf(Fw - Fe, kdx, (Gs[v] - Gn[v]) * kdy);
-                    }
+                for (int v = 0; v < 3; ++v) old[v] = A.buf[out][v][gi];
+            }
+            // x faces of (t, s): west and east states
+            SweFace fw, fe;
+            if (SCHEME == LXF) {
+                fw = fe = swe_face(q0[0], q0[1], q0[2], g, half_g);
+            } else {
+                float ql[3], qr[3], wv[3], ev[3];
+                qat(t, s - 1, ql);
+                qat(t, s + 1, qr);
 #pragma unroll
-                    for (int v = 0; v < 3; ++v) {
-                        float* dst = A.buf[out][v] + gi;
-                        const float o = blend ? 0.5f * (*dst + qn[v]) : qn[v];
-                        *dst = o;
-                        if (sums) my_sums[v] += (double)o;
-                    }
-                    if (sc.do_cfl) my_cfl = fminf(my_cfl, cell_cfl(qn[0], qn[1], qn[2], A.dx, A.dy, g));
+                for (int v = 0; v < 3; ++v) {
+                    const float sl = minmod_slope(ql[v], q0[v], qr[v], theta);
+                    wv[v] = fmaf(-0.5f, sl, q0[v]);
+                    ev[v] = fmaf(0.5f, sl, q0[v]);
                 }
-#pragma unroll
-                for (int v = 0; v < 3; ++v) Gs[v] = Gn[v];
-                s_cur = s_nxt;
-                n_cur = n_nxt;
+                fw = swe_face(wv[0], wv[1], wv[2], g, half_g);
+                fe = swe_face(ev[0], ev[1], ev[2], g, half_g);
             }
+            const SweFace le = shfl_up_face(fe, 1);  // east state of the column to the left
+            float Fw[3], Fe[3];
+            if (SCHEME == LXF) swe_lxf_2d(le, fw, k4x, Fw);
+            else swe_central_upwind(le, fw, Fw);
+#pragma unroll
+            for (int v = 0; v < 3; ++v) Fe[v] = __shfl_down_sync(0xffffffffu, Fw[v], 1);
+            // y: states of row t+1, flux at the north face of row t
+            float qn2[3];
+            qat(t + 2, s, qn2);
+            SweFace s_nxt, n_nxt;
+            ystates(q0, qp, qn2, s_nxt, n_nxt);
+            float Gn[3];
+            yflux(n_cur, s_nxt, Gn);
+            if (store) {
+                float qn[3];
+#pragma unroll
+                for (int v = 0; v < 3; ++v) qn[v] = q0[v] + fmaf(Fw[v] - Fe[v], kdx, (Gs[v] - Gn[v]) * kdy);
+#pragma unroll
+                for (int v = 0; v < 3; ++v) {
+                    const float o = blend ? 0.5f * (old[v] + qn[v]) : qn[v];
+                    A.buf[out][v][gi] = o;
+                    if (sums) my_sums[v] += (double)o;
+                }
+                if (sc.do_cfl) my_cfl = fminf(my_cfl, cell_cfl(qn[0], qn[1], qn[2], A.dx, A.dy, g));
+            }
+#pragma unroll
+            for (int v = 0; v < 3; ++v) {
+                Gs[v] = Gn[v];
+                qm[v] = q0[v];
+                q0[v] = qp[v];
+                qp[v] = qn2[v];
+            }
+            s_cur = s_nxt;
+            n_cur = n_nxt;
         }
     }
     stage_epilogue<NT, 3>(A, sc, my_cfl, my_sums, sums);
