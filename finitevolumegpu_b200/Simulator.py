@@ -319,6 +319,19 @@ class BaseSimulator(object):
     def dt(self):
         return self._time()[2]
 
+    def get_control(self):
+        """(t, nt, dt, cfl_min): the time-stepping state a checkpoint stores."""
+        t, nt = ctypes.c_double(), ctypes.c_longlong()
+        dt, cfl = ctypes.c_float(), ctypes.c_float()
+        _lib.check(_lib.lib().fv_sim_get_control(self._handle, ctypes.byref(t), ctypes.byref(nt), ctypes.byref(dt),
+                                                 ctypes.byref(cfl)))
+        return t.value, nt.value, np.float32(dt.value), np.float32(cfl.value)
+
+    def set_control(self, t, nt, dt, cfl_min):
+        """Restore the time-stepping state saved by get_control (checkpoint resume)."""
+        _lib.check(_lib.lib().fv_sim_set_control(self._handle, float(t), int(nt), float(np.float32(dt)),
+                                                 float(np.float32(cfl_min))))
+
     def getExtent(self):
         return [0, 0, self.nx * self.dx, self.ny * self.dy]
 

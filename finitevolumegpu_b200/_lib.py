@@ -77,6 +77,9 @@ _SIGNATURES = {
     "fv_sim_check": ([_P, ctypes.POINTER(_I)], _I),
     "fv_sim_synchronize": ([_P], _I),
     "fv_sim_set_boundary_conditions": ([_P, _I], _I),
+    "fv_sim_get_control": ([_P, ctypes.POINTER(_D), ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_float),
+                            ctypes.POINTER(ctypes.c_float)], _I),
+    "fv_sim_set_control": ([_P, _D, ctypes.c_longlong, ctypes.c_float, ctypes.c_float], _I),
     "fv_sim_buffers": ([_P, ctypes.POINTER(_FP), ctypes.POINTER(_I), ctypes.POINTER(_I)], _I),
     "fv_sim_stream": ([_P, ctypes.POINTER(_P)], _I),
     "fv_sim_info": ([_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)], _I),

@@ -905,6 +905,27 @@ int fv_sim_set_boundary_conditions(fv_sim* s, int bc) {
     return FV_OK;
 }
 
+int fv_sim_get_control(fv_sim* s, double* t, long long* nt, float* dt, float* cfl_min) {
+    FV_TRY(check_sim(s));
+    FV_TRY(read_ctl(s));
+    if (t) *t = s->ctl_h->t;
+    if (nt) *nt = s->ctl_h->nt;
+    if (dt) *dt = s->ctl_h->dt;
+    if (cfl_min) *cfl_min = s->ctl_h->cfl_min;
+    return FV_OK;
+}
+
+int fv_sim_set_control(fv_sim* s, double t, long long nt, float dt, float cfl_min) {
+    FV_TRY(check_sim(s));
+    if (nt < 0) return fail(FV_ERR_INVALID, "negative step count");
+    FV_TRY(read_ctl(s));
+    s->ctl_h->t = t;
+    s->ctl_h->nt = nt;
+    s->ctl_h->dt = dt;
+    s->ctl_h->cfl_min = cfl_min;
+    return write_ctl(s);
+}
+
 int fv_sim_buffers(fv_sim* s, float** ptrs, int* pitch, int* cur) {
     FV_TRY(check_sim(s));
     if (!ptrs || !pitch || !cur) return fail(FV_ERR_INVALID, "bad argument");

@@ -135,6 +135,15 @@ FV_API int fv_sim_synchronize(fv_sim* sim);
 /* setBoundaryConditions (Simulator.py:245-247). */
 FV_API int fv_sim_set_boundary_conditions(fv_sim* sim, int bc);
 
+/* Time-stepping state of a simulation: simulated time t, steps nt, the
+ * current time step dt and the last CFL minimum (from which simulate()
+ * derives dt every 100 steps).  get/set let a caller checkpoint a simulation
+ * and resume it later with the same continuation; no reference counterpart
+ * (the reference keeps t, nt and dt as Python attributes,
+ * GPUSimulators/Simulator.py:139-143, and has no resume). */
+FV_API int fv_sim_get_control(fv_sim* sim, double* t, long long* nt, float* dt, float* cfl_min);
+FV_API int fv_sim_set_control(fv_sim* sim, double t, long long nt, float dt, float cfl_min);
+
 /* Device state of a simulation for halo exchange between row stripes
  * (replaces the PyCUDA array access of MPISimulator.full_exchange,
  * GPUSimulators/MPISimulator.py:371-480).  ptrs[b * 4 + v] receives the base
