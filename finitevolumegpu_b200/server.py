@@ -29,9 +29,13 @@ import numpy as np
 from .batch import Batch
 from .Simulator import BoundaryCondition
 
+# Default physical parameters per scheme; a request may set its own g and gamma.
 SCHEME_PARAMS = {
-    "KP07_dimsplit": dict(g=9.81),
-    "HLL": dict(g=9.81),
+    "KP07_dimsplit": dict(g=9.81, gamma=1.4),
+    "HLL": dict(g=9.81, gamma=1.4),
+    "HLL2": dict(g=9.81, gamma=1.4),
+    "WAF": dict(g=9.81, gamma=1.4),
+    "FORCE": dict(g=9.81, gamma=1.4),
     "EE2D_KP07_dimsplit": dict(g=0.0, gamma=1.4),
 }
 
@@ -48,6 +52,13 @@ class Request:
     t_end: float
     arrival: float = 0.0  # seconds after the start of serve()
     boundary_conditions: Optional[BoundaryCondition] = None
+    g: Optional[float] = None      # gravity; None: the scheme's default (SCHEME_PARAMS)
+    gamma: Optional[float] = None  # ratio of specific heats (Euler); None: the default
+
+    def batch_key(self):
+        d = SCHEME_PARAMS[self.scheme]
+        return (self.scheme, float(d["g"] if self.g is None else self.g),
+                float(d["gamma"] if self.gamma is None else self.gamma))
 
 
 @dataclasses.dataclass
@@ -81,12 +92,21 @@ class Server(object):
         self.return_threads = max(1, int(return_threads))
         self.budget = float(budget_bytes)
         self.chunk = int(chunk_steps)
-        schemes = schemes or list(SCHEME_PARAMS)
-        self.batches: Dict[str, Batch] = {
-            s: Batch(context, s, cfl_scale=cfl_scale, max_instances=max_instances, **SCHEME_PARAMS[s])
-            for s in schemes
-        }
+        self.cfl_scale = cfl_scale
+        self.max_instances = max_instances
+        # one batch per (scheme, g, gamma), created when a request first needs it
+        self.batches: Dict[tuple, Batch] = {}
+        for s in (schemes or ("KP07_dimsplit", "HLL", "EE2D_KP07_dimsplit")):
+            self._batch((s, float(SCHEME_PARAMS[s]["g"]), float(SCHEME_PARAMS[s]["gamma"])))
         self.used = 0.0
+
+    def _batch(self, key):
+        b = self.batches.get(key)
+        if b is None:
+            scheme, g, gamma = key
+            b = self.batches[key] = Batch(self.context, scheme, g=g, gamma=gamma, cfl_scale=self.cfl_scale,
+                                          max_instances=self.max_instances)
+        return b
 
     def serve(self, requests: List[Request], clock=time.perf_counter):
         """Serve `requests` (arrival times relative to the call) until all are done.
@@ -114,10 +134,11 @@ class Server(object):
                 item = returns.get()
                 if item is None:
                     return
-                (s, slot), r, admitted, need = item
+                (bk, slot), r, admitted, need = item
+                s = bk[0]
                 ta = clock()
                 try:
-                    b = self.batches[s]
+                    b = self.batches[bk]
                     st = b.status(slot)
                     state = b.download(slot)
                     b.remove(slot)
@@ -164,15 +185,16 @@ class Server(object):
                     with lock:
                         if self.used + need > self.budget:
                             break
+                    bk = r.batch_key()
                     try:
-                        slot = self.batches[r.scheme].add(r.variables, r.nx, r.ny, r.dx, r.dy, r.t_end,
-                                                          r.boundary_conditions)
+                        slot = self._batch(bk).add(r.variables, r.nx, r.ny, r.dx, r.dy, r.t_end,
+                                                   r.boundary_conditions)
                     except MemoryError:
                         break
                     pending.popleft()
                     with lock:
                         self.used += need
-                    running[(r.scheme, slot)] = (r, clock() - t0, need)
+                    running[(bk, slot)] = (r, clock() - t0, need)
                 timers["admit"] += clock() - ta
                 # 3. wait for the chunk; hand the scenarios at t_end to the return thread
                 ta = clock()
