@@ -10,6 +10,9 @@ from . import Simulator
 from .Simulator import BoundaryCondition
 
 
+FLUXES = {"HLL": 0, "HLLC": 1, "GodC": 2}
+
+
 class HLL(Simulator.BaseSimulator):
     _scheme = "HLL"
     _gc = 1
@@ -22,8 +25,14 @@ class HLL(Simulator.BaseSimulator):
                  g,
                  cfl_scale=0.9,
                  boundary_conditions=BoundaryCondition(),
-                 block_width=16, block_height=16):
+                 block_width=16, block_height=16,
+                 flux="HLL"):
+        """`flux` (not in the reference's class): "HLL" (the reference's), or the
+        variants its SWECommon.h defines but no scheme uses: "HLLC"
+        (SWECommon.h:334-387) and "GodC", Godunov's centred flux (:248-255)."""
+        assert flux in FLUXES, "flux must be one of %s" % (tuple(FLUXES),)
         super().__init__(context, nx, ny, dx, dy, boundary_conditions, cfl_scale, 1, block_width,
                          block_height)
         self.g = np.float32(g)
-        self._create([h0, hu0, hv0], g=g)
+        self.flux = flux
+        self._create([h0, hu0, hv0], g=g, variant=FLUXES[flux])

@@ -148,7 +148,7 @@ class BaseSimulator(object):
         self._cur = None    # buffer holding the current state, tracked across substeps; None = ask the device
 
     # -- construction helper used by the scheme classes
-    def _create(self, variables, g=9.81, gamma=1.4, theta=1.3, order=2):
+    def _create(self, variables, g=9.81, gamma=1.4, theta=1.3, order=2, variant=0, variant_beta=0.0):
         scheme = _lib.SCHEME_IDS[self._scheme]
         nx, ny, gc = int(self.nx), int(self.ny), self._gc
         arrays = []
@@ -165,7 +165,8 @@ class BaseSimulator(object):
         tile = -1
         if getattr(self.context, "autotuner", None) is not None:
             tile = self.context.autotuner.get_tile(self._scheme, nx, ny, self.context.device_name)
-        p = _lib.fv_params(float(g), float(gamma), float(theta), float(self.cfl_scale), int(order), int(tile))
+        p = _lib.fv_params(float(g), float(gamma), float(theta), float(self.cfl_scale), int(order), int(tile),
+                           int(variant), float(variant_beta))
         ptrs = (_lib._FP * len(arrays))(*[a.ctypes.data_as(_lib._FP) for a in arrays])
         h = ctypes.c_void_p()
         _lib.check(_lib.lib().fv_sim_create(self.context.handle, scheme, nx, ny, float(self.dx), float(self.dy),

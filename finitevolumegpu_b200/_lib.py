@@ -40,6 +40,8 @@ class fv_params(ctypes.Structure):
         ("cfl_scale", ctypes.c_float),
         ("order", ctypes.c_int),
         ("tile", ctypes.c_int),
+        ("variant", ctypes.c_int),
+        ("variant_beta", ctypes.c_float),
     ]
 
 

@@ -32,7 +32,7 @@ class Batch(object):
     """Simulations of one split scheme advanced together by a persistent kernel."""
 
     def __init__(self, context, scheme, g=9.81, gamma=1.4, theta=None, cfl_scale=0.9, max_instances=1024,
-                 tile=None):
+                 tile=None, variant=0, variant_beta=0.0):
         if scheme not in BATCH_SCHEMES:
             raise ValueError("batched kernels exist for %s" % (BATCH_SCHEMES,))
         self.context = context
@@ -45,7 +45,9 @@ class Batch(object):
             if tuner is not None and hasattr(tuner, "get_batch_tile"):
                 tile = tuner.get_batch_tile(scheme, context.device_name)
         theta = DEFAULT_THETA.get(scheme, 1.3) if theta is None else theta
-        p = _lib.fv_params(float(g), float(gamma), float(theta), float(cfl_scale), 2, int(tile))
+        # variant: HLL's flux or WAF's limiter id (HLL.FLUXES, WAF.LIMITERS)
+        p = _lib.fv_params(float(g), float(gamma), float(theta), float(cfl_scale), 2, int(tile), int(variant),
+                           float(variant_beta))
         h = ctypes.c_void_p()
         _lib.check(_L().fv_batch_create(context.handle, _lib.SCHEME_IDS[scheme], ctypes.byref(p), int(max_instances),
                                         ctypes.byref(h)))

@@ -466,6 +466,14 @@ int copy_d2h(fv_context* ctx, cudaStream_t st, float* dst, size_t dpitch, const 
     return FV_OK;
 }
 
+// Flux variants exist for HLL (3) and limiters for WAF (9); other schemes take 0.
+int check_variant(int scheme, const fv_params* p) {
+    const int n = (scheme == FV_HLL) ? 3 : (scheme == FV_WAF) ? 9 : 1;
+    if (p->variant < 0 || p->variant >= n)
+        return fail(FV_ERR_INVALID, "variant %d does not exist for scheme %d", p->variant, scheme);
+    return FV_OK;
+}
+
 int read_ctl(fv_sim* s) {
     FV_CK(cudaMemcpyAsync(s->ctl_h, s->ctl, sizeof(SimCtl), cudaMemcpyDeviceToHost, s->stream));
     FV_CK(cudaStreamSynchronize(s->stream));
@@ -604,6 +612,7 @@ int fv_sim_create(fv_context* ctx, int scheme, int nx, int ny, float dx, float d
     if (!ctx || !params || !host_vars || !out) return fail(FV_ERR_INVALID, "null argument");
     if (scheme < FV_LXF || scheme > FV_EE2D_KP07_DIMSPLIT) return fail(FV_ERR_INVALID, "unknown scheme %d", scheme);
     if (nx < 1 || ny < 1 || nx > (1 << 20) || ny > (1 << 20)) return fail(FV_ERR_INVALID, "bad grid %d x %d", nx, ny);
+    FV_TRY(check_variant(scheme, params));
     for (int side = 0; side < 4; ++side)
         if (((bc >> (8 * side)) & 0xF) == fv::BC_NEUMANN)
             return fail(FV_ERR_UNSUPPORTED, "Neumann boundary condition not supported");
@@ -726,6 +735,8 @@ int fv_sim_create(fv_context* ctx, int scheme, int nx, int ny, float dx, float d
     a.dt_scale = s->dt_scale;
     a.bc = bc;
     a.order = params->order;
+    a.variant = params->variant;
+    a.variant_beta = params->variant_beta;
     *out = s;
     return FV_OK;
 }
@@ -1114,6 +1125,7 @@ extern "C" {
 
 int fv_batch_create(fv_context* ctx, int scheme, const fv_params* params, int max_instances, fv_batch** out) {
     if (!ctx || !params || !out) return fail(FV_ERR_INVALID, "null argument");
+    FV_TRY(check_variant(scheme, params));
     if (max_instances < 1 || max_instances > (1 << 20)) return fail(FV_ERR_INVALID, "bad max_instances");
     const int cfg = params->tile < 0 ? 0 : params->tile;
     const BEntry* be = find_batch_entry(scheme, cfg);
@@ -1279,6 +1291,8 @@ int fv_batch_add(fv_batch* b, int nx, int ny, float dx, float dy, int bc, const 
     I.gamma = b->p.gamma;
     I.theta = b->p.theta;
     I.dt_scale = b->dt_scale;
+    I.variant = b->p.variant;
+    I.variant_beta = b->p.variant_beta;
     auto enc = encode_fn();
     for (int k = 0; k < 2; ++k)
         for (int v = 0; v < b->nv; ++v) {

@@ -136,6 +136,26 @@ __device__ __forceinline__ float generalized_minmod(float r, float theta) {
     return fmaxf(0.0f, fminf(theta * r, fminf((1.0f + r) * 0.5f, theta)));
 }
 
+// Flux limiters phi(r) of GPUSimulators/cuda/limiters.h:84-118, by id:
+// 0 generalized minmod with theta = 1.9 (the one WAF uses, SWECommon.h:199-201),
+// 1 minmod, 2 superbee, 3 van Leer, 4 van Albada 1, 5 van Albada 2,
+// 6 monotonized central, 7 Osher(beta), 8 Sweby(beta).  van Albada 2 is the
+// textbook 2r/(r^2+1); the reference's spelling `r_*r_* + 1.0f` parses as
+// r^2 (limiters.h:110), and no reference scheme calls it.
+__device__ __forceinline__ float flux_limiter(float r, int id, float beta) {
+    switch (id) {
+    case 1: return fmaxf(0.0f, fminf(1.0f, r));
+    case 2: return fmaxf(0.0f, fmaxf(fminf(2.0f * r, 1.0f), fminf(r, 2.0f)));
+    case 3: return (r + fabsf(r)) / (1.0f + fabsf(r));
+    case 4: return (r * r + r) / (r * r + 1.0f);
+    case 5: return 2.0f * r / (r * r + 1.0f);
+    case 6: return fmaxf(0.0f, fminf(2.0f, fminf(2.0f * r, 0.5f * (1.0f + r))));
+    case 7: return fmaxf(0.0f, fminf(beta, r));
+    case 8: return fmaxf(0.0f, fmaxf(fminf(r, beta), fminf(beta * r, 1.0f)));
+    default: return fmaxf(0.0f, fminf(1.9f * r, fminf((1.0f + r) * 0.5f, 1.9f)));
+    }
+}
+
 // GPUSimulators/cuda/common.h:81-83
 __device__ __forceinline__ float desingularize(float x, float eps) {
     return copysignf(fmaxf(fabsf(x), fminf(x * x / (2.0f * eps) + 0.5f * eps, eps)), x);
@@ -356,7 +376,7 @@ __device__ __forceinline__ float waf_h_star(const WafCell& l, const WafCell& r, 
 // hd_l, hd, hd_r are the star depths of the pairs (l2,l1), (l1,r1), (r1,r2).
 __device__ __forceinline__ void waf_flux(const WafCell& l2, const WafCell& l1, const WafCell& r1,
                                          const WafCell& r2, float hd_l, float hd, float hd_r, float dtdx,
-                                         float out[3]) {
+                                         float out[3], int limiter = 0, float beta = 0.0f) {
     const float h_l = l1.q[0], h_r = r1.q[0];
     const float q_l = (hd > h_l) ? sqrtf(0.5f * ((hd + h_l) * hd)) / h_l : 1.0f;
     const float q_r = (hd > h_r) ? sqrtf(0.5f * ((hd + h_r) * hd)) / h_r : 1.0f;
@@ -377,9 +397,9 @@ __device__ __forceinline__ void waf_flux(const WafCell& l2, const WafCell& l1, c
     const float r_2 = desingularize((c_2 > 0.0f) ? (l1.v - l2.v) : (r2.v - r1.v), eps) / desingularize(r1.v - l1.v, eps);
     const float r_3 = desingularize((c_3 > 0.0f) ? (h_l - hd_l) : (r2.q[0] - hd_r), eps) / desingularize(h_r - hd, eps);
     // A_k = sign(c_k) * (1 - (1 - |c_k|) * limiter(r_k)) (SWECommon.h:109-111, :199-201)
-    const float A_1 = copysignf(1.0f, c_1) * (1.0f - (1.0f - fabsf(c_1)) * generalized_minmod(r_1, 1.9f));
-    const float A_2 = copysignf(1.0f, c_2) * (1.0f - (1.0f - fabsf(c_2)) * generalized_minmod(r_2, 1.9f));
-    const float A_3 = copysignf(1.0f, c_3) * (1.0f - (1.0f - fabsf(c_3)) * generalized_minmod(r_3, 1.9f));
+    const float A_1 = copysignf(1.0f, c_1) * (1.0f - (1.0f - fabsf(c_1)) * flux_limiter(r_1, limiter, beta));
+    const float A_2 = copysignf(1.0f, c_2) * (1.0f - (1.0f - fabsf(c_2)) * flux_limiter(r_2, limiter, beta));
+    const float A_3 = copysignf(1.0f, c_3) * (1.0f - (1.0f - fabsf(c_3)) * flux_limiter(r_3, limiter, beta));
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
         const float F1 = l1.f[v], F4 = r1.f[v];
@@ -391,6 +411,50 @@ __device__ __forceinline__ void waf_flux(const WafCell& l2, const WafCell& l1, c
 }
 
 // ------------------------------------------------------------------ first-order fluxes
+
+// HLLC flux (GPUSimulators/cuda/SWECommon.h:334-387): HLL's wave speeds plus
+// the contact speed S*, with the star states h (S - u) / (S - S*) (1, S*, v)
+// on either side of it.
+__device__ __forceinline__ void swe_hllc(const SweFace& l, const SweFace& r, float out[3]) {
+    const float h_l = l.q[0], h_r = r.q[0];
+    const float hsum = fadd(h_l, h_r);
+    const float h_dag = fsub(fmul(0.5f, hsum), fmul(fmul(0.25f, fsub(r.u, l.u)), hsum) / fadd(l.c, r.c));
+    const float q_l = (h_dag > h_l) ? sqrtf(fmul(0.5f, fmul(fadd(h_dag, h_l), h_dag) / fmul(h_l, h_l))) : 1.0f;
+    const float q_r = (h_dag > h_r) ? sqrtf(fmul(0.5f, fmul(fadd(h_dag, h_r), h_dag) / fmul(h_r, h_r))) : 1.0f;
+    const float S_l = ffma(-l.c, q_l, l.u);
+    const float S_r = ffma(r.c, q_r, r.u);
+    const float a_r = fmul(h_r, fsub(r.u, S_r)), a_l = fmul(h_l, fsub(l.u, S_l));
+    const float S_star = fsub(fmul(S_l, a_r), fmul(S_r, a_l)) / fsub(a_r, a_l);
+    if (S_l >= 0.0f) {
+#pragma unroll
+        for (int v = 0; v < 3; ++v) out[v] = l.f[v];
+    } else if (S_r <= 0.0f) {
+#pragma unroll
+        for (int v = 0; v < 3; ++v) out[v] = r.f[v];
+    } else if (S_star >= 0.0f) {
+        const float k = fmul(h_l, fsub(S_l, l.u)) / fsub(S_l, S_star);
+        const float qs[3] = {k, fmul(k, S_star), fmul(k, l.q[2] / h_l)};
+#pragma unroll
+        for (int v = 0; v < 3; ++v) out[v] = ffma(S_l, fsub(qs[v], l.q[v]), l.f[v]);
+    } else {
+        const float k = fmul(h_r, fsub(S_r, r.u)) / fsub(S_r, S_star);
+        const float qs[3] = {k, fmul(k, S_star), fmul(k, r.q[2] / h_r)};
+#pragma unroll
+        for (int v = 0; v < 3; ++v) out[v] = ffma(S_r, fsub(qs[v], r.q[v]), r.f[v]);
+    }
+}
+
+// Godunov's centred flux (GPUSimulators/cuda/SWECommon.h:248-255):
+// F(0.5 (Ql + Qr) + dt/dx (F(Ql) - F(Qr))); kdx = dt/dx.
+__device__ __forceinline__ void swe_godc(const SweFace& l, const SweFace& r, float g, float half_g, float kdx,
+                                         float out[3]) {
+    float q[3];
+#pragma unroll
+    for (int v = 0; v < 3; ++v) q[v] = ffma(kdx, fsub(l.f[v], r.f[v]), fmul(0.5f, fadd(l.q[v], r.q[v])));
+    const SweFace c = swe_face(q[0], q[1], q[2], g, half_g);
+#pragma unroll
+    for (int v = 0; v < 3; ++v) out[v] = c.f[v];
+}
 
 // FORCE = (LxF + Lax-Wendroff two-step) / 2 (GPUSimulators/cuda/SWECommon.h:404-409,
 // :443-450, :466-470).  kx = dx/(2dt), kw = dt/(2dx).

@@ -72,6 +72,8 @@ struct StageArgs {
     int explicit_dt;     // take the step dt from dt_step instead of the control block
     float dt_step;
     int want_sums;       // compute FP64 sums of the new state at the end of a step
+    int variant;         // HLL: flux variant; WAF: flux limiter (0 = the reference's)
+    float variant_beta;  // parameter of the Osher and Sweby limiters
 };
 
 // Storage: per variable, rows y = -2 .. ny+1 and columns x = -4 .. pitch-5,
@@ -463,11 +465,14 @@ __device__ __forceinline__ void walk_mh(float* line, int step, int a, int b, con
 
 // Two-point flux walker (FORCE, HLL: GPUSimulators/cuda/SWE2D_FORCE.cu:29-81,
 // SWE2D_HLL.cu:32-86).  pre holds Q[a-1] (slot 1) and Q[b] (slot 2).
+// For HLL, `variant` picks the flux: 0 HLL, 1 HLLC, 2 Godunov centred.
 template <int SCHEME, bool SWAP, int PS>
 __device__ __forceinline__ void walk_2pt(float* line, int step, int a, int b, const float (&pre)[4][3], float g,
-                                         float half_g, float kx, float kw, float kdx) {
+                                         float half_g, float kx, float kw, float kdx, int variant) {
     auto face_flux = [&](const SweFace& l, const SweFace& r, float (&F)[3]) {
         if (SCHEME == FORCE) swe_force(l, r, g, half_g, kx, kw, F);
+        else if (variant == 1) swe_hllc(l, r, F);
+        else if (variant == 2) swe_godc(l, r, g, half_g, kdx, F);
         else swe_hll(l, r, F);
     };
     SweFace sL = swe_face(pre[1][0], pre[1][1], pre[1][2], g, half_g);
@@ -507,7 +512,7 @@ __device__ __forceinline__ void walk_2pt(float* line, int step, int a, int b, co
 // pairs are carried along the window.
 template <bool SWAP, int PS>
 __device__ __forceinline__ void walk_waf(float* line, int step, int a, int b, const float (&pre)[4][3], float g,
-                                         float half_g, float inv_g, float dtdx, float kdx) {
+                                         float half_g, float inv_g, float dtdx, float kdx, int limiter, float beta) {
     WafCell C0 = waf_cell(pre[0], g, half_g);
     WafCell C1 = waf_cell(pre[1], g, half_g);
     float q[3];
@@ -517,7 +522,7 @@ __device__ __forceinline__ void walk_waf(float* line, int step, int a, int b, co
     WafCell C3 = waf_cell(q, g, half_g);
     float hs01 = waf_h_star(C0, C1, inv_g), hs12 = waf_h_star(C1, C2, inv_g), hs23 = waf_h_star(C2, C3, inv_g);
     float Fprev[3];
-    waf_flux(C0, C1, C2, C3, hs01, hs12, hs23, dtdx, Fprev);  // face a-1/2
+    waf_flux(C0, C1, C2, C3, hs01, hs12, hs23, dtdx, Fprev, limiter, beta);  // face a-1/2
     for (int c = a + 1; c <= b; ++c) {
         if (c + 1 < b) {
             ld_cell<3, SWAP, PS>(line, c + 1, step, q);
@@ -534,7 +539,7 @@ __device__ __forceinline__ void walk_waf(float* line, int step, int a, int b, co
         hs12 = hs23;
         hs23 = waf_h_star(C2, C3, inv_g);
         float F[3];
-        waf_flux(C0, C1, C2, C3, hs01, hs12, hs23, dtdx, F);  // face c-1/2
+        waf_flux(C0, C1, C2, C3, hs01, hs12, hs23, dtdx, F, limiter, beta);  // face c-1/2
         float out[3];
 #pragma unroll
         for (int v = 0; v < 3; ++v) out[v] = fmaf(Fprev[v] - F[v], kdx, C1.q[v]);
@@ -549,6 +554,8 @@ struct SweepPar {
     float theta, g, half_g, inv_g, gamma;
     float kdt;   // kernel dt
     float dxx;   // cell size along the sweep
+    int variant;  // HLL: flux variant; WAF: flux limiter (see walk_2pt, flux_limiter)
+    float beta;   // parameter of the Osher and Sweby limiters
 };
 
 template <int SCHEME, bool SWAP, int PS>
@@ -563,10 +570,10 @@ __device__ __forceinline__ void walk_line(float* line, int step, int a, int b, c
         // x sweeps use HLL, y sweeps central-upwind (GPUSimulators/cuda/EE2D_KP07_dimsplit.cu:62, :106)
         walk_mh<EulerPhys, !SWAP, SWAP, PS>(line, step, a, b, pre, P, kdx);
     } else if constexpr (SCHEME == WAF) {
-        walk_waf<SWAP, PS>(line, step, a, b, pre, p.g, p.half_g, p.inv_g, kdx, kdx);
+        walk_waf<SWAP, PS>(line, step, a, b, pre, p.g, p.half_g, p.inv_g, kdx, kdx, p.variant, p.beta);
     } else {
         walk_2pt<SCHEME, SWAP, PS>(line, step, a, b, pre, p.g, p.half_g, p.dxx / (2.0f * p.kdt),
-                                   p.kdt / (2.0f * p.dxx), kdx);
+                                   p.kdt / (2.0f * p.dxx), kdx, p.variant);
     }
 }
 
@@ -621,6 +628,8 @@ struct SplitPar {
     float dx, dy, g, gamma, theta;
     float kdt;  // kernel dt of this substep
     int substep;
+    int variant;  // flux variant (HLL) or limiter (WAF)
+    float beta;
 };
 
 // Load, ghost cells, both sweeps and copy-out of one tile of a split scheme
@@ -648,6 +657,8 @@ __device__ bool process_tile_dimsplit(float* Qs, uint64_t* bar, uint32_t phase, 
     p.inv_g = 1.0f / P.g;
     p.gamma = P.gamma;
     p.kdt = P.kdt;
+    p.variant = P.variant;
+    p.beta = P.beta;
     const bool x_first = (SCHEME == FORCE || SCHEME == HLL) ? true : (P.substep == 0);
     if (x_first) {
         p.dxx = P.dx;
@@ -743,7 +754,7 @@ __global__ void __launch_bounds__(NT) dimsplit_stage_kernel(const __grid_constan
     J.bc = A.bc;
     J.x0 = blockIdx.x * W;
     J.y0 = blockIdx.y * H;
-    SplitPar P{A.dx, A.dy, A.g, A.gamma, A.theta, sc.dt * A.dt_scale, A.substep};
+    SplitPar P{A.dx, A.dy, A.g, A.gamma, A.theta, sc.dt * A.dt_scale, A.substep, A.variant, A.variant_beta};
     process_tile_dimsplit<SCHEME, W, H, NT>(Qs, &bar, 0, true, J, P, sc.do_cfl, sums, &A.ctl->error, my_cfl, my_sums);
     stage_epilogue<NT, NV>(A, sc, my_cfl, my_sums, sums);
 }
@@ -761,6 +772,8 @@ struct alignas(64) BatchInstance {
     int nx, ny, pitch, bc;
     int tiles_x, ntiles;
     float dx, dy, g, gamma, theta, dt_scale;
+    int variant;         // flux variant (HLL) or limiter (WAF)
+    float variant_beta;
 };
 
 struct BatchArgs {
@@ -810,7 +823,7 @@ __global__ void __launch_bounds__(NT) batched_stage_kernel(const __grid_constant
         const int ty = job.y / I.tiles_x;
         J.x0 = (job.y - ty * I.tiles_x) * W;
         J.y0 = ty * H;
-        SplitPar P{I.dx, I.dy, I.g, I.gamma, I.theta, sc.dt * I.dt_scale, B.substep};
+        SplitPar P{I.dx, I.dy, I.g, I.gamma, I.theta, sc.dt * I.dt_scale, B.substep, I.variant, I.variant_beta};
         process_tile_dimsplit<SCHEME, W, H, NT, true>(Qs, &bar, phase, init, J, P, sc.do_cfl, sums, B.err, my_cfl,
                                                       my_sums);
         init = false;

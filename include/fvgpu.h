@@ -56,6 +56,14 @@ typedef struct fv_params {
     float cfl_scale; /* Courant number used by simulate() */
     int order;       /* Runge-Kutta order of KP07 (1 or 2) */
     int tile;        /* tile configuration index, or -1 for the scheme default */
+    /* Options the reference defines but none of its schemes uses
+     * (GPUSimulators/cuda/SWECommon.h:248-255, :334-387; limiters.h:84-118):
+     * HLL's flux (0 HLL, 1 HLLC, 2 Godunov centred) or WAF's limiter (0 the
+     * reference's generalized minmod with theta 1.9, 1 minmod, 2 superbee,
+     * 3 van Leer, 4 van Albada 1, 5 van Albada 2, 6 monotonized central,
+     * 7 Osher, 8 Sweby); 0 for every other scheme. */
+    int variant;
+    float variant_beta; /* beta of the Osher and Sweby limiters */
 } fv_params;
 
 /* Library version (major*10000 + minor*100 + patch). */

@@ -114,6 +114,25 @@ template <typename T> inline T generalized_minmod(T r, T theta) {
     return fmax_(T(0), fmin_(theta * r, fmin_((T(1) + r) / T(2), theta)));
 }
 
+// Flux limiters of GPUSimulators/cuda/limiters.h:84-118, by id: 0 generalized
+// minmod with theta 1.9 (WAF's, SWECommon.h:199-201), 1 minmod, 2 superbee,
+// 3 van Leer, 4 van Albada 1, 5 van Albada 2 (2r/(r^2+1): the reference's
+// `r_*r_* + 1.0f` parses as r^2, limiters.h:110), 6 monotonized central,
+// 7 Osher(beta), 8 Sweby(beta).
+template <typename T> inline T flux_limiter(T r, int id, T beta) {
+    switch (id) {
+    case 1: return fmax_(T(0), fmin_(T(1), r));                                            // limiters.h:96-98
+    case 2: return fmax_(T(0), fmax_(fmin_(T(2) * r, T(1)), fmin_(r, T(2))));              // :104-106
+    case 3: return (r + fabs_(r)) / (T(1) + fabs_(r));                                     // :116-118
+    case 4: return (r * r + r) / (r * r + T(1));                                           // :108-110
+    case 5: return T(2) * r / (r * r + T(1));                                              // :112-114
+    case 6: return fmax_(T(0), fmin_(T(2), fmin_(T(2) * r, T(0.5) * (T(1) + r))));          // :84-86
+    case 7: return fmax_(T(0), fmin_(beta, r));                                            // :88-90
+    case 8: return fmax_(T(0), fmax_(fmin_(r, beta), fmin_(beta * r, T(1))));               // :92-94
+    default: return generalized_minmod(r, T(1.9));
+    }
+}
+
 // GPUSimulators/cuda/common.h:81-83
 template <typename T> inline T desingularize(T x, T eps) {
     return sgn1(x) * fmax_(fabs_(x), fmin_(x * x / (T(2) * eps) + T(0.5) * eps, eps));
@@ -172,6 +191,49 @@ template <typename T> inline Vec<T, 3> swe_hll(const Vec<T, 3>& Ql, const Vec<T,
     return f;
 }
 
+// GPUSimulators/cuda/SWECommon.h:334-387
+template <typename T> inline Vec<T, 3> swe_hllc(const Vec<T, 3>& Ql, const Vec<T, 3>& Qr, T g) {
+    const T h_l = Ql.c[0];
+    const T h_r = Qr.c[0];
+    const T u_l = Ql.c[1] / h_l;
+    const T u_r = Qr.c[1] / h_r;
+    const T c_l = sqrt_(g * h_l);
+    const T c_r = sqrt_(g * h_r);
+    const T h_dag = T(0.5) * (h_l + h_r) - T(0.25) * (u_r - u_l) * (h_l + h_r) / (c_l + c_r);
+    const T q_l_tmp = sqrt_(T(0.5) * ((h_dag + h_l) * h_dag / (h_l * h_l)));
+    const T q_r_tmp = sqrt_(T(0.5) * ((h_dag + h_r) * h_dag / (h_r * h_r)));
+    const T q_l = (h_dag > h_l) ? q_l_tmp : T(1);
+    const T q_r = (h_dag > h_r) ? q_r_tmp : T(1);
+    const T S_l = u_l - c_l * q_l;
+    const T S_r = u_r + c_r * q_r;
+    const T S_star = (S_l * h_r * (u_r - S_r) - S_r * h_l * (u_l - S_l)) / (h_r * (u_r - S_r) - h_l * (u_l - S_l));
+    const Vec<T, 3> F_l = swe_F(Ql, g);
+    const Vec<T, 3> F_r = swe_F(Qr, g);
+    if (S_l >= T(0)) return F_l;
+    if (S_r <= T(0)) return F_r;
+    Vec<T, 3> f;
+    if (S_l <= T(0) && T(0) <= S_star) {
+        const T v_l = Ql.c[2] / h_l;
+        const T k = h_l * (S_l - u_l) / (S_l - S_star);
+        const T qs[3] = {k * T(1), k * S_star, k * v_l};
+        for (int v = 0; v < 3; ++v) f.c[v] = F_l.c[v] + S_l * (qs[v] - Ql.c[v]);
+        return f;
+    }
+    const T v_r = Qr.c[2] / h_r;
+    const T k = h_r * (S_r - u_r) / (S_r - S_star);
+    const T qs[3] = {k * T(1), k * S_star, k * v_r};
+    for (int v = 0; v < 3; ++v) f.c[v] = F_r.c[v] + S_r * (qs[v] - Qr.c[v]);
+    return f;
+}
+
+// GPUSimulators/cuda/SWECommon.h:248-255
+template <typename T> inline Vec<T, 3> swe_godc_1d(const Vec<T, 3>& Ql, const Vec<T, 3>& Qr, T g, T dx, T dt) {
+    const Vec<T, 3> F_l = swe_F(Ql, g), F_r = swe_F(Qr, g);
+    Vec<T, 3> q;
+    for (int v = 0; v < 3; ++v) q.c[v] = T(0.5) * (Ql.c[v] + Qr.c[v]) + (dt / dx) * (F_l.c[v] - F_r.c[v]);
+    return swe_F(q, g);
+}
+
 // GPUSimulators/cuda/SWECommon.h:109-111
 template <typename T> inline T limiter_to_waf_limiter(T r, T c) { return T(1) - (T(1) - fabs_(c)) * r; }
 
@@ -186,7 +248,7 @@ template <typename T> inline T compute_h_star(T h_l, T h_r, T u_l, T u_r, T c_l,
 // GPUSimulators/cuda/SWECommon.h:131-210 (interface i+1/2 from Q_{i-1}, Q_i, Q_{i+1}, Q_{i+2})
 template <typename T>
 inline Vec<T, 3> swe_waf(const Vec<T, 3>& Ql2, const Vec<T, 3>& Ql1, const Vec<T, 3>& Qr1, const Vec<T, 3>& Qr2,
-                         T g, T dx, T dt) {
+                         T g, T dx, T dt, int limiter = 0, T beta = T(0)) {
     const T h_l = Ql1.c[0], h_r = Qr1.c[0];
     const T h_l2 = Ql2.c[0], h_r2 = Qr2.c[0];
     const T u_l = Ql1.c[1] / h_l, u_r = Qr1.c[1] / h_r;
@@ -223,9 +285,9 @@ inline Vec<T, 3> swe_waf(const Vec<T, 3>& Ql2, const Vec<T, 3>& Ql1, const Vec<T
     const T r_1 = desingularize((c_1 > T(0)) ? (h_dag_l - h_l2) : (h_dag_r - h_r), eps) / desingularize(h_dag - h_l, eps);
     const T r_2 = desingularize((c_2 > T(0)) ? (v_l - v_l2) : (v_r2 - v_r), eps) / desingularize(v_r - v_l, eps);
     const T r_3 = desingularize((c_3 > T(0)) ? (h_l - h_dag_l) : (h_r2 - h_dag_r), eps) / desingularize(h_r - h_dag, eps);
-    const T A_1 = sgn1(c_1) * limiter_to_waf_limiter(generalized_minmod(r_1, T(1.9)), c_1);
-    const T A_2 = sgn1(c_2) * limiter_to_waf_limiter(generalized_minmod(r_2, T(1.9)), c_2);
-    const T A_3 = sgn1(c_3) * limiter_to_waf_limiter(generalized_minmod(r_3, T(1.9)), c_3);
+    const T A_1 = sgn1(c_1) * limiter_to_waf_limiter(flux_limiter(r_1, limiter, beta), c_1);
+    const T A_2 = sgn1(c_2) * limiter_to_waf_limiter(flux_limiter(r_2, limiter, beta), c_2);
+    const T A_3 = sgn1(c_3) * limiter_to_waf_limiter(flux_limiter(r_3, limiter, beta), c_3);
     Vec<T, 3> f;
     for (int v = 0; v < 3; ++v)
         f.c[v] = T(0.5) * (F_1.c[v] + F_4.c[v]) -
@@ -389,6 +451,8 @@ template <typename T> struct Params {
     int scheme;
     T dx, dy, dt, g, gamma, theta;
     int step, order, bc;
+    int variant;  // HLL: flux (0 HLL, 1 HLLC, 2 GodC); WAF: limiter id (flux_limiter)
+    T beta;       // Osher / Sweby limiter parameter
 };
 
 // A line (row or column) of NV variables, accessed with a stride.  For the
@@ -444,10 +508,12 @@ inline Vec<T, 3> swe_face_flux(const Params<T>& P, const Line<T, 3>& L, int k, T
     switch (P.scheme) {
     case FORCE:  // GPUSimulators/cuda/SWE2D_FORCE.cu:34-50
         return swe_force_1d(L.get(k), L.get(k + 1), g, dxx, P.dt);
-    case HLL:  // GPUSimulators/cuda/SWE2D_HLL.cu:36-52
+    case HLL:  // GPUSimulators/cuda/SWE2D_HLL.cu:36-52 (variant 0)
+        if (P.variant == 1) return swe_hllc(L.get(k), L.get(k + 1), g);
+        if (P.variant == 2) return swe_godc_1d(L.get(k), L.get(k + 1), g, dxx, P.dt);
         return swe_hll(L.get(k), L.get(k + 1), g);
-    case WAF:  // GPUSimulators/cuda/SWE2D_WAF.cu:39-53
-        return swe_waf(L.get(k - 1), L.get(k), L.get(k + 1), L.get(k + 2), g, dxx, P.dt);
+    case WAF:  // GPUSimulators/cuda/SWE2D_WAF.cu:39-53 (limiter 0)
+        return swe_waf(L.get(k - 1), L.get(k), L.get(k + 1), L.get(k + 2), g, dxx, P.dt, P.variant, P.beta);
     case HLL2:
     case KP07_DIMSPLIT: {
         const T c = P.dt / (T(2) * dxx);
@@ -677,14 +743,14 @@ void unsplit_substep(const Params<T>& P, const T* const* in, T* const* out, int 
 
 template <typename T>
 int substep_impl(int scheme, int nx, int ny, const T* const* in, T* const* out, T dx, T dy, T dt, T g, T gamma,
-                 T theta, int step, int order, int bc, T* cfl, int nthreads) {
+                 T theta, int step, int order, int bc, T* cfl, int nthreads, int variant = 0, T beta = T(0)) {
     if (scheme < 0 || scheme > 7 || nx <= 0 || ny <= 0) return 1;
 #ifdef _OPENMP
     if (nthreads > 0) omp_set_num_threads(nthreads);
 #else
     (void)nthreads;
 #endif
-    Params<T> P{scheme, dx, dy, dt, g, gamma, theta, step, order, bc};
+    Params<T> P{scheme, dx, dy, dt, g, gamma, theta, step, order, bc, variant, beta};
     if (scheme == LXF || scheme == KP07) {
         unsplit_substep<T>(P, in, out, nx, ny, cfl);
     } else if (scheme == EE2D_KP07_DIMSPLIT) {
@@ -704,17 +770,37 @@ extern "C" {
 // (ny+2g) x (nx+2g) values including ghost cells; only interior cells of `out`
 // are written (the reference never writes ghost cells, common.h:376).  `cfl`
 // (nullable) receives the minimum CFL time step of the updated state.
+// `variant`, `beta`: HLL's flux or WAF's limiter (see Params); 0 for the reference's.
 int fvo_substep_f32(int scheme, int nx, int ny, const float* const* in, float* const* out, float dx, float dy,
                     float dt, float g, float gamma, float theta, int step, int order, int bc, float* cfl,
-                    int nthreads) {
-    return substep_impl<float>(scheme, nx, ny, in, out, dx, dy, dt, g, gamma, theta, step, order, bc, cfl, nthreads);
+                    int nthreads, int variant, float beta) {
+    return substep_impl<float>(scheme, nx, ny, in, out, dx, dy, dt, g, gamma, theta, step, order, bc, cfl, nthreads,
+                               variant, beta);
 }
 
 int fvo_substep_f64(int scheme, int nx, int ny, const double* const* in, double* const* out, double dx, double dy,
                     double dt, double g, double gamma, double theta, int step, int order, int bc, double* cfl,
-                    int nthreads) {
+                    int nthreads, int variant, double beta) {
     return substep_impl<double>(scheme, nx, ny, in, out, dx, dy, dt, g, gamma, theta, step, order, bc, cfl,
-                                nthreads);
+                                nthreads, variant, beta);
+}
+
+// One face flux in FP32 for n face pairs (ql, qr: n x 3): kind 0 HLL, 1 HLLC,
+// 2 Godunov centred (dx, dt used by 2 only).
+int fvo_flux_eval(int kind, int n, const float* ql, const float* qr, float g, float dx, float dt, float* out) {
+    for (int i = 0; i < n; ++i) {
+        const Vec<float, 3> l{{ql[3 * i], ql[3 * i + 1], ql[3 * i + 2]}}, r{{qr[3 * i], qr[3 * i + 1], qr[3 * i + 2]}};
+        const Vec<float, 3> f = kind == 1 ? swe_hllc(l, r, g) : kind == 2 ? swe_godc_1d(l, r, g, dx, dt)
+                                                                           : swe_hll(l, r, g);
+        for (int v = 0; v < 3; ++v) out[3 * i + v] = f.c[v];
+    }
+    return 0;
+}
+
+// A flux limiter (flux_limiter ids) in FP32 on n ratios.
+int fvo_limiter_eval(int id, int n, const float* r, float beta, float* out) {
+    for (int i = 0; i < n; ++i) out[i] = flux_limiter(r[i], id, beta);
+    return 0;
 }
 
 // Floating-point operations of one substep as the reference formulates it:

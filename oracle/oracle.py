@@ -78,6 +78,7 @@ def lib():
                 fp, fp, fp, fp, fp, fp,
                 ctypes.c_int, ctypes.c_int, ctypes.c_int,
                 P, ctypes.c_int,
+                ctypes.c_int, fp,
             ]
             f.restype = ctypes.c_int
         _lib = L
@@ -98,7 +99,7 @@ def substep_factor(scheme: str) -> float:
 
 
 def oracle_substep(scheme, u_in, u_out, nx, ny, dx, dy, dt, g, gamma, theta, step, order, bc, want_cfl=True,
-                   nthreads=0):
+                   nthreads=0, variant=0, beta=0.0):
     """Run one stage kernel of `scheme` on full (ny+2g, nx+2g) arrays; returns the CFL minimum or None."""
     dtype = u_in[0].dtype
     f64 = dtype == np.float64
@@ -112,10 +113,33 @@ def oracle_substep(scheme, u_in, u_out, nx, ny, dx, dy, dt, g, gamma, theta, ste
     cfl = fp(0)
     fn = lib().fvo_substep_f64 if f64 else lib().fvo_substep_f32
     rc = fn(SCHEMES[scheme], nx, ny, ins, outs, dx, dy, dt, g, gamma, theta, step, order, bc,
-            ctypes.pointer(cfl) if want_cfl else None, nthreads)
+            ctypes.pointer(cfl) if want_cfl else None, nthreads, int(variant), beta)
     if rc != 0:
         raise RuntimeError("oracle substep failed")
     return dtype.type(cfl.value) if want_cfl else None
+
+
+def flux_eval(kind, ql, qr, g, dx=1.0, dt=0.1):
+    """FP32 oracle face fluxes for n face pairs (n x 3 arrays): kind 0 HLL, 1 HLLC, 2 Godunov centred."""
+    L = lib()
+    P = ctypes.POINTER(ctypes.c_float)
+    ql = np.ascontiguousarray(ql, dtype=np.float32)
+    qr = np.ascontiguousarray(qr, dtype=np.float32)
+    out = np.empty_like(ql)
+    L.fvo_flux_eval.argtypes = [ctypes.c_int, ctypes.c_int, P, P, ctypes.c_float, ctypes.c_float, ctypes.c_float, P]
+    L.fvo_flux_eval(int(kind), ql.shape[0], ql.ctypes.data_as(P), qr.ctypes.data_as(P), g, dx, dt, out.ctypes.data_as(P))
+    return out
+
+
+def limiter_eval(limiter_id, r, beta=0.0):
+    """FP32 oracle flux limiter (fv_oracle.cpp flux_limiter ids) on an array of ratios."""
+    L = lib()
+    P = ctypes.POINTER(ctypes.c_float)
+    r = np.ascontiguousarray(r, dtype=np.float32)
+    out = np.empty_like(r)
+    L.fvo_limiter_eval.argtypes = [ctypes.c_int, ctypes.c_int, P, ctypes.c_float, P]
+    L.fvo_limiter_eval(int(limiter_id), r.size, r.ctypes.data_as(P), beta, out.ctypes.data_as(P))
+    return out
 
 
 OP_NAMES = ("add", "sub", "mul", "div", "sqrt", "minmax")
@@ -189,7 +213,7 @@ class OracleSim:
     """A reference simulator's host semantics, on the CPU oracle."""
 
     def __init__(self, scheme, variables, nx, ny, dx, dy, g, gamma=1.4, theta=None, cfl_scale=0.9, order=2,
-                 bc=0x03030303, dtype=np.float32, nthreads=0):
+                 bc=0x03030303, dtype=np.float32, nthreads=0, variant=0, beta=0.0):
         self.scheme = scheme
         self.dtype = np.dtype(dtype)
         self.nx, self.ny = int(nx), int(ny)
@@ -205,6 +229,8 @@ class OracleSim:
         self.order = int(order)
         self.bc = int(bc)
         self.nthreads = nthreads
+        self.variant = int(variant)  # HLL's flux or WAF's limiter (fv_oracle.cpp Params)
+        self.beta = self.dtype.type(beta)
         if scheme in ("LxF", "FORCE", "HLL"):
             self.num_substeps = 1
         elif scheme == "KP07":
@@ -281,7 +307,7 @@ class OracleSim:
     def _launch(self, kdt, step_number):
         return oracle_substep(self.scheme, self.u0, self.u1, self.nx, self.ny, self.dx, self.dy, kdt, self.g,
                               self.gamma, self.theta, step_number, self.order, self.bc,
-                              want_cfl=True, nthreads=self.nthreads)
+                              want_cfl=True, nthreads=self.nthreads, variant=self.variant, beta=self.beta)
 
     def computeDt(self):
         T = self.dtype.type
