@@ -92,6 +92,23 @@ const KEntry kTable[] = {
 };
 constexpr int kNumEntries = sizeof(kTable) / sizeof(kTable[0]);
 
+// Kernels of HLL's HLLC and Godunov-centred fluxes and of WAF's other limiters
+// (variant 0 is the reference's own and uses kTable), one tile configuration
+// each: the variant is a template parameter, so the default kernels carry no
+// switch in their cell loops.
+struct VEntry {
+    int variant;
+    KEntry k;
+};
+const VEntry kVariantTable[] = {
+#define FV_V(S, ES, V) {V, {S, 124, 60, 256, true, fv::dimsplit_stage_kernel<ES, 124, 60, 256, V>}}
+    FV_V(FV_HLL, fv::HLL, 1), FV_V(FV_HLL, fv::HLL, 2),
+    FV_V(FV_WAF, fv::WAF, 1), FV_V(FV_WAF, fv::WAF, 2), FV_V(FV_WAF, fv::WAF, 3), FV_V(FV_WAF, fv::WAF, 4),
+    FV_V(FV_WAF, fv::WAF, 5), FV_V(FV_WAF, fv::WAF, 6), FV_V(FV_WAF, fv::WAF, 7), FV_V(FV_WAF, fv::WAF, 8),
+#undef FV_V
+};
+constexpr int kNumVariants = sizeof(kVariantTable) / sizeof(kVariantTable[0]);
+
 using BatchFn = void (*)(fv::BatchArgs);
 struct BEntry {
     int scheme;
@@ -117,9 +134,31 @@ const BEntry kBatchTable[] = {
 };
 constexpr int kNumBatchEntries = sizeof(kBatchTable) / sizeof(kBatchTable[0]);
 
+// Batched kernels of the variants other than 0, one tile configuration each.
+struct VBEntry {
+    int variant;
+    BEntry b;
+};
+const VBEntry kBatchVariantTable[] = {
+#define FV_V(S, ES, V) {V, {S, 60, 28, 128, fv::batched_stage_kernel<ES, 60, 28, 128, V>}}
+    FV_V(FV_HLL, fv::HLL, 1), FV_V(FV_HLL, fv::HLL, 2),
+    FV_V(FV_WAF, fv::WAF, 1), FV_V(FV_WAF, fv::WAF, 2), FV_V(FV_WAF, fv::WAF, 3), FV_V(FV_WAF, fv::WAF, 4),
+    FV_V(FV_WAF, fv::WAF, 5), FV_V(FV_WAF, fv::WAF, 6), FV_V(FV_WAF, fv::WAF, 7), FV_V(FV_WAF, fv::WAF, 8),
+#undef FV_V
+};
+constexpr int kNumBatchVariants = sizeof(kBatchVariantTable) / sizeof(kBatchVariantTable[0]);
+
 size_t batch_smem(const BEntry& e) { return scheme_nv(e.scheme) * (size_t)(e.W + 8) * (e.H + 4) * sizeof(float); }
 
-const BEntry* find_batch_entry(int scheme, int cfg) {
+// The batched kernel of tile configuration `cfg`, or for variant > 0 the
+// variant's single kernel (cfg is then ignored).
+const BEntry* find_batch_entry(int scheme, int cfg, int variant) {
+    if (variant > 0) {
+        for (int i = 0; i < kNumBatchVariants; ++i)
+            if (kBatchVariantTable[i].b.scheme == scheme && kBatchVariantTable[i].variant == variant)
+                return &kBatchVariantTable[i].b;
+        return nullptr;
+    }
     int k = 0;
     for (int i = 0; i < kNumBatchEntries; ++i) {
         if (kBatchTable[i].scheme != scheme) continue;
@@ -135,7 +174,15 @@ size_t entry_smem(const KEntry& e) {
     return scheme_nv(e.scheme) * tile;
 }
 
-const KEntry* find_entry(int scheme, int cfg) {
+// The stage kernel of tile configuration `cfg`, or for variant > 0 the
+// variant's single kernel (cfg is then ignored).
+const KEntry* find_entry(int scheme, int cfg, int variant) {
+    if (variant > 0) {
+        for (int i = 0; i < kNumVariants; ++i)
+            if (kVariantTable[i].k.scheme == scheme && kVariantTable[i].variant == variant)
+                return &kVariantTable[i].k;
+        return nullptr;
+    }
     int k = 0;
     for (int i = 0; i < kNumEntries; ++i) {
         if (kTable[i].scheme != scheme) continue;
@@ -571,6 +618,9 @@ int fv_context_create(int device, fv_context** out) {
     for (int i = 0; i < kNumEntries; ++i)
         FV_CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(kTable[i].fn),
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)entry_smem(kTable[i])));
+    for (int i = 0; i < kNumVariants; ++i)
+        FV_CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(kVariantTable[i].k.fn),
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)entry_smem(kVariantTable[i].k)));
     // Device memory of finished simulations stays in the stream-ordered pool
     // for the next ones instead of being unmapped at every synchronisation
     // (the pool is trimmed when the context is destroyed).  Memory freed on
@@ -624,7 +674,7 @@ int fv_sim_create(fv_context* ctx, int scheme, int nx, int ny, float dx, float d
     for (int v = 0; v < nv; ++v)
         if (!host_vars[v]) return fail(FV_ERR_INVALID, "variable %d is null", v);
     const int cfg = params->tile < 0 ? 0 : params->tile;
-    const KEntry* ke = find_entry(scheme, cfg);
+    const KEntry* ke = find_entry(scheme, cfg, params->variant);
     if (!ke) return fail(FV_ERR_INVALID, "tile configuration %d does not exist for scheme %d", cfg, scheme);
     FV_CK(cudaSetDevice(ctx->device));
 
@@ -735,7 +785,6 @@ int fv_sim_create(fv_context* ctx, int scheme, int nx, int ny, float dx, float d
     a.dt_scale = s->dt_scale;
     a.bc = bc;
     a.order = params->order;
-    a.variant = params->variant;
     a.variant_beta = params->variant_beta;
     *out = s;
     return FV_OK;
@@ -1128,7 +1177,7 @@ int fv_batch_create(fv_context* ctx, int scheme, const fv_params* params, int ma
     FV_TRY(check_variant(scheme, params));
     if (max_instances < 1 || max_instances > (1 << 20)) return fail(FV_ERR_INVALID, "bad max_instances");
     const int cfg = params->tile < 0 ? 0 : params->tile;
-    const BEntry* be = find_batch_entry(scheme, cfg);
+    const BEntry* be = find_batch_entry(scheme, cfg, params->variant);
     if (!be) return fail(FV_ERR_INVALID, "no batched kernel for scheme %d (tile %d)", scheme, cfg);
     FV_CK(cudaSetDevice(ctx->device));
     FV_CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(be->fn), cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1291,7 +1340,6 @@ int fv_batch_add(fv_batch* b, int nx, int ny, float dx, float dy, int bc, const 
     I.gamma = b->p.gamma;
     I.theta = b->p.theta;
     I.dt_scale = b->dt_scale;
-    I.variant = b->p.variant;
     I.variant_beta = b->p.variant_beta;
     auto enc = encode_fn();
     for (int k = 0; k < 2; ++k)

@@ -72,8 +72,7 @@ struct StageArgs {
     int explicit_dt;     // take the step dt from dt_step instead of the control block
     float dt_step;
     int want_sums;       // compute FP64 sums of the new state at the end of a step
-    int variant;         // HLL: flux variant; WAF: flux limiter (0 = the reference's)
-    float variant_beta;  // parameter of the Osher and Sweby limiters
+    float variant_beta;  // parameter of the Osher and Sweby limiters (the variant itself is a kernel template)
 };
 
 // Storage: per variable, rows y = -2 .. ny+1 and columns x = -4 .. pitch-5,
@@ -465,14 +464,14 @@ __device__ __forceinline__ void walk_mh(float* line, int step, int a, int b, con
 
 // Two-point flux walker (FORCE, HLL: GPUSimulators/cuda/SWE2D_FORCE.cu:29-81,
 // SWE2D_HLL.cu:32-86).  pre holds Q[a-1] (slot 1) and Q[b] (slot 2).
-// For HLL, `variant` picks the flux: 0 HLL, 1 HLLC, 2 Godunov centred.
-template <int SCHEME, bool SWAP, int PS>
+// For HLL, VAR picks the flux: 0 HLL, 1 HLLC, 2 Godunov centred.
+template <int SCHEME, bool SWAP, int PS, int VAR>
 __device__ __forceinline__ void walk_2pt(float* line, int step, int a, int b, const float (&pre)[4][3], float g,
-                                         float half_g, float kx, float kw, float kdx, int variant) {
+                                         float half_g, float kx, float kw, float kdx) {
     auto face_flux = [&](const SweFace& l, const SweFace& r, float (&F)[3]) {
-        if (SCHEME == FORCE) swe_force(l, r, g, half_g, kx, kw, F);
-        else if (variant == 1) swe_hllc(l, r, F);
-        else if (variant == 2) swe_godc(l, r, g, half_g, kdx, F);
+        if constexpr (SCHEME == FORCE) swe_force(l, r, g, half_g, kx, kw, F);
+        else if constexpr (VAR == 1) swe_hllc(l, r, F);
+        else if constexpr (VAR == 2) swe_godc(l, r, g, half_g, kdx, F);
         else swe_hll(l, r, F);
     };
     SweFace sL = swe_face(pre[1][0], pre[1][1], pre[1][2], g, half_g);
@@ -510,9 +509,10 @@ __device__ __forceinline__ void walk_2pt(float* line, int step, int a, int b, co
 // WAF walker (GPUSimulators/cuda/SWE2D_WAF.cu:35-87): the flux at c-1/2 uses
 // cells c-2 .. c+1; per-cell quantities and the star depths of neighbouring
 // pairs are carried along the window.
-template <bool SWAP, int PS>
+template <bool SWAP, int PS, int LIM>
 __device__ __forceinline__ void walk_waf(float* line, int step, int a, int b, const float (&pre)[4][3], float g,
-                                         float half_g, float inv_g, float dtdx, float kdx, int limiter, float beta) {
+                                         float half_g, float inv_g, float dtdx, float kdx, float beta) {
+    constexpr int limiter = LIM;
     WafCell C0 = waf_cell(pre[0], g, half_g);
     WafCell C1 = waf_cell(pre[1], g, half_g);
     float q[3];
@@ -527,9 +527,10 @@ __device__ __forceinline__ void walk_waf(float* line, int step, int a, int b, co
         if (c + 1 < b) {
             ld_cell<3, SWAP, PS>(line, c + 1, step, q);
         } else {
-            const int k = (c + 1 == b) ? 2 : 3;
+            // a select, not pre[k]: a run-time index would put pre in local memory
+            const bool first = (c + 1 == b);
 #pragma unroll
-            for (int v = 0; v < 3; ++v) q[v] = pre[k][v];
+            for (int v = 0; v < 3; ++v) q[v] = first ? pre[2][v] : pre[3][v];
         }
         C0 = C1;
         C1 = C2;
@@ -554,11 +555,12 @@ struct SweepPar {
     float theta, g, half_g, inv_g, gamma;
     float kdt;   // kernel dt
     float dxx;   // cell size along the sweep
-    int variant;  // HLL: flux variant; WAF: flux limiter (see walk_2pt, flux_limiter)
     float beta;   // parameter of the Osher and Sweby limiters
 };
 
-template <int SCHEME, bool SWAP, int PS>
+// VAR: HLL's flux variant or WAF's limiter (walk_2pt, flux_limiter); 0 is the
+// reference's.  It is a template parameter so that each kernel inlines one.
+template <int SCHEME, bool SWAP, int PS, int VAR>
 __device__ __forceinline__ void walk_line(float* line, int step, int a, int b, const float (&pre)[4][(SCHEME == EE2D) ? 4 : 3],
                                           const SweepPar& p) {
     const float kdx = p.kdt / p.dxx;
@@ -570,15 +572,15 @@ __device__ __forceinline__ void walk_line(float* line, int step, int a, int b, c
         // x sweeps use HLL, y sweeps central-upwind (GPUSimulators/cuda/EE2D_KP07_dimsplit.cu:62, :106)
         walk_mh<EulerPhys, !SWAP, SWAP, PS>(line, step, a, b, pre, P, kdx);
     } else if constexpr (SCHEME == WAF) {
-        walk_waf<SWAP, PS>(line, step, a, b, pre, p.g, p.half_g, p.inv_g, kdx, kdx, p.variant, p.beta);
+        walk_waf<SWAP, PS, VAR>(line, step, a, b, pre, p.g, p.half_g, p.inv_g, kdx, kdx, p.beta);
     } else {
-        walk_2pt<SCHEME, SWAP, PS>(line, step, a, b, pre, p.g, p.half_g, p.dxx / (2.0f * p.kdt),
-                                   p.kdt / (2.0f * p.dxx), kdx, p.variant);
+        walk_2pt<SCHEME, SWAP, PS, VAR>(line, step, a, b, pre, p.g, p.half_g, p.dxx / (2.0f * p.kdt),
+                                        p.kdt / (2.0f * p.dxx), kdx);
     }
 }
 
 // x sweep over tile rows [t0, t1): interior columns updated in place.
-template <int SCHEME, int NV, int W, int H, int NT>
+template <int SCHEME, int NV, int W, int H, int NT, int VAR>
 __device__ __forceinline__ void sweep_x(float* Qs, int t0, int t1, const SweepPar& p) {
     constexpr int SP = W + 8, PS = SP * (H + 4), NSEG = 4, R = W / NSEG;
     const int item = threadIdx.x;
@@ -594,12 +596,12 @@ __device__ __forceinline__ void sweep_x(float* Qs, int t0, int t1, const SweepPa
         ld_cell<NV, false, PS>(line, b + 1, 1, pre[3]);
     }
     __syncthreads();
-    if (has) walk_line<SCHEME, false, PS>(line, 1, a, b, pre, p);
+    if (has) walk_line<SCHEME, false, PS, VAR>(line, 1, a, b, pre, p);
     __syncthreads();
 }
 
 // y sweep over tile columns [s0, s1): interior rows updated in place.
-template <int SCHEME, int NV, int W, int H, int NT>
+template <int SCHEME, int NV, int W, int H, int NT, int VAR>
 __device__ __forceinline__ void sweep_y(float* Qs, int s0, int s1, const SweepPar& p) {
     constexpr int SP = W + 8, PS = SP * (H + 4);
     constexpr int NSEG = NT / (W + 4), R = H / NSEG;
@@ -617,7 +619,7 @@ __device__ __forceinline__ void sweep_y(float* Qs, int s0, int s1, const SweepPa
         ld_cell<NV, true, PS>(line, b + 1, SP, pre[3]);
     }
     __syncthreads();
-    if (has) walk_line<SCHEME, true, PS>(line, SP, a, b, pre, p);
+    if (has) walk_line<SCHEME, true, PS, VAR>(line, SP, a, b, pre, p);
     __syncthreads();
 }
 
@@ -628,15 +630,14 @@ struct SplitPar {
     float dx, dy, g, gamma, theta;
     float kdt;  // kernel dt of this substep
     int substep;
-    int variant;  // flux variant (HLL) or limiter (WAF)
-    float beta;
+    float beta;  // parameter of the Osher and Sweby limiters
 };
 
 // Load, ghost cells, both sweeps and copy-out of one tile of a split scheme
 // (FORCE, HLL, HLL2, WAF, KP07_dimsplit, EE2D).  Accumulates the tile's CFL
 // minimum and FP64 sums into the per-thread values.  Returns false if the tile
 // load gave up (nothing was written).
-template <int SCHEME, int W, int H, int NT, bool GLOBAL_TMAP = false>
+template <int SCHEME, int W, int H, int NT, bool GLOBAL_TMAP = false, int VAR = 0>
 __device__ bool process_tile_dimsplit(float* Qs, uint64_t* bar, uint32_t phase, bool init_bar, const TileJob& J,
                                       const SplitPar& P, bool do_cfl, bool sums, int* err, float& my_cfl,
                                       double (&my_sums)[(SCHEME == EE2D) ? 4 : 3]) {
@@ -657,19 +658,18 @@ __device__ bool process_tile_dimsplit(float* Qs, uint64_t* bar, uint32_t phase, 
     p.inv_g = 1.0f / P.g;
     p.gamma = P.gamma;
     p.kdt = P.kdt;
-    p.variant = P.variant;
     p.beta = P.beta;
     const bool x_first = (SCHEME == FORCE || SCHEME == HLL) ? true : (P.substep == 0);
     if (x_first) {
         p.dxx = P.dx;
-        sweep_x<SCHEME, NV, W, H, NT>(Qs, 2 - G, H + 2 + G, p);
+        sweep_x<SCHEME, NV, W, H, NT, VAR>(Qs, 2 - G, H + 2 + G, p);
         p.dxx = P.dy;
-        sweep_y<SCHEME, NV, W, H, NT>(Qs, 4, W + 4, p);
+        sweep_y<SCHEME, NV, W, H, NT, VAR>(Qs, 4, W + 4, p);
     } else {
         p.dxx = P.dy;
-        sweep_y<SCHEME, NV, W, H, NT>(Qs, 4 - G, W + 4 + G, p);
+        sweep_y<SCHEME, NV, W, H, NT, VAR>(Qs, 4 - G, W + 4 + G, p);
         p.dxx = P.dx;
-        sweep_x<SCHEME, NV, W, H, NT>(Qs, 2, H + 2, p);
+        sweep_x<SCHEME, NV, W, H, NT, VAR>(Qs, 2, H + 2, p);
     }
 
     // copy-out of the interior (+ gravity source, CFL, sums)
@@ -728,7 +728,7 @@ __device__ bool process_tile_dimsplit(float* Qs, uint64_t* bar, uint32_t phase, 
     return true;
 }
 
-template <int SCHEME, int W, int H, int NT>
+template <int SCHEME, int W, int H, int NT, int VAR = 0>
 __global__ void __launch_bounds__(NT) dimsplit_stage_kernel(const __grid_constant__ StageArgs A) {
     constexpr int NV = (SCHEME == EE2D) ? 4 : 3;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -754,8 +754,8 @@ __global__ void __launch_bounds__(NT) dimsplit_stage_kernel(const __grid_constan
     J.bc = A.bc;
     J.x0 = blockIdx.x * W;
     J.y0 = blockIdx.y * H;
-    SplitPar P{A.dx, A.dy, A.g, A.gamma, A.theta, sc.dt * A.dt_scale, A.substep, A.variant, A.variant_beta};
-    process_tile_dimsplit<SCHEME, W, H, NT>(Qs, &bar, 0, true, J, P, sc.do_cfl, sums, &A.ctl->error, my_cfl, my_sums);
+    SplitPar P{A.dx, A.dy, A.g, A.gamma, A.theta, sc.dt * A.dt_scale, A.substep, A.variant_beta};
+    process_tile_dimsplit<SCHEME, W, H, NT, false, VAR>(Qs, &bar, 0, true, J, P, sc.do_cfl, sums, &A.ctl->error, my_cfl, my_sums);
     stage_epilogue<NT, NV>(A, sc, my_cfl, my_sums, sums);
 }
 
@@ -772,8 +772,7 @@ struct alignas(64) BatchInstance {
     int nx, ny, pitch, bc;
     int tiles_x, ntiles;
     float dx, dy, g, gamma, theta, dt_scale;
-    int variant;         // flux variant (HLL) or limiter (WAF)
-    float variant_beta;
+    float variant_beta;  // parameter of the Osher and Sweby limiters
 };
 
 struct BatchArgs {
@@ -792,7 +791,7 @@ struct BatchArgs {
 // control block exactly as the single-simulation kernel does.  Simulations
 // that reached t_end are skipped.  The work list lives in device memory, so
 // one captured CUDA graph serves any batch composition.
-template <int SCHEME, int W, int H, int NT>
+template <int SCHEME, int W, int H, int NT, int VAR = 0>
 __global__ void __launch_bounds__(NT) batched_stage_kernel(const __grid_constant__ BatchArgs B) {
     constexpr int NV = (SCHEME == EE2D) ? 4 : 3;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -823,8 +822,8 @@ __global__ void __launch_bounds__(NT) batched_stage_kernel(const __grid_constant
         const int ty = job.y / I.tiles_x;
         J.x0 = (job.y - ty * I.tiles_x) * W;
         J.y0 = ty * H;
-        SplitPar P{I.dx, I.dy, I.g, I.gamma, I.theta, sc.dt * I.dt_scale, B.substep, I.variant, I.variant_beta};
-        process_tile_dimsplit<SCHEME, W, H, NT, true>(Qs, &bar, phase, init, J, P, sc.do_cfl, sums, B.err, my_cfl,
+        SplitPar P{I.dx, I.dy, I.g, I.gamma, I.theta, sc.dt * I.dt_scale, B.substep, I.variant_beta};
+        process_tile_dimsplit<SCHEME, W, H, NT, true, VAR>(Qs, &bar, phase, init, J, P, sc.do_cfl, sums, B.err, my_cfl,
                                                       my_sums);
         init = false;
         phase ^= 1u;
