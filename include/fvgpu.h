@@ -61,7 +61,8 @@ typedef struct fv_params {
      * HLL's flux (0 HLL, 1 HLLC, 2 Godunov centred) or WAF's limiter (0 the
      * reference's generalized minmod with theta 1.9, 1 minmod, 2 superbee,
      * 3 van Leer, 4 van Albada 1, 5 van Albada 2, 6 monotonized central,
-     * 7 Osher, 8 Sweby); 0 for every other scheme. */
+     * 7 Osher, 8 Sweby); 0 for every other scheme.  Each variant other
+     * than 0 has one kernel of its own, and `tile` is then ignored. */
     int variant;
     float variant_beta; /* beta of the Osher and Sweby limiters */
 } fv_params;
