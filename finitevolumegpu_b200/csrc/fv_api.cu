@@ -615,9 +615,12 @@ int fv_context_create(int device, fv_context** out) {
     FV_CK(cudaGetDeviceProperties(&prop, device));
     if (prop.major != 10) return fail(FV_ERR_UNSUPPORTED, "libfvgpu is built for sm_100a; device is sm_%d%d", prop.major, prop.minor);
     if (!encode_fn()) return fail(FV_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
-    for (int i = 0; i < kNumEntries; ++i)
+    for (int i = 0; i < kNumEntries; ++i) {
         FV_CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(kTable[i].fn),
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)entry_smem(kTable[i])));
+        FV_CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(kTable[i].fn),
+                                   cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    }
     for (int i = 0; i < kNumVariants; ++i)
         FV_CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(kVariantTable[i].k.fn),
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)entry_smem(kVariantTable[i].k)));

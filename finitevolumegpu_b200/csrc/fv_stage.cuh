@@ -38,7 +38,7 @@ __host__ __device__ inline int bc_east(int bc) { return (bc >> 8) & 0xF; }
 __host__ __device__ inline int bc_west(int bc) { return bc & 0xF; }
 
 // Control block of one simulation, resident in device memory.
-struct SimCtl {
+struct alignas(16) SimCtl {
     double t;          // simulation time (BaseSimulator.t, FP64)
     double t_end;      // end time of the current simulate() call
     long long nt;      // completed steps (BaseSimulator.nt)
@@ -94,25 +94,43 @@ struct StepCtl {
 // dt of the current step: float32(min(dt, t_end - t)) (GPUSimulators/Simulator.py:199),
 // with Python's min() tie and NaN behaviour; a step runs while t < t_end and
 // dt > 0 (Simulator.py:192, :202).
+//
+// The control block changes only between launches, or in this launch after
+// every tile of the simulation has read it (the last tile's epilogue), so its
+// first 48 bytes are read with three 16-byte relaxed loads issued together: one
+// L2 round trip per warp instead of one per field.
+__device__ __forceinline__ int4 ld_relaxed_v4(const void* p) {
+    int4 r;
+    asm volatile("ld.relaxed.gpu.global.v4.s32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+                 : "l"(p));
+    return r;
+}
+
 __device__ __forceinline__ StepCtl read_step(const SimCtl* ctl, bool explicit_dt, float dt_step, bool force_cfl,
                                              bool is_last) {
-    const volatile SimCtl* c = ctl;
+    static_assert(offsetof(SimCtl, t_end) == 8 && offsetof(SimCtl, nt) == 16 && offsetof(SimCtl, dt) == 24 &&
+                      offsetof(SimCtl, update_dt) == 40 && offsetof(SimCtl, cur) == 44,
+                  "read_step's vector loads follow SimCtl's layout");
+    const int4 w0 = ld_relaxed_v4(ctl);                                          // t, t_end
+    const int4 w1 = ld_relaxed_v4(reinterpret_cast<const char*>(ctl) + 16);      // nt, dt, cfl_min
+    const int4 w2 = ld_relaxed_v4(reinterpret_cast<const char*>(ctl) + 32);      // factor, cfl_scale, update_dt, cur
     StepCtl s;
-    s.cur = c->cur;
-    const double t = c->t;
-    const double t_end = c->t_end;
+    s.cur = w2.w;
+    const double t = __hiloint2double(w0.y, w0.x);
+    const double t_end = __hiloint2double(w0.w, w0.z);
     if (explicit_dt) {
         s.dt = dt_step;
         s.active = true;
     } else {
         const double rem = t_end - t;
-        const double d = (double)c->dt;
+        const double d = (double)__int_as_float(w1.z);
         s.dt = (float)((rem < d) ? rem : d);
         s.active = (t < t_end) && !(s.dt <= 0.0f);
     }
     s.t_new = t + (double)s.dt;
-    const long long nt = c->nt;
-    const bool sched = c->update_dt && ((nt + 1) % 100 == 0);
+    const long long nt = (long long)(((unsigned long long)(unsigned)w1.y << 32) | (unsigned)w1.x);
+    const bool sched = w2.z && ((nt + 1) % 100 == 0);
     s.do_cfl = force_cfl || (is_last && !explicit_dt && (sched || !(s.t_new < t_end)));
     return s;
 }
