@@ -226,20 +226,26 @@ __device__ __forceinline__ void swe_hll(const SweFace& l, const SweFace& r, floa
 // minmod slope, face values Q -+ slope/2, and the half-step predictor
 // Q_face + dt/(2dx) * (F(Q_west) - F(Q_east)), which is the same flux
 // difference for both faces of the cell.  w/e: predicted west/east face states.
-// bd holds theta*(q0 - qm) on entry and theta*(qp - q0) on return: a cell's
+// bd holds theta2*(q0 - qm) on entry and theta2*(qp - q0) on return: a cell's
 // forward difference is the backward difference of the next one, so a line
 // walker computes each difference once.
+//
+// The slope is formed at twice its size: with theta2 = 2*theta, minmod of
+// (theta2*b, qp - qm, theta2*f) is exactly 2 * minmod(theta*b, (qp - qm)/2,
+// theta*f), since scaling by 2 commutes with rounding, and the face values
+// q0 -+ s2/4 equal q0 -+ s/2 bit for bit.  This saves the multiply of the
+// central difference.
 __device__ __forceinline__ void swe_muscl_hancock(const float (&qm)[3], const float (&q0)[3], const float (&qp)[3],
-                                                  float (&bd)[3], float theta, float g, float half_g, float k2,
+                                                  float (&bd)[3], float theta2, float g, float half_g, float k2,
                                                   SweFace& w, SweFace& e) {
     float W[3], E[3];
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
-        const float f = fmul(fsub(qp[v], q0[v]), theta);
-        const float s = minmod3(bd[v], fmul(fsub(qp[v], qm[v]), 0.5f), f);
+        const float f = fmul(fsub(qp[v], q0[v]), theta2);
+        const float s2 = minmod3(bd[v], fsub(qp[v], qm[v]), f);
         bd[v] = f;
-        W[v] = ffma(-0.5f, s, q0[v]);
-        E[v] = ffma(0.5f, s, q0[v]);
+        W[v] = ffma(-0.25f, s2, q0[v]);
+        E[v] = ffma(0.25f, s2, q0[v]);
     }
     const float uw = W[1] / W[0];
     const float ue = E[1] / E[0];
@@ -317,18 +323,19 @@ __device__ __forceinline__ void euler_hll(const EulerFace& l, const EulerFace& r
 // (GPUSimulators/cuda/EE2D_KP07_dimsplit.cu:33-58 and :78-103).  The reference's
 // predictor calls F_func(Q, gamma_), whose second argument is the pressure, so
 // the predictor flux uses gamma in place of P; that is reproduced here.
-// bd: theta*(q0 - qm) on entry, theta*(qp - q0) on return (as in swe_muscl_hancock).
+// bd: theta2*(q0 - qm) on entry, theta2*(qp - q0) on return, theta2 = 2*theta,
+// and the slope at twice its size (as in swe_muscl_hancock).
 __device__ __forceinline__ void euler_muscl_hancock(const float (&qm)[4], const float (&q0)[4], const float (&qp)[4],
-                                                    float (&bd)[4], float theta, float gamma, float k2, EulerFace& w,
+                                                    float (&bd)[4], float theta2, float gamma, float k2, EulerFace& w,
                                                     EulerFace& e) {
     float W[4], E[4];
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-        const float f = fmul(fsub(qp[v], q0[v]), theta);
-        const float s = minmod3(bd[v], fmul(fsub(qp[v], qm[v]), 0.5f), f);
+        const float f = fmul(fsub(qp[v], q0[v]), theta2);
+        const float s2 = minmod3(bd[v], fsub(qp[v], qm[v]), f);
         bd[v] = f;
-        W[v] = ffma(-0.5f, s, q0[v]);
-        E[v] = ffma(0.5f, s, q0[v]);
+        W[v] = ffma(-0.25f, s2, q0[v]);
+        E[v] = ffma(0.25f, s2, q0[v]);
     }
     const float uw = W[1] / W[0];
     const float ue = E[1] / E[0];

@@ -389,10 +389,10 @@ __device__ __forceinline__ void st_cell(float* line, int k, int step, const floa
 struct SwePhys {
     static constexpr int NV = 3;
     using Face = SweFace;
-    float theta, g, half_g, k2;
+    float theta2, g, half_g, k2;  // theta2 = 2 * theta (swe_muscl_hancock)
     __device__ __forceinline__ void recon(const float (&qm)[3], const float (&q0)[3], const float (&qp)[3],
                                           float (&bd)[3], Face& w, Face& e) const {
-        swe_muscl_hancock(qm, q0, qp, bd, theta, g, half_g, k2, w, e);
+        swe_muscl_hancock(qm, q0, qp, bd, theta2, g, half_g, k2, w, e);
     }
     template <bool HLLF> __device__ __forceinline__ static void flux(const Face& l, const Face& r, float (&F)[3]) {
         if (HLLF) swe_hll(l, r, F);
@@ -403,10 +403,10 @@ struct SwePhys {
 struct EulerPhys {
     static constexpr int NV = 4;
     using Face = EulerFace;
-    float theta, gamma, k2;
+    float theta2, gamma, k2;  // theta2 = 2 * theta
     __device__ __forceinline__ void recon(const float (&qm)[4], const float (&q0)[4], const float (&qp)[4],
                                           float (&bd)[4], Face& w, Face& e) const {
-        euler_muscl_hancock(qm, q0, qp, bd, theta, gamma, k2, w, e);
+        euler_muscl_hancock(qm, q0, qp, bd, theta2, gamma, k2, w, e);
     }
     template <bool HLLF> __device__ __forceinline__ static void flux(const Face& l, const Face& r, float (&F)[4]) {
         if (HLLF) euler_hll(l, r, F);
@@ -464,7 +464,7 @@ __device__ __forceinline__ void walk_mh(float* line, int step, int a, int b, con
             qm[v] = q0[v];
             q0[v] = qp[v];
             qp[v] = qn[v];
-            bd[v] = fmul(fsub(q0[v], qm[v]), P.theta);
+            bd[v] = fmul(fsub(q0[v], qm[v]), P.theta2);
         }
         typename Phys::Face w;
         P.recon(qm, q0, qp, bd, w, eL);
@@ -583,10 +583,10 @@ __device__ __forceinline__ void walk_line(float* line, int step, int a, int b, c
                                           const SweepPar& p) {
     const float kdx = p.kdt / p.dxx;
     if constexpr (SCHEME == KP07_DIMSPLIT || SCHEME == HLL2) {
-        const SwePhys P{p.theta, p.g, p.half_g, p.kdt / (2.0f * p.dxx)};
+        const SwePhys P{2.0f * p.theta, p.g, p.half_g, p.kdt / (2.0f * p.dxx)};
         walk_mh<SwePhys, SCHEME == HLL2, SWAP, PS>(line, step, a, b, pre, P, kdx);
     } else if constexpr (SCHEME == EE2D) {
-        const EulerPhys P{p.theta, p.gamma, p.kdt / (2.0f * p.dxx)};
+        const EulerPhys P{2.0f * p.theta, p.gamma, p.kdt / (2.0f * p.dxx)};
         // x sweeps use HLL, y sweeps central-upwind (GPUSimulators/cuda/EE2D_KP07_dimsplit.cu:62, :106)
         walk_mh<EulerPhys, !SWAP, SWAP, PS>(line, step, a, b, pre, P, kdx);
     } else if constexpr (SCHEME == WAF) {
