@@ -120,11 +120,27 @@ __device__ __forceinline__ float ffma(float a, float b, float c) {
 // magnitude with b's sign, or zero.
 // minmod3 takes the scaled differences b = theta*(center - left),
 // c = (right - left)/2 and f = theta*(right - center).
+//
+// It is computed with min/max only.  With lo and hi the smallest and largest
+// of the three: all positive gives lo, all negative gives hi (the one nearest
+// zero), and mixed signs give max(lo, min(hi, 0)) = 0.  NaN follows the
+// reference's sign test, which reads a NaN's sign bit and drops it from the
+// magnitude min: the differences come from FP32 arithmetic, so a NaN among
+// them is the canonical positive NaN and acts as +infinity.  hi and the final
+// max therefore propagate NaN (max.NaN; it reaches the result only when all
+// three are NaN, as the reference's 0.25*...*NaN does), lo drops it (fminf).
+// A zero slope may come out as -0 where the sign test gave +0, which changes
+// no nonzero value.
+__device__ __forceinline__ float fmax_nan(float a, float b) {
+    float r;
+    asm("max.NaN.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    return r;
+}
+
 __device__ __forceinline__ float minmod3(float b, float c, float f) {
-    const float mag = fminf(fminf(fabsf(b), fabsf(c)), fabsf(f));
-    const uint32_t sb = __float_as_uint(b), sc = __float_as_uint(c), sf = __float_as_uint(f);
-    const bool same = (((sb ^ sc) | (sc ^ sf)) & 0x80000000u) == 0u;
-    return same ? copysignf(mag, b) : 0.0f;
+    const float lo = fminf(fminf(b, c), f);
+    const float hi = fmax_nan(fmax_nan(b, c), f);
+    return fmax_nan(lo, fminf(hi, 0.0f));
 }
 
 __device__ __forceinline__ float minmod_slope(float left, float center, float right, float theta) {

@@ -472,6 +472,9 @@ __device__ __forceinline__ void walk_mh(float* line, int step, int a, int b, con
     // c = a: first face, no update
     ld_cell<NV, SWAP, PS>(line, a + 1, step, qn);
     mh_step<Phys, HLLF, SWAP, PS>(line, step, a, qm, q0, qp, qn, bd, eL, Fprev, P, kdx, false);
+    // unrolled by the window's length, so the rotation of the three-cell
+    // window becomes register renaming instead of moves
+#pragma unroll 3
     for (int c = a + 1; c < b - 1; ++c) {
         ld_cell<NV, SWAP, PS>(line, c + 1, step, qn);
         mh_step<Phys, HLLF, SWAP, PS>(line, step, c, qm, q0, qp, qn, bd, eL, Fprev, P, kdx, true);
