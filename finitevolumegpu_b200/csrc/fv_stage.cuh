@@ -503,6 +503,7 @@ __device__ __forceinline__ void walk_2pt(float* line, int step, int a, int b, co
     face_flux(sL, s, Fprev);
     float qprev[3] = {qa[0], qa[1], qa[2]};
     sL = s;
+#pragma unroll 2
     for (int c = a + 1; c <= b; ++c) {
         float q[3];
         if (c < b) {
@@ -544,6 +545,7 @@ __device__ __forceinline__ void walk_waf(float* line, int step, int a, int b, co
     float hs01 = waf_h_star(C0, C1, inv_g), hs12 = waf_h_star(C1, C2, inv_g), hs23 = waf_h_star(C2, C3, inv_g);
     float Fprev[3];
     waf_flux(C0, C1, C2, C3, hs01, hs12, hs23, dtdx, Fprev, limiter, beta);  // face a-1/2
+#pragma unroll 4
     for (int c = a + 1; c <= b; ++c) {
         if (c + 1 < b) {
             ld_cell<3, SWAP, PS>(line, c + 1, step, q);
