@@ -147,6 +147,12 @@ __device__ __forceinline__ float minmod_slope(float left, float center, float ri
     return minmod3(fmul(fsub(center, left), theta), fmul(fsub(right, left), 0.5f), fmul(fsub(right, center), theta));
 }
 
+// Twice minmod_slope, bit for bit, without the multiply of the central
+// difference: theta2 = 2 * theta (scaling by 2 commutes with rounding).
+__device__ __forceinline__ float minmod_slope2(float left, float center, float right, float theta2) {
+    return minmod3(fmul(fsub(center, left), theta2), fsub(right, left), fmul(fsub(right, center), theta2));
+}
+
 // GPUSimulators/cuda/limiters.h:100-102
 __device__ __forceinline__ float generalized_minmod(float r, float theta) {
     return fmaxf(0.0f, fminf(theta * r, fminf((1.0f + r) * 0.5f, theta)));

@@ -910,7 +910,7 @@ __global__ void __launch_bounds__(NT) unsplit_stage_kernel(const __grid_constant
     if (load_tile<3, SP, TR>(Qs, J.tmap, x0, y0, &bar, 0, true, &A.ctl->error)) {
         if (x0 == 0 || x0 + W + 2 > A.nx || y0 == 0 || y0 + H + 2 > A.ny) apply_boundary<3, W, H, NT>(Qs, J);
         const float kdt = sc.dt * A.dt_scale;
-        const float g = A.g, half_g = 0.5f * g, theta = A.theta;
+        const float g = A.g, half_g = 0.5f * g, theta2 = 2.0f * A.theta;
         const float k4x = A.dx / (4.0f * kdt), k4y = A.dy / (4.0f * kdt);
         const float kdx = kdt / A.dx, kdy = kdt / A.dy;
         const int out = sc.cur ^ 1;
@@ -930,9 +930,12 @@ __global__ void __launch_bounds__(NT) unsplit_stage_kernel(const __grid_constant
         };
         // y-face states of row t (south, north) from rows t-1, t, t+1 of this
         // column, components swapped to (h, hv, hu) as computeFluxG does
-        // (GPUSimulators/cuda/SWE2D_KP07.cu:117-131)
-        auto ystates = [&](const float (&qm)[3], const float (&q0)[3], const float (&qp)[3], SweFace& sf,
-                           SweFace& nf) {
+        // (GPUSimulators/cuda/SWE2D_KP07.cu:117-131).  The slope is formed at
+        // twice its size (minmod_slope2); bd carries theta2*(q0 - qm) in and
+        // theta2*(qp - q0) out, in q's component order, since a row's forward
+        // difference is the next row's backward one.
+        auto ystates = [&](const float (&qm)[3], const float (&q0)[3], const float (&qp)[3], float (&bd)[3],
+                           SweFace& sf, SweFace& nf) {
             float sv[3], nv[3];
 #pragma unroll
             for (int v = 0; v < 3; ++v) {
@@ -940,9 +943,11 @@ __global__ void __launch_bounds__(NT) unsplit_stage_kernel(const __grid_constant
                 if (SCHEME == LXF) {
                     sv[v] = nv[v] = q0[k];
                 } else {
-                    const float sl = minmod_slope(qm[k], q0[k], qp[k], theta);
-                    sv[v] = fmaf(-0.5f, sl, q0[k]);
-                    nv[v] = fmaf(0.5f, sl, q0[k]);
+                    const float f = fmul(fsub(qp[k], q0[k]), theta2);
+                    const float sl2 = minmod3(bd[k], fsub(qp[k], qm[k]), f);
+                    bd[k] = f;
+                    sv[v] = fmaf(-0.25f, sl2, q0[k]);
+                    nv[v] = fmaf(0.25f, sl2, q0[k]);
                 }
             }
             sf = swe_face(sv[0], sv[1], sv[2], g, half_g);
@@ -963,15 +968,20 @@ __global__ void __launch_bounds__(NT) unsplit_stage_kernel(const __grid_constant
         qat(a, s, q0);
         qat(a + 1, s, qp);
         SweFace s_cur, n_cur, n_prev;
+        float bdy[3];
         {
             float qmm[3];
             qat(a - 2, s, qmm);
+#pragma unroll
+            for (int v = 0; v < 3; ++v) bdy[v] = fmul(fsub(qm[v], qmm[v]), theta2);
             SweFace sd;
-            ystates(qmm, qm, q0, sd, n_prev);  // row a-1
+            ystates(qmm, qm, q0, bdy, sd, n_prev);  // row a-1
         }
-        ystates(qm, q0, qp, s_cur, n_cur);  // row a
+        ystates(qm, q0, qp, bdy, s_cur, n_cur);  // row a
         float Gs[3];
         yflux(n_prev, s_cur, Gs);  // south face of row a
+        // unrolled by the row window's length: its rotation becomes renaming
+#pragma unroll 3
         for (int t = a; t < b; ++t) {
             const int y = y0 + t - 2;
             const bool store = owner && x < A.nx && y < A.ny;
@@ -991,9 +1001,9 @@ __global__ void __launch_bounds__(NT) unsplit_stage_kernel(const __grid_constant
                 qat(t, s + 1, qr);
 #pragma unroll
                 for (int v = 0; v < 3; ++v) {
-                    const float sl = minmod_slope(ql[v], q0[v], qr[v], theta);
-                    wv[v] = fmaf(-0.5f, sl, q0[v]);
-                    ev[v] = fmaf(0.5f, sl, q0[v]);
+                    const float sl2 = minmod_slope2(ql[v], q0[v], qr[v], theta2);
+                    wv[v] = fmaf(-0.25f, sl2, q0[v]);
+                    ev[v] = fmaf(0.25f, sl2, q0[v]);
                 }
                 fw = swe_face(wv[0], wv[1], wv[2], g, half_g);
                 fe = swe_face(ev[0], ev[1], ev[2], g, half_g);
@@ -1008,7 +1018,7 @@ __global__ void __launch_bounds__(NT) unsplit_stage_kernel(const __grid_constant
             float qn2[3];
             qat(t + 2, s, qn2);
             SweFace s_nxt, n_nxt;
-            ystates(q0, qp, qn2, s_nxt, n_nxt);
+            ystates(q0, qp, qn2, bdy, s_nxt, n_nxt);
             float Gn[3];
             yflux(n_cur, s_nxt, Gn);
             if (store) {
