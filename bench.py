@@ -240,9 +240,17 @@ def run_batched(ctx, n_inst=512, seed=4, check=4):
         ny = int(round(np.exp(rng.uniform(np.log(64), np.log(1024)))))
         q = bump_ic(nx, ny, rng) if rng.random() < 0.5 else dam_ic(nx, ny, rng)
         cases.append((q, nx, ny, float(rng.uniform(5.0, 50.0))))
-    # batched: admit all, run to completion, download all
+    # Warm-up: one untimed admission of the whole workload grows the device
+    # memory pool and the pinned staging ring once, as a long-running service
+    # would have them; the plain path below runs with the same warm pool.
     import torch
 
+    w = Batch(ctx, "KP07_dimsplit", max_instances=n_inst)
+    for (q, nx, ny, t_end) in cases:
+        w.add(q, nx, ny, 1.0, 1.0, t_end)
+    w.sync()
+    del w
+    # batched: admit all, run to completion, download all
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     b = Batch(ctx, "KP07_dimsplit", max_instances=n_inst)
