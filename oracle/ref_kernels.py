@@ -24,17 +24,24 @@ REF_DIR = os.path.join(HERE, "_ref")
 _libs = {}
 
 
-def ref_lib_path(scheme: str) -> str:
-    return os.path.join(REF_DIR, "libref_%s.so" % scheme)
+# Block shapes built besides each kernel's default (oracle/Makefile REF_BLOCKS).
+BLOCKS = ((32, 8), (32, 16), (32, 4), (8, 8))
 
 
-def available(scheme: str = "KP07_dimsplit") -> bool:
-    return os.path.exists(ref_lib_path(scheme))
+def ref_lib_path(scheme: str, block=None) -> str:
+    if block is None:
+        return os.path.join(REF_DIR, "libref_%s.so" % scheme)
+    return os.path.join(REF_DIR, "libref_%s_%dx%d.so" % (scheme, block[0], block[1]))
 
 
-def ref_lib(scheme: str):
-    if scheme not in _libs:
-        L = ctypes.CDLL(ref_lib_path(scheme))
+def available(scheme: str = "KP07_dimsplit", block=None) -> bool:
+    return os.path.exists(ref_lib_path(scheme, block))
+
+
+def ref_lib(scheme: str, block=None):
+    key = (scheme, block)
+    if key not in _libs:
+        L = ctypes.CDLL(ref_lib_path(scheme, block))
         P = ctypes.c_void_p
         L.ref_last_error.restype = ctypes.c_char_p
         L.ref_malloc.argtypes = [ctypes.POINTER(P), ctypes.c_size_t]
@@ -49,8 +56,8 @@ def ref_lib(scheme: str):
         FP = ctypes.POINTER(ctypes.c_float)
         L.ref_substep.argtypes = [ctypes.c_int, ctypes.c_int] + [ctypes.c_float] * 6 + [ctypes.c_int] * 3 + [
             ctypes.POINTER(FP), ctypes.POINTER(FP), ctypes.c_int, FP]
-        _libs[scheme] = L
-    return _libs[scheme]
+        _libs[key] = L
+    return _libs[key]
 
 
 def _ck(L, rc):
@@ -59,12 +66,13 @@ def _ck(L, rc):
 
 
 class RefKernelSim(OracleSim):
-    """OracleSim's host loop with the reference kernels doing the substeps."""
+    """OracleSim's host loop with the reference kernels doing the substeps;
+    `block` = (w, h) picks one of the other block shapes (BLOCKS)."""
 
-    def __init__(self, scheme, variables, nx, ny, dx, dy, g, **kw):
+    def __init__(self, scheme, variables, nx, ny, dx, dy, g, block=None, **kw):
         kw["dtype"] = np.float32
         super().__init__(scheme, variables, nx, ny, dx, dy, g, **kw)
-        self.L = ref_lib(scheme)
+        self.L = ref_lib(scheme, block)
         L = self.L
         self.bw, self.bh = L.ref_block_width(), L.ref_block_height()
         H, W = self.u0[0].shape
