@@ -361,11 +361,41 @@ struct HostStaging {
     }
 };
 
+// Pinned host mirrors of the simulations' control blocks, handed out from
+// chunks of 64 so that creating and destroying a simulation pins and unpins
+// no memory (cudaMallocHost/cudaFreeHost cost milliseconds each).
+struct CtlSlab {
+    static constexpr int kPerChunk = 64;
+    std::mutex mu;
+    std::vector<SimCtl*> chunks;
+    std::vector<SimCtl*> free_list;
+    SimCtl* acquire() {
+        std::lock_guard<std::mutex> lock(mu);
+        if (free_list.empty()) {
+            SimCtl* c = nullptr;
+            if (cudaMallocHost(&c, kPerChunk * sizeof(SimCtl)) != cudaSuccess) return nullptr;
+            chunks.push_back(c);
+            for (int i = kPerChunk - 1; i >= 0; --i) free_list.push_back(c + i);
+        }
+        SimCtl* p = free_list.back();
+        free_list.pop_back();
+        return p;
+    }
+    void release(SimCtl* p) {
+        std::lock_guard<std::mutex> lock(mu);
+        free_list.push_back(p);
+    }
+    ~CtlSlab() {
+        for (SimCtl* c : chunks) cudaFreeHost(c);
+    }
+};
+
 struct fv_context {
     int device = 0;
     int sm_count = 0;
     char name[256] = {0};
     HostStaging staging;
+    CtlSlab ctl_slab;
 };
 
 struct fv_sim {
@@ -376,9 +406,10 @@ struct fv_sim {
     int bc = 0;
     float dt_scale = 1.0f;
     float factor = 0.5f;
+    void* mem = nullptr;      // one pool allocation: both buffers, control block, scratch
     float* buf[2][4] = {{nullptr}};
     SimCtl* ctl = nullptr;    // device
-    SimCtl* ctl_h = nullptr;  // pinned host mirror
+    SimCtl* ctl_h = nullptr;  // pinned host mirror (from the context's slab)
     float* block_cfl = nullptr;
     double* block_sums = nullptr;
     double* sum_part = nullptr;
@@ -711,21 +742,35 @@ int fv_sim_create(fv_context* ctx, int scheme, int nx, int ny, float dx, float d
     };
     if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
         return cleanup(fail(FV_ERR_CUDA, "stream creation failed"));
+    // One stream-ordered allocation, zero-filled, holds both state buffers
+    // (planes of 128-byte-aligned rows) and the small device objects; no
+    // cudaMalloc/cudaFree, which synchronise the device, on create or destroy.
     const size_t plane = (size_t)(ny + 4) * s->pitch * sizeof(float);
-    for (int b = 0; b < 2; ++b)
-        for (int v = 0; v < nv; ++v) {
-            if (cudaMallocAsync(&s->buf[b][v], plane, s->stream) != cudaSuccess)
-                return cleanup(fail(FV_ERR_NOMEM, "out of device memory"));
-            if (cudaMemsetAsync(s->buf[b][v], 0, plane, s->stream) != cudaSuccess)
-                return cleanup(fail(FV_ERR_CUDA, "memset failed"));
-        }
     const size_t nblocks = (size_t)s->grid.x * s->grid.y;
-    if (cudaMalloc(&s->ctl, sizeof(SimCtl)) != cudaSuccess || cudaMallocHost(&s->ctl_h, sizeof(SimCtl)) != cudaSuccess ||
-        cudaMalloc(&s->block_cfl, nblocks * sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&s->block_sums, nblocks * 4 * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&s->sum_part, (size_t)(ny + 1) * sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&s->flag, sizeof(int)) != cudaSuccess)
+    auto r256 = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t off_ctl = 2 * nv * plane;
+    const size_t off_cfl = off_ctl + r256(sizeof(SimCtl));
+    const size_t off_sums = off_cfl + r256(nblocks * sizeof(float));
+    const size_t off_part = off_sums + r256(nblocks * 4 * sizeof(double));
+    const size_t off_flag = off_part + r256((size_t)(ny + 1) * sizeof(double));
+    const size_t total = off_flag + 256;
+    if (cudaMallocAsync(&s->mem, total, s->stream) != cudaSuccess) {
+        cudaGetLastError();
+        s->mem = nullptr;
         return cleanup(fail(FV_ERR_NOMEM, "out of device memory"));
+    }
+    if (cudaMemsetAsync(s->mem, 0, total, s->stream) != cudaSuccess)
+        return cleanup(fail(FV_ERR_CUDA, "memset failed"));
+    char* base = static_cast<char*>(s->mem);
+    for (int b = 0; b < 2; ++b)
+        for (int v = 0; v < nv; ++v) s->buf[b][v] = reinterpret_cast<float*>(base + (size_t)(b * nv + v) * plane);
+    s->ctl = reinterpret_cast<SimCtl*>(base + off_ctl);
+    s->block_cfl = reinterpret_cast<float*>(base + off_cfl);
+    s->block_sums = reinterpret_cast<double*>(base + off_sums);
+    s->sum_part = reinterpret_cast<double*>(base + off_part);
+    s->flag = reinterpret_cast<int*>(base + off_flag);
+    s->ctl_h = ctx->ctl_slab.acquire();
+    if (!s->ctl_h) return cleanup(fail(FV_ERR_NOMEM, "out of pinned host memory"));
     if (cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess)
         return cleanup(fail(FV_ERR_CUDA, "event creation failed"));
 
@@ -799,15 +844,8 @@ int fv_sim_destroy(fv_sim* s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     if (s->graph1) cudaGraphExecDestroy(s->graph1);
     if (s->graph16) cudaGraphExecDestroy(s->graph16);
-    for (int b = 0; b < 2; ++b)
-        for (int v = 0; v < 4; ++v)
-            if (s->buf[b][v]) cudaFreeAsync(s->buf[b][v], s->stream);
-    if (s->ctl) cudaFree(s->ctl);
-    if (s->ctl_h) cudaFreeHost(s->ctl_h);
-    if (s->block_cfl) cudaFree(s->block_cfl);
-    if (s->block_sums) cudaFree(s->block_sums);
-    if (s->sum_part) cudaFree(s->sum_part);
-    if (s->flag) cudaFree(s->flag);
+    if (s->mem) cudaFreeAsync(s->mem, s->stream);
+    if (s->ctl_h) s->ctx->ctl_slab.release(s->ctl_h);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
     if (s->stream) cudaStreamDestroy(s->stream);
