@@ -100,6 +100,8 @@ _SIGNATURES = {
     "fv_batch_info": ([_P, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(_I), ctypes.POINTER(_I),
                        ctypes.POINTER(_D)], _I),
     "fv_batch_tile": ([_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)], _I),
+    "fv_sim_set_wait_limit": ([_P, _I], _I),
+    "fv_selftest_bounded_wait": ([_I, ctypes.POINTER(_I)], _I),
     "fv_host_alloc": ([ctypes.POINTER(_P), ctypes.c_size_t], _I),
     "fv_host_free": ([_P], _I),
 }

@@ -279,6 +279,22 @@ __global__ void cfl0_partial_kernel(const float* __restrict__ h, const float* __
 // estimate, dt = the estimate (a simulator before simulate(),
 // EE2D_KP07_dimsplit.py:107) or dt = estimate * factor * cfl_scale (a batch
 // instance, whose first step is simulate()'s step 0).
+// Self-test of the stage kernels' bounded wait: one warp waits on an mbarrier
+// whose expected transaction bytes no copy will ever deliver (no copy is
+// issued, so nothing lands in shared memory later); out[0] = 1 when the wait
+// ended by its poll limit, 0 if it completed.
+__global__ void selftest_wait_kernel(uint32_t polls, int* out) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        fv::mbar_init(&bar, 1);
+        fv::fence_barrier_init();
+        fv::mbar_arrive_expect_tx(&bar, 16);
+    }
+    __syncthreads();
+    const bool ok = fv::mbar_wait_bounded(&bar, 0, polls);
+    if (threadIdx.x == 0) out[0] = ok ? 0 : 1;
+}
+
 __global__ void cfl0_final_kernel(const float2* __restrict__ part, int n, SimCtl* ctl, int scaled) {
     float mx = INFINITY, my = INFINITY;
     bool nan_x = false, nan_y = false;
@@ -1003,6 +1019,30 @@ int fv_sim_set_boundary_conditions(fv_sim* s, int bc) {
     if (s->graph1) cudaGraphExecDestroy(s->graph1);
     if (s->graph16) cudaGraphExecDestroy(s->graph16);
     s->graph1 = s->graph16 = nullptr;
+    return FV_OK;
+}
+
+int fv_sim_set_wait_limit(fv_sim* s, int polls) {
+    FV_TRY(check_sim(s));
+    FV_CK(cudaStreamSynchronize(s->stream));
+    s->args.wait_limit = polls < 0 ? 0 : (polls == 0 ? -1 : polls);
+    if (s->graph1) cudaGraphExecDestroy(s->graph1);
+    if (s->graph16) cudaGraphExecDestroy(s->graph16);
+    s->graph1 = s->graph16 = nullptr;
+    return FV_OK;
+}
+
+int fv_selftest_bounded_wait(int polls, int* gave_up) {
+    if (!gave_up || polls < 0) return fail(FV_ERR_INVALID, "bad argument");
+    int* d = nullptr;
+    FV_CK(cudaMalloc(&d, sizeof(int)));
+    selftest_wait_kernel<<<1, 32>>>((uint32_t)polls, d);
+    int h = -1;
+    const cudaError_t e1 = cudaGetLastError();
+    const cudaError_t e2 = cudaMemcpy(&h, d, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e1 != cudaSuccess || e2 != cudaSuccess) return fail(FV_ERR_CUDA, "self-test kernel failed");
+    *gave_up = h;
     return FV_OK;
 }
 

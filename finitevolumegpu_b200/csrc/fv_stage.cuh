@@ -73,15 +73,22 @@ struct StageArgs {
     float dt_step;
     int want_sums;       // compute FP64 sums of the new state at the end of a step
     float variant_beta;  // parameter of the Osher and Sweby limiters (the variant itself is a kernel template)
+    int wait_limit;      // tile-load wait: 0 = kWaitPolls polls (the default, also for zero-filled
+                         // arguments), n > 0 = n polls, negative = give up at once (tests)
 };
+
+// Polls of a bounded mbarrier wait before it gives up (each poll may suspend
+// the thread for a short hardware-defined time; in all about a second).
+constexpr uint32_t kWaitPolls = 1u << 20;
+__host__ __device__ inline uint32_t wait_polls(int wait_limit) {
+    return wait_limit == 0 ? kWaitPolls : (wait_limit < 0 ? 0u : (uint32_t)wait_limit);
+}
 
 // Storage: per variable, rows y = -2 .. ny+1 and columns x = -4 .. pitch-5,
 // element (y, x) at [(y + 2) * pitch + (x + 4)].
 __host__ __device__ inline long long cell_index(int y, int x, int pitch) {
     return (long long)(y + 2) * pitch + (x + 4);
 }
-
-constexpr uint32_t kWaitPolls = 1u << 20;
 
 struct StepCtl {
     float dt;      // step dt (before dt_scale)
@@ -251,11 +258,12 @@ struct TileJob {
 };
 
 // Issues the TMA loads of the tile (thread 0) and waits for them with a bounded
-// wait on `phase` of the mbarrier (initialised here when `init`).  Returns false
-// (uniformly across the CTA) if the wait gave up; *err is then set.
+// wait of `polls` polls on `phase` of the mbarrier (initialised here when
+// `init`).  Returns false (uniformly across the CTA) if the wait gave up; *err
+// is then set, after a second bounded wait has let the copies in flight land.
 template <int NV, int SP, int TR, bool GLOBAL_TMAP = false>
 __device__ __forceinline__ bool load_tile(float* Qs, const CUtensorMap* tmap, int x0, int y0, uint64_t* bar,
-                                          uint32_t phase, bool init, int* err) {
+                                          uint32_t phase, bool init, int* err, uint32_t polls = kWaitPolls) {
     constexpr int PS = SP * TR;
     if (threadIdx.x == 0) {
         if (GLOBAL_TMAP) {
@@ -275,7 +283,7 @@ __device__ __forceinline__ bool load_tile(float* Qs, const CUtensorMap* tmap, in
         for (int v = 0; v < NV; ++v) tma_load_2d(Qs + v * PS, tmap + v, x0, y0, bar);
     }
     __syncthreads();
-    const bool ok = mbar_wait_bounded(bar, phase, kWaitPolls);
+    const bool ok = mbar_wait_bounded(bar, phase, polls);
     const int failed = __syncthreads_or(ok ? 0 : 1);
     if (failed) {
         if (threadIdx.x == 0) atomicExch(err, 1);
@@ -663,14 +671,14 @@ struct SplitPar {
 template <int SCHEME, int W, int H, int NT, bool GLOBAL_TMAP = false, int VAR = 0>
 __device__ bool process_tile_dimsplit(float* Qs, uint64_t* bar, uint32_t phase, bool init_bar, const TileJob& J,
                                       const SplitPar& P, bool do_cfl, bool sums, int* err, float& my_cfl,
-                                      double (&my_sums)[(SCHEME == EE2D) ? 4 : 3]) {
+                                      double (&my_sums)[(SCHEME == EE2D) ? 4 : 3], uint32_t polls = kWaitPolls) {
     constexpr int NV = (SCHEME == EE2D) ? 4 : 3;
     constexpr int G = (SCHEME == FORCE || SCHEME == HLL) ? 1 : 2;
     constexpr int SP = W + 8, TR = H + 4, PS = SP * TR;
     static_assert(W % 4 == 0 && (W / 4) % 2 == 1, "row segments must be odd for conflict-free x sweeps");
     static_assert(TR * 4 <= NT, "one x-sweep segment per thread");
     static_assert(NT % (W + 4) == 0 && H % (NT / (W + 4)) == 0, "y-sweep segments must tile the block");
-    if (!load_tile<NV, SP, TR, GLOBAL_TMAP>(Qs, J.tmap, J.x0, J.y0, bar, phase, init_bar, err)) return false;
+    if (!load_tile<NV, SP, TR, GLOBAL_TMAP>(Qs, J.tmap, J.x0, J.y0, bar, phase, init_bar, err, polls)) return false;
     const int x0 = J.x0, y0 = J.y0;
     if (x0 == 0 || x0 + W + 2 > J.nx || y0 == 0 || y0 + H + 2 > J.ny) apply_boundary<NV, W, H, NT>(Qs, J);
 
@@ -778,7 +786,8 @@ __global__ void __launch_bounds__(NT) dimsplit_stage_kernel(const __grid_constan
     J.x0 = blockIdx.x * W;
     J.y0 = blockIdx.y * H;
     SplitPar P{A.dx, A.dy, A.g, A.gamma, A.theta, sc.dt * A.dt_scale, A.substep, A.variant_beta};
-    process_tile_dimsplit<SCHEME, W, H, NT, false, VAR>(Qs, &bar, 0, true, J, P, sc.do_cfl, sums, &A.ctl->error, my_cfl, my_sums);
+    process_tile_dimsplit<SCHEME, W, H, NT, false, VAR>(Qs, &bar, 0, true, J, P, sc.do_cfl, sums, &A.ctl->error, my_cfl,
+                                                        my_sums, wait_polls(A.wait_limit));
     stage_epilogue<NT, NV>(A, sc, my_cfl, my_sums, sums);
 }
 
@@ -907,7 +916,7 @@ __global__ void __launch_bounds__(NT) unsplit_stage_kernel(const __grid_constant
     J.bc = A.bc;
     J.x0 = x0;
     J.y0 = y0;
-    if (load_tile<3, SP, TR>(Qs, J.tmap, x0, y0, &bar, 0, true, &A.ctl->error)) {
+    if (load_tile<3, SP, TR>(Qs, J.tmap, x0, y0, &bar, 0, true, &A.ctl->error, wait_polls(A.wait_limit))) {
         if (x0 == 0 || x0 + W + 2 > A.nx || y0 == 0 || y0 + H + 2 > A.ny) apply_boundary<3, W, H, NT>(Qs, J);
         const float kdt = sc.dt * A.dt_scale;
         const float g = A.g, half_g = 0.5f * g, theta2 = 2.0f * A.theta;

@@ -144,6 +144,17 @@ FV_API int fv_sim_synchronize(fv_sim* sim);
 /* setBoundaryConditions (Simulator.py:245-247). */
 FV_API int fv_sim_set_boundary_conditions(fv_sim* sim, int bc);
 
+/* Test hooks (no counterpart in the reference): the give-up path of the
+ * stage kernels' bounded waits, exercised without faulting or hanging a GPU.
+ * fv_sim_set_wait_limit sets how many times a stage kernel polls for its
+ * tile load before it gives up (negative: the default, about a second); 0
+ * gives up at once, after which the kernel still waits, boundedly, for its
+ * copies to land, writes nothing and the next synchronising call returns
+ * FV_ERR_DEVICE.  fv_selftest_bounded_wait runs one warp that waits `polls`
+ * times on a barrier that nothing completes; *gave_up = 1 when it gave up. */
+FV_API int fv_sim_set_wait_limit(fv_sim* sim, int polls);
+FV_API int fv_selftest_bounded_wait(int polls, int* gave_up);
+
 /* Time-stepping state of a simulation: simulated time t, steps nt, the
  * current time step dt and the last CFL minimum (from which simulate()
  * derives dt every 100 steps).  get/set let a caller checkpoint a simulation
