@@ -315,7 +315,7 @@ def run_batched(ctx, n_inst=512, seed=4, check=4):
     }
 
 
-def run_served(ctx, n_req=400, rates=(300.0, 3000.0), seed=5, plain_sample=60, warmup_req=16):
+def run_served(ctx, n_req=400, rates=(300.0, 3000.0), seed=5, plain_sample=60, warmup_req=64):
     """Config 5: scenario requests with Poisson arrivals, scheme uniform over {KP07_dimsplit, HLL, EE2D},
     sides log-uniform [128, 2048], t_end ~ U(1, 20), served with continuous batching under a 120 GB budget.
     The same scenarios are served at each arrival rate of the sweep (the last one saturates the server);
