@@ -581,6 +581,23 @@ int write_ctl(fv_sim* s) {
     return FV_OK;
 }
 
+// Stage kernels are launched with programmatic stream serialization: the next
+// substep's CTAs may launch while this one's last CTAs run, and wait in the
+// kernel (grid_dependency_wait) for its completion before reading anything.
+cudaError_t launch_dependent(const void* fn, dim3 grid, dim3 block, void** args, size_t smem, cudaStream_t stream) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
 int launch_stage(fv_sim* s, int substep, bool is_last, bool force_cfl, bool explicit_dt, float dt, bool sums) {
     alignas(64) StageArgs a = s->args;
     a.substep = substep;
@@ -590,7 +607,7 @@ int launch_stage(fv_sim* s, int substep, bool is_last, bool force_cfl, bool expl
     a.dt_step = dt;
     a.want_sums = sums ? 1 : 0;
     void* kargs[] = {&a};
-    FV_CK(cudaLaunchKernel(reinterpret_cast<const void*>(s->ke->fn), s->grid, dim3(s->ke->NT), kargs,
+    FV_CK(launch_dependent(reinterpret_cast<const void*>(s->ke->fn), s->grid, dim3(s->ke->NT), kargs,
                            entry_smem(*s->ke), s->stream));
     return FV_OK;
 }
@@ -1180,7 +1197,7 @@ int batch_launch_step(fv_batch* b) {
         a.want_sums = 0;
         a.err = b->d_err;
         void* kargs[] = {&a};
-        FV_CK(cudaLaunchKernel(reinterpret_cast<const void*>(b->be->fn), dim3(b->grid), dim3(b->be->NT), kargs,
+        FV_CK(launch_dependent(reinterpret_cast<const void*>(b->be->fn), dim3(b->grid), dim3(b->be->NT), kargs,
                                batch_smem(*b->be), b->stream));
     }
     return FV_OK;

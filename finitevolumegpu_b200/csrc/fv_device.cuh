@@ -55,6 +55,15 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
     return ok != 0;
 }
 
+// Programmatic dependent launch.  A stage kernel launched with programmatic
+// stream serialization may start while the previous kernel of its stream is
+// finishing: grid_launch_dependents lets the next kernel's CTAs launch into
+// SMs this grid frees once all of this grid's CTAs have started, and
+// grid_dependency_wait blocks until the previous kernel has completed and its
+// memory is visible (a no-op for a launch without the attribute).
+__device__ __forceinline__ void grid_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Bounded wait: gives up after `limit` polls (each poll may suspend the thread
 // for a short hardware-defined time) and returns false.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase, uint32_t limit) {

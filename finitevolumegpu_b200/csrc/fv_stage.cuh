@@ -242,6 +242,9 @@ __device__ void tile_epilogue(SimCtl* ctl, float* block_cfl, double* block_sums,
 template <int NT, int NV>
 __device__ __forceinline__ void stage_epilogue(const StageArgs& A, const StepCtl& s, float my_cfl,
                                                const double (&my_sums)[NV], bool sums) {
+    // The tile is written: the next substep's CTAs may launch once every CTA
+    // of this grid is here (they wait in grid_dependency_wait for its end).
+    grid_launch_dependents();
     tile_epilogue<NT, NV>(A.ctl, A.block_cfl, A.block_sums, blockIdx.y * gridDim.x + blockIdx.x,
                           gridDim.x * gridDim.y, A.is_last != 0, A.explicit_dt != 0, s, my_cfl, my_sums, sums);
 }
@@ -766,6 +769,7 @@ __global__ void __launch_bounds__(NT) dimsplit_stage_kernel(const __grid_constan
     float* Qs = reinterpret_cast<float*>(smem_raw);
     __shared__ __align__(8) uint64_t bar;
 
+    grid_dependency_wait();  // the previous substep's state and control block
     StepCtl sc = read_step(A);
     if (!sc.active) return;
     if (SCHEME == WAF) sc.do_cfl = false;  // WAFKernel has no CFL output (GPUSimulators/cuda/SWE2D_WAF.cu:103-119)
@@ -829,6 +833,7 @@ __global__ void __launch_bounds__(NT) batched_stage_kernel(const __grid_constant
     extern __shared__ __align__(128) unsigned char smem_raw[];
     float* Qs = reinterpret_cast<float*>(smem_raw);
     __shared__ __align__(8) uint64_t bar;
+    grid_dependency_wait();  // the previous substep's states and control blocks
     const int n = *B.nwork;
     uint32_t phase = 0;
     bool init = true;
@@ -899,6 +904,7 @@ __global__ void __launch_bounds__(NT) unsplit_stage_kernel(const __grid_constant
     float* Qs = reinterpret_cast<float*>(smem_raw);
     __shared__ __align__(8) uint64_t bar;
 
+    grid_dependency_wait();  // the previous stage's state and control block
     const StepCtl sc = read_step(A);
     if (!sc.active) return;
     const int x0 = blockIdx.x * W, y0 = blockIdx.y * H;
