@@ -25,23 +25,23 @@ import numpy as np
 
 # Number of tile configurations per scheme in libfvgpu's kernel table.
 TILE_CONFIGS = {
-    "KP07_dimsplit": 3,
-    "HLL2": 2,
-    "WAF": 2,
-    "FORCE": 2,
-    "HLL": 3,
-    "EE2D_KP07_dimsplit": 3,
-    "LxF": 3,
-    "KP07": 3,
+    "KP07_dimsplit": 4,
+    "HLL2": 3,
+    "WAF": 3,
+    "FORCE": 3,
+    "HLL": 4,
+    "EE2D_KP07_dimsplit": 4,
+    "LxF": 4,
+    "KP07": 4,
 }
 # Tile configurations of the batched (persistent) kernels per scheme.
 BATCH_TILE_CONFIGS = {
-    "KP07_dimsplit": 3,
-    "HLL": 3,
-    "EE2D_KP07_dimsplit": 2,
-    "HLL2": 2,
-    "WAF": 2,
-    "FORCE": 2,
+    "KP07_dimsplit": 4,
+    "HLL": 4,
+    "EE2D_KP07_dimsplit": 3,
+    "HLL2": 3,
+    "WAF": 3,
+    "FORCE": 3,
 }
 
 DEFAULT_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "autotuning_data.json")

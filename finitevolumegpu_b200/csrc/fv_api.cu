@@ -71,24 +71,32 @@ const KEntry kTable[] = {
     {FV_KP07_DIMSPLIT, 124, 60, 256, true, fv::dimsplit_stage_kernel<fv::KP07_DIMSPLIT, 124, 60, 256>},
     {FV_KP07_DIMSPLIT, 124, 28, 128, true, fv::dimsplit_stage_kernel<fv::KP07_DIMSPLIT, 124, 28, 128>},
     {FV_KP07_DIMSPLIT, 60, 28, 128, true, fv::dimsplit_stage_kernel<fv::KP07_DIMSPLIT, 60, 28, 128>},
+    {FV_KP07_DIMSPLIT, 28, 28, 128, true, fv::dimsplit_stage_kernel<fv::KP07_DIMSPLIT, 28, 28, 128>},
     {FV_HLL2, 124, 60, 256, true, fv::dimsplit_stage_kernel<fv::HLL2, 124, 60, 256>},
     {FV_HLL2, 124, 28, 128, true, fv::dimsplit_stage_kernel<fv::HLL2, 124, 28, 128>},
+    {FV_HLL2, 28, 28, 128, true, fv::dimsplit_stage_kernel<fv::HLL2, 28, 28, 128>},
     {FV_WAF, 124, 60, 256, true, fv::dimsplit_stage_kernel<fv::WAF, 124, 60, 256>},
     {FV_WAF, 124, 28, 128, true, fv::dimsplit_stage_kernel<fv::WAF, 124, 28, 128>},
+    {FV_WAF, 28, 28, 128, true, fv::dimsplit_stage_kernel<fv::WAF, 28, 28, 128>},
     {FV_FORCE, 124, 60, 256, true, fv::dimsplit_stage_kernel<fv::FORCE, 124, 60, 256>},
     {FV_FORCE, 124, 28, 128, true, fv::dimsplit_stage_kernel<fv::FORCE, 124, 28, 128>},
+    {FV_FORCE, 28, 28, 128, true, fv::dimsplit_stage_kernel<fv::FORCE, 28, 28, 128>},
     {FV_HLL, 124, 60, 256, true, fv::dimsplit_stage_kernel<fv::HLL, 124, 60, 256>},
     {FV_HLL, 124, 28, 128, true, fv::dimsplit_stage_kernel<fv::HLL, 124, 28, 128>},
     {FV_HLL, 60, 28, 128, true, fv::dimsplit_stage_kernel<fv::HLL, 60, 28, 128>},
+    {FV_HLL, 28, 28, 128, true, fv::dimsplit_stage_kernel<fv::HLL, 28, 28, 128>},
     {FV_EE2D_KP07_DIMSPLIT, 124, 28, 128, true, fv::dimsplit_stage_kernel<fv::EE2D, 124, 28, 128>},
     {FV_EE2D_KP07_DIMSPLIT, 124, 60, 256, true, fv::dimsplit_stage_kernel<fv::EE2D, 124, 60, 256>},
     {FV_EE2D_KP07_DIMSPLIT, 60, 28, 128, true, fv::dimsplit_stage_kernel<fv::EE2D, 60, 28, 128>},
+    {FV_EE2D_KP07_DIMSPLIT, 28, 28, 128, true, fv::dimsplit_stage_kernel<fv::EE2D, 28, 28, 128>},
     {FV_LXF, 120, 60, 256, false, fv::unsplit_stage_kernel<fv::LXF, 120, 60, 256>},
     {FV_LXF, 120, 28, 128, false, fv::unsplit_stage_kernel<fv::LXF, 120, 28, 128>},
     {FV_LXF, 120, 60, 128, false, fv::unsplit_stage_kernel<fv::LXF, 120, 60, 128>},
+    {FV_LXF, 60, 28, 128, false, fv::unsplit_stage_kernel<fv::LXF, 60, 28, 128>},
     {FV_KP07, 120, 28, 128, false, fv::unsplit_stage_kernel<fv::KP07, 120, 28, 128>},
     {FV_KP07, 120, 60, 128, false, fv::unsplit_stage_kernel<fv::KP07, 120, 60, 128>},
     {FV_KP07, 120, 60, 256, false, fv::unsplit_stage_kernel<fv::KP07, 120, 60, 256>},
+    {FV_KP07, 60, 28, 128, false, fv::unsplit_stage_kernel<fv::KP07, 60, 28, 128>},
 };
 constexpr int kNumEntries = sizeof(kTable) / sizeof(kTable[0]);
 
@@ -120,17 +128,23 @@ const BEntry kBatchTable[] = {
     {FV_KP07_DIMSPLIT, 60, 28, 128, fv::batched_stage_kernel<fv::KP07_DIMSPLIT, 60, 28, 128>},
     {FV_KP07_DIMSPLIT, 124, 28, 128, fv::batched_stage_kernel<fv::KP07_DIMSPLIT, 124, 28, 128>},
     {FV_KP07_DIMSPLIT, 124, 60, 256, fv::batched_stage_kernel<fv::KP07_DIMSPLIT, 124, 60, 256>},
+    {FV_KP07_DIMSPLIT, 28, 28, 128, fv::batched_stage_kernel<fv::KP07_DIMSPLIT, 28, 28, 128>},
     {FV_HLL, 60, 28, 128, fv::batched_stage_kernel<fv::HLL, 60, 28, 128>},
     {FV_HLL, 124, 28, 128, fv::batched_stage_kernel<fv::HLL, 124, 28, 128>},
     {FV_HLL, 124, 60, 256, fv::batched_stage_kernel<fv::HLL, 124, 60, 256>},
+    {FV_HLL, 28, 28, 128, fv::batched_stage_kernel<fv::HLL, 28, 28, 128>},
     {FV_EE2D_KP07_DIMSPLIT, 60, 28, 128, fv::batched_stage_kernel<fv::EE2D, 60, 28, 128>},
     {FV_EE2D_KP07_DIMSPLIT, 124, 28, 128, fv::batched_stage_kernel<fv::EE2D, 124, 28, 128>},
+    {FV_EE2D_KP07_DIMSPLIT, 28, 28, 128, fv::batched_stage_kernel<fv::EE2D, 28, 28, 128>},
     {FV_HLL2, 60, 28, 128, fv::batched_stage_kernel<fv::HLL2, 60, 28, 128>},
     {FV_HLL2, 124, 28, 128, fv::batched_stage_kernel<fv::HLL2, 124, 28, 128>},
+    {FV_HLL2, 28, 28, 128, fv::batched_stage_kernel<fv::HLL2, 28, 28, 128>},
     {FV_WAF, 60, 28, 128, fv::batched_stage_kernel<fv::WAF, 60, 28, 128>},
     {FV_WAF, 124, 28, 128, fv::batched_stage_kernel<fv::WAF, 124, 28, 128>},
+    {FV_WAF, 28, 28, 128, fv::batched_stage_kernel<fv::WAF, 28, 28, 128>},
     {FV_FORCE, 60, 28, 128, fv::batched_stage_kernel<fv::FORCE, 60, 28, 128>},
     {FV_FORCE, 124, 28, 128, fv::batched_stage_kernel<fv::FORCE, 124, 28, 128>},
+    {FV_FORCE, 28, 28, 128, fv::batched_stage_kernel<fv::FORCE, 28, 28, 128>},
 };
 constexpr int kNumBatchEntries = sizeof(kBatchTable) / sizeof(kBatchTable[0]);
 
