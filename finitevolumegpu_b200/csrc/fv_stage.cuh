@@ -268,6 +268,10 @@ template <int NV, int SP, int TR, bool GLOBAL_TMAP = false>
 __device__ __forceinline__ bool load_tile(float* Qs, const CUtensorMap* tmap, int x0, int y0, uint64_t* bar,
                                           uint32_t phase, bool init, int* err, uint32_t polls = kWaitPolls) {
     constexpr int PS = SP * TR;
+    // Each variable's plane is the destination of a tensor copy, which must
+    // start on a 128-byte boundary: tiles whose (W+8) x (H+4) plane is not a
+    // multiple of 32 floats would misalign every plane after the first.
+    static_assert((PS * sizeof(float)) % 128 == 0, "variable planes in shared memory must be 128-byte aligned");
     if (threadIdx.x == 0) {
         if (GLOBAL_TMAP) {
 #pragma unroll
