@@ -1163,7 +1163,8 @@ struct fv_batch {
     fv::BatchInstance* d_inst = nullptr;  // device, max_inst entries
     fv::BatchInstance* h_inst = nullptr;  // pinned staging
     SimCtl* d_ctl = nullptr;              // device, one control block per slot
-    SimCtl* h_ctl = nullptr;              // pinned host view
+    SimCtl* h_ctl = nullptr;              // pinned host view, refreshed by fv_batch_sync
+    SimCtl* h_ctl_up = nullptr;           // pinned source of an admitted slot's first control block
     int2* d_work = nullptr;
     int2* h_work[2] = {nullptr, nullptr};  // pinned staging, alternated between publishes
     int* h_nwork[2] = {nullptr, nullptr};
@@ -1176,6 +1177,7 @@ struct fv_batch {
     cudaStream_t copy_stream = nullptr;  // uploads/downloads, concurrent with the kernels
     cudaEvent_t ev_up = nullptr, ev_compute = nullptr;
     std::vector<int> done_at_sync;        // slot finished as of the last fv_batch_sync
+    std::vector<int> registered;          // slot fully admitted (its instance and control block are queued)
     bool dirty = false;                   // work list changed since the last publish
     std::vector<int> used;               // slot in use
     std::vector<void*> slot_mem;          // per-slot device allocation (planes + tile scratch)
@@ -1239,9 +1241,11 @@ int batch_build_graph(fv_batch* b, int nsteps, cudaGraphExec_t* out) {
 // the ones after it the new one.  The two pinned staging buffers alternate;
 // a buffer is rewritten only after its previous copy has completed.
 int batch_publish(fv_batch* b) {
+    // Slots reserved by an fv_batch_add still in progress (on another host
+    // thread) are not registered yet and stay out of the list.
     int n = 0;
     for (int s = 0; s < b->max_inst; ++s)
-        if (b->used[s]) n += b->h_inst[s].ntiles;
+        if (b->used[s] && b->registered[s]) n += b->h_inst[s].ntiles;
     if (n > b->work_cap) {
         int cap = b->work_cap;
         while (cap < n) cap *= 2;
@@ -1261,7 +1265,7 @@ int batch_publish(fv_batch* b) {
     FV_CK(cudaEventSynchronize(b->ev_work[k]));
     int i = 0;
     for (int s = 0; s < b->max_inst; ++s) {
-        if (!b->used[s]) continue;
+        if (!b->used[s] || !b->registered[s]) continue;
         for (int t = 0; t < b->h_inst[s].ntiles; ++t) b->h_work[k][i++] = make_int2(s, t);
     }
     *b->h_nwork[k] = n;
@@ -1326,11 +1330,13 @@ int fv_batch_create(fv_context* ctx, int scheme, const fv_params* params, int ma
         cudaEventCreateWithFlags(&b->ev_work[1], cudaEventDisableTiming) != cudaSuccess)
         return bail(fail(FV_ERR_CUDA, "stream/event creation failed"));
     b->done_at_sync.assign(max_instances, 0);
+    b->registered.assign(max_instances, 0);
     b->work_cap = 4096;
     if (cudaMalloc(&b->d_inst, (size_t)max_instances * sizeof(fv::BatchInstance)) != cudaSuccess ||
         cudaMallocHost(&b->h_inst, (size_t)max_instances * sizeof(fv::BatchInstance)) != cudaSuccess ||
         cudaMalloc(&b->d_ctl, (size_t)max_instances * sizeof(SimCtl)) != cudaSuccess ||
         cudaMallocHost(&b->h_ctl, (size_t)max_instances * sizeof(SimCtl)) != cudaSuccess ||
+        cudaMallocHost(&b->h_ctl_up, (size_t)max_instances * sizeof(SimCtl)) != cudaSuccess ||
         cudaMalloc(&b->d_work, (size_t)b->work_cap * sizeof(int2)) != cudaSuccess ||
         cudaMallocHost(&b->h_work[0], (size_t)b->work_cap * sizeof(int2)) != cudaSuccess ||
         cudaMallocHost(&b->h_work[1], (size_t)b->work_cap * sizeof(int2)) != cudaSuccess ||
@@ -1340,6 +1346,7 @@ int fv_batch_create(fv_context* ctx, int scheme, const fv_params* params, int ma
         return bail(fail(FV_ERR_NOMEM, "out of memory creating the batch"));
     memset(b->h_inst, 0, (size_t)max_instances * sizeof(fv::BatchInstance));
     memset(b->h_ctl, 0, (size_t)max_instances * sizeof(SimCtl));
+    memset(b->h_ctl_up, 0, (size_t)max_instances * sizeof(SimCtl));
     *b->h_nwork[0] = *b->h_nwork[1] = 0;
     if (cudaMemsetAsync(b->d_ctl, 0, (size_t)max_instances * sizeof(SimCtl), b->stream) != cudaSuccess ||
         cudaMemsetAsync(b->d_err, 0, sizeof(int), b->stream) != cudaSuccess ||
@@ -1363,6 +1370,7 @@ int fv_batch_destroy(fv_batch* b) {
     if (b->h_inst) cudaFreeHost(b->h_inst);
     if (b->d_ctl) cudaFree(b->d_ctl);
     if (b->h_ctl) cudaFreeHost(b->h_ctl);
+    if (b->h_ctl_up) cudaFreeHost(b->h_ctl_up);
     if (b->d_work) cudaFree(b->d_work);
     if (b->d_nwork) cudaFree(b->d_nwork);
     for (int k = 0; k < 2; ++k) {
@@ -1478,14 +1486,17 @@ int fv_batch_add(fv_batch* b, int nx, int ny, float dx, float dy, int bc, const 
     std::lock_guard<std::mutex> lock(b->mu);
     FV_CK(cudaEventRecord(b->ev_up, b->copy_stream));
     FV_CK(cudaStreamWaitEvent(b->stream, b->ev_up, 0));  // later kernels see the uploaded state
-    SimCtl& c = b->h_ctl[s];
+    // The upload's source is h_ctl_up, not h_ctl: an fv_batch_sync on another
+    // thread may have queued a copy of every control block into h_ctl ahead of
+    // this upload, which would overwrite the new values before they are read.
+    SimCtl& c = b->h_ctl_up[s];
     memset(&c, 0, sizeof(c));
     const float c2 = (b->scheme == FV_EE2D_KP07_DIMSPLIT) ? b->p.gamma : b->p.g;
     c.t_end = t_end;
     c.factor = b->factor;
     c.cfl_scale = b->p.cfl_scale;
     c.update_dt = 1;
-    // From pinned staging (h_ctl, h_inst): asynchronous, ordered before the next kernels.
+    // From pinned staging (h_ctl_up, h_inst): asynchronous, ordered before the next kernels.
     FV_CK(cudaMemcpyAsync(b->d_ctl + s, &c, sizeof(SimCtl), cudaMemcpyHostToDevice, b->stream));
     FV_CK(cudaMemcpyAsync(b->d_inst + s, &I, sizeof(fv::BatchInstance), cudaMemcpyHostToDevice, b->stream));
     // cfl_min = the initial CFL estimate, dt = estimate * factor * cfl_scale
@@ -1497,6 +1508,7 @@ int fv_batch_add(fv_batch* b, int nx, int ny, float dx, float dy, int bc, const 
     b->slot_mem[s] = mem;
     b->slot_bytes[s] = total;
     b->bytes += total;
+    b->registered[s] = 1;
     b->dirty = true;  // joins the work list at the next fv_batch_run
     *slot = s;
     return FV_OK;
@@ -1507,6 +1519,7 @@ int fv_batch_remove(fv_batch* b, int slot) {
     std::lock_guard<std::mutex> lock(b->mu);
     if (slot < 0 || slot >= b->max_inst || !b->used[slot]) return fail(FV_ERR_INVALID, "slot %d is not in use", slot);
     b->used[slot] = 0;
+    b->registered[slot] = 0;
     b->dirty = true;  // leaves the work list at the next fv_batch_run
     // Freed in stream order, after every kernel already queued that may read it.
     FV_CK(cudaFreeAsync(b->slot_mem[slot], b->stream));
@@ -1552,7 +1565,7 @@ int fv_batch_sync(fv_batch* b) {
     FV_CK(cudaMemcpy(&err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost));
     std::lock_guard<std::mutex> lock(b->mu);
     for (int s = 0; s < b->max_inst; ++s) {
-        if (!b->used[s]) continue;
+        if (!b->used[s] || !b->registered[s]) continue;
         const SimCtl& c = b->h_ctl[s];
         const double rem = c.t_end - c.t;
         const float cur = (float)((rem < (double)c.dt) ? rem : (double)c.dt);

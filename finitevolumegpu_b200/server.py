@@ -10,14 +10,16 @@ while others run join the running batches at the next chunk boundary.
 
 Each scenario follows the reference's simulate(t_end) semantics on its own
 (see batch.py), so its result does not depend on what else is in the batch.
-Finished scenarios are downloaded and released by return threads, so
-host-to-device uploads of new requests and device-to-host reads of results
-overlap.
+Arrived requests are uploaded by admission threads and finished scenarios
+are downloaded and released by return threads, so host-to-device uploads of
+new requests, device-to-host reads of results and the queuing of the next
+chunk overlap.
 """
 
 from __future__ import annotations
 
 import collections
+import concurrent.futures
 import dataclasses
 import queue
 import threading
@@ -87,9 +89,10 @@ def state_bytes(scheme, nx, ny, tile_w=60, tile_h=28):
 
 class Server(object):
     def __init__(self, context, budget_bytes=120e9, chunk_steps=8, max_instances=4096, schemes=None,
-                 cfl_scale=0.9, return_threads=3):
+                 cfl_scale=0.9, return_threads=3, admit_threads=3):
         self.context = context
         self.return_threads = max(1, int(return_threads))
+        self.admit_threads = max(1, int(admit_threads))
         self.budget = float(budget_bytes)
         self.chunk = int(chunk_steps)
         self.cfl_scale = cfl_scale
@@ -112,10 +115,11 @@ class Server(object):
         """Serve `requests` (arrival times relative to the call) until all are done.
 
         The calling thread queues the next chunk of steps for every batch with
-        running scenarios, admits arrived requests while the budget allows
-        (their uploads run on each batch's copy stream and they join the chunk
-        after), then waits for the chunk and hands the scenarios that reached
-        t_end to the return threads.  These download and release them while the
+        running scenarios, hands arrived requests to the admission threads
+        while the budget allows (their uploads run on each batch's copy stream
+        and they join the first chunk queued after their upload was issued),
+        then waits for the chunk and hands the scenarios that reached t_end to
+        the return threads.  These download and release them while the
         calling thread queues and admits the next chunk: their state is final
         (later chunks skip them), and their memory returns to the budget once
         released.  Several return threads copy results out in parallel.
@@ -155,18 +159,45 @@ class Server(object):
                     shared["outstanding"] -= 1
                     timers["return"] += clock() - ta
 
+        def admit(b, r):
+            ta = clock()
+            slot = b.add(r.variables, r.nx, r.ny, r.dx, r.dy, r.t_end, r.boundary_conditions)
+            with lock:
+                timers["admit_upload"] += clock() - ta
+            return slot
+
         workers = [threading.Thread(target=return_finished, name="fvgpu-return-%d" % k, daemon=True)
                    for k in range(self.return_threads)]
         for w in workers:
             w.start()
+        admitting = []  # (future, request, batch key, bytes) of uploads in flight
         busy_since = None
+        pool = concurrent.futures.ThreadPoolExecutor(self.admit_threads, thread_name_prefix="fvgpu-admit")
         try:
             while True:
                 with lock:
                     outstanding = shared["outstanding"]
                     if shared["error"] is not None:
                         raise shared["error"]
-                if not (pending or running or outstanding):
+                # 0. admissions whose upload has been issued join the running set
+                still = []
+                requeue = []
+                for fut, r, bk, need in admitting:
+                    if not fut.done():
+                        still.append((fut, r, bk, need))
+                        continue
+                    try:
+                        slot = fut.result()
+                    except MemoryError:  # the GPU is full after all: retry once others have left
+                        with lock:
+                            self.used -= need
+                        requeue.append(r)
+                        continue
+                    running[(bk, slot)] = (r, clock() - t0, need)
+                admitting = still
+                if requeue:
+                    pending.extendleft(sorted(requeue, key=lambda r: r.arrival, reverse=True))
+                if not (pending or running or outstanding or admitting):
                     break
                 # 1. queue the next chunk
                 active = {key[0] for key in running}
@@ -176,24 +207,38 @@ class Server(object):
                 timers["queue"] += clock() - ta
                 if active and busy_since is None:
                     busy_since = ta - t0
-                # 2. admit arrived requests while the budget allows
+                # 2. admit arrived requests while the budget allows: a burst of
+                #    them goes to the admission threads, whose uploads proceed in
+                #    parallel; one or two are admitted here, which keeps them in
+                #    the very next chunk
                 ta = clock()
                 now = ta - t0
+                ready = 0
+                for r in pending:
+                    if r.arrival > now:
+                        break
+                    ready += 1
+                burst = ready > self.admit_threads
                 while pending and pending[0].arrival <= now:
                     r = pending[0]
                     need = state_bytes(r.scheme, r.nx, r.ny)
                     with lock:
                         if self.used + need > self.budget:
                             break
+                        self.used += need
                     bk = r.batch_key()
+                    if burst:
+                        pending.popleft()
+                        admitting.append((pool.submit(admit, self._batch(bk), r), r, bk, need))
+                        continue
                     try:
                         slot = self._batch(bk).add(r.variables, r.nx, r.ny, r.dx, r.dy, r.t_end,
                                                    r.boundary_conditions)
                     except MemoryError:
+                        with lock:
+                            self.used -= need
                         break
                     pending.popleft()
-                    with lock:
-                        self.used += need
                     running[(bk, slot)] = (r, clock() - t0, need)
                 timers["admit"] += clock() - ta
                 # 3. wait for the chunk; hand the scenarios at t_end to the return thread
@@ -208,10 +253,11 @@ class Server(object):
                         returns.put((key, r, admitted, need))
                 timers["wait"] += clock() - ta
                 if not active:
-                    # nothing on the GPU: wait for the next arrival or for returns to free memory
+                    # nothing on the GPU: wait for the next arrival, an upload or returns to free memory
                     wait = (pending[0].arrival - (clock() - t0)) if pending else 0.001
                     time.sleep(min(max(wait, 0.0005), 0.005))
         finally:
+            pool.shutdown(wait=True)
             for _ in workers:
                 returns.put(None)
             for w in workers:
