@@ -266,7 +266,7 @@ def run_batched(ctx, n_inst=512, seed=4, check=4):
         b.run(16)
         steps += 16
     t_run = time.perf_counter()
-    batched_out = [b.download(s) for s in slots]
+    batched_out = b.download_many(slots)
     nts = [b.status(s)["nt"] for s in slots]
     t1 = time.perf_counter()
     info = b.info()

@@ -103,6 +103,18 @@ class Batch(object):
             out.append(a)
         return out
 
+    def download_many(self, slots, threads=4):
+        """download() of several simulations, copied out on `threads` host
+        threads at once (their device-to-host copies and the host copies out of
+        pinned staging overlap).  Returns the states in the order of `slots`."""
+        slots = list(slots)
+        if threads <= 1 or len(slots) < 2:
+            return [self.download(s) for s in slots]
+        import concurrent.futures
+
+        with concurrent.futures.ThreadPoolExecutor(int(threads), thread_name_prefix="fvgpu-download") as pool:
+            return list(pool.map(self.download, slots))
+
     def info(self):
         b, a, w, ms = ctypes.c_size_t(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
         _lib.check(_L().fv_batch_info(self._h, ctypes.byref(b), ctypes.byref(a), ctypes.byref(w), ctypes.byref(ms)))

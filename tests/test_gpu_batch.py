@@ -58,9 +58,12 @@ def test_batch_equals_plain(ctx, scheme):
         slot = b.add(q, nx, ny, dx, dy, t_end, bc)
         cases[slot] = (q, nx, ny, dx, dy, t_end)
     b.run_to_completion()
+    many = dict(zip(cases, b.download_many(list(cases), threads=4)))
     for slot, (q, nx, ny, dx, dy, t_end) in cases.items():
         st = b.status(slot)
         got = b.download(slot)
+        for a, m in zip(got, many[slot]):
+            assert np.array_equal(a, m)  # the threaded download returns the same arrays
         want, nt, t = plain(ctx, scheme, q, nx, ny, dx, dy, t_end, bc)
         assert st["nt"] == nt and st["t"] == t, (slot, st, nt, t)
         for a, w in zip(got, want):
