@@ -18,9 +18,16 @@ from oracle import ref_kernels
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(scope="module")
+def tuned_ctx():
+    """A context with the autotuner on, as CudaContext() gives users by default."""
+    return fv.CudaContext.CudaContext(device=0, autotuning=True)
+
+
 @pytest.mark.parametrize("scheme", ["KP07_dimsplit", "HLL2", "WAF", "FORCE", "HLL", "LxF", "KP07",
                                     "EE2D_KP07_dimsplit"])
-def test_faster_than_reference_kernels(ctx, scheme):
+def test_faster_than_reference_kernels(tuned_ctx, scheme):
+    ctx = tuned_ctx
     if scheme == "EE2D_KP07_dimsplit":
         nx, ny = 4096, 2048
         from conftest import kelvin_helmholtz as kh
