@@ -86,10 +86,29 @@ class _VariableView(object):
         self.x_halo = self.y_halo = sim._gc
 
     def download(self, stream=None, cpu_data=None, asynch=False, extent=None):
-        if extent is not None:
-            raise NotImplementedError("extent downloads are not supported")
-        out = self._sim._download_var(self._var, cpu_data)
-        return out
+        """The interior, or with extent = [x, y, nx, ny] that region of the array
+        including its ghost cells (GPUSimulators/Common.py:543-584)."""
+        if extent is None:
+            return self._sim._download_var(self._var, cpu_data)
+        x, y, nx, ny = (int(v) for v in extent)
+        if cpu_data is None:
+            cpu_data = np.empty((ny, nx), dtype=np.float32)
+        assert cpu_data.shape == (ny, nx), "cpu_data shape does not match the extent"
+        assert cpu_data.dtype == np.float32 and cpu_data.flags.c_contiguous
+        _lib.check(_lib.lib().fv_sim_download_region(self._sim._handle, self._var, x, y, nx, ny,
+                                                     cpu_data.ctypes.data_as(_lib._FP), nx))
+        return cpu_data
+
+    def upload(self, stream, cpu_data, extent=None):
+        """The interior (cpu_data of shape (ny, nx)), or with extent = [x, y, nx, ny]
+        that region of the array including its ghost cells (Common.py:587-616)."""
+        if extent is None:
+            return self._sim.upload(self._var, cpu_data)
+        x, y, nx, ny = (int(v) for v in extent)
+        data = np.ascontiguousarray(cpu_data, dtype=np.float32)
+        assert data.shape == (ny, nx), "cpu_data shape does not match the extent"
+        _lib.check(_lib.lib().fv_sim_upload_region(self._sim._handle, self._var, x, y, nx, ny,
+                                                   data.ctypes.data_as(_lib._FP), nx))
 
 
 class _StateView(object):

@@ -74,6 +74,8 @@ _SIGNATURES = {
     "fv_sim_compute_dt": ([_P, ctypes.POINTER(_F)], _I),
     "fv_sim_download": ([_P, _I, _FP, _I], _I),
     "fv_sim_upload": ([_P, _I, _FP, _I], _I),
+    "fv_sim_download_region": ([_P, _I, _I, _I, _I, _I, _FP, _I], _I),
+    "fv_sim_upload_region": ([_P, _I, _I, _I, _I, _I, _FP, _I], _I),
     "fv_sim_time": ([_P, ctypes.POINTER(_D), ctypes.POINTER(_LL), ctypes.POINTER(_F)], _I),
     "fv_sim_conservation": ([_P, ctypes.POINTER(_D)], _I),
     "fv_sim_check": ([_P, ctypes.POINTER(_I)], _I),

@@ -994,6 +994,37 @@ int fv_sim_upload(fv_sim* s, int var, const float* host, int host_pitch) {
     return FV_OK;
 }
 
+// The region's first cell in storage coordinates, after checking that the
+// region lies inside the reference's halo-inclusive array (Common.py:564-565).
+int region_check(fv_sim* s, int var, int x, int y, int w, int h, const void* host, int host_pitch) {
+    const int gc = s->gc;
+    if (var < 0 || var >= s->nv || !host || w < 1 || h < 1 || host_pitch < w || x < 0 || y < 0 ||
+        x + w > s->nx + 2 * gc || y + h > s->ny + 2 * gc)
+        return fail(FV_ERR_INVALID, "region (%d, %d, %d, %d) outside the %d x %d array with ghost cells", x, y, w, h,
+                    s->nx + 2 * gc, s->ny + 2 * gc);
+    return FV_OK;
+}
+
+int fv_sim_download_region(fv_sim* s, int var, int x, int y, int w, int h, float* host, int host_pitch) {
+    FV_TRY(check_sim(s));
+    FV_TRY(region_check(s, var, x, y, w, h, host, host_pitch));
+    FV_TRY(read_ctl(s));
+    const float* src = s->buf[s->ctl_h->cur][var] + fv::cell_index(y - s->gc, x - s->gc, s->pitch);
+    return copy_d2h(s->ctx, s->stream, host, (size_t)host_pitch * sizeof(float), src, (size_t)s->pitch * sizeof(float),
+                    (size_t)w * sizeof(float), h);
+}
+
+int fv_sim_upload_region(fv_sim* s, int var, int x, int y, int w, int h, const float* host, int host_pitch) {
+    FV_TRY(check_sim(s));
+    FV_TRY(region_check(s, var, x, y, w, h, host, host_pitch));
+    FV_TRY(read_ctl(s));
+    float* dst = s->buf[s->ctl_h->cur][var] + fv::cell_index(y - s->gc, x - s->gc, s->pitch);
+    FV_TRY(copy_h2d(s->ctx, s->stream, dst, (size_t)s->pitch * sizeof(float), host, (size_t)host_pitch * sizeof(float),
+                    (size_t)w * sizeof(float), h));
+    FV_CK(cudaStreamSynchronize(s->stream));
+    return FV_OK;
+}
+
 int fv_sim_time(fv_sim* s, double* t, long long* nt, float* dt) {
     FV_TRY(check_sim(s));
     FV_TRY(read_ctl(s));

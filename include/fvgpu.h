@@ -127,6 +127,14 @@ FV_API int fv_sim_download(fv_sim* sim, int var, float* host, int host_pitch);
  * GPUSimulators/Common.py:587-616). */
 FV_API int fv_sim_upload(fv_sim* sim, int var, const float* host, int host_pitch);
 
+/* CudaArray2D.download/upload with an extent (GPUSimulators/Common.py:543-616):
+ * the w x h region whose first cell is (x, y) in the reference's coordinates,
+ * which count the ghost cells (x in [0, nx + 2g), y in [0, ny + 2g), g = 1 for
+ * LxF, FORCE and HLL, 2 otherwise), of variable `var` of u0.  The download
+ * waits for its copy; regions outside [0, nx + 2g) x [0, ny + 2g) are rejected. */
+FV_API int fv_sim_download_region(fv_sim* sim, int var, int x, int y, int w, int h, float* host, int host_pitch);
+FV_API int fv_sim_upload_region(fv_sim* sim, int var, int x, int y, int w, int h, const float* host, int host_pitch);
+
 /* simTime(), simSteps() and the current dt (Simulator.py:236-240). */
 FV_API int fv_sim_time(fv_sim* sim, double* t, long long* nt, float* dt);
 
