@@ -44,6 +44,16 @@ class CudaContext(object):
         # Every simulator synchronises its own stream; nothing is pending here.
         pass
 
+    def get_module(self, kernel_filename, include_dirs=(), defines=None, compile_args=None, jit_compile_args=None):
+        """The reference compiles one PyCUDA module per kernel file at run time
+        (GPUSimulators/CudaContext.py:178-260).  libfvgpu's kernels are compiled
+        ahead of time into one library, so there is no module to return."""
+        raise NotImplementedError("kernels are built into libfvgpu.so; %s has no run-time module" % kernel_filename)
+
+    def clear_kernel_cache(self):
+        """No run-time kernel cache exists (GPUSimulators/CudaContext.py:263-268)."""
+        pass
+
     def __del__(self):
         h = getattr(self, "_handle", None)
         if h is not None and _lib._lib is not None:
