@@ -33,9 +33,9 @@ import numpy as np
 # Number of tile configurations per scheme in libfvgpu's kernel table.
 TILE_CONFIGS = {
     "KP07_dimsplit": 4,
-    "HLL2": 3,
-    "WAF": 3,
-    "FORCE": 3,
+    "HLL2": 4,
+    "WAF": 4,
+    "FORCE": 4,
     "HLL": 4,
     "EE2D_KP07_dimsplit": 4,
     "LxF": 4,

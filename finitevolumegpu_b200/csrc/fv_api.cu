@@ -75,12 +75,15 @@ const KEntry kTable[] = {
     {FV_HLL2, 124, 60, 256, true, fv::dimsplit_stage_kernel<fv::HLL2, 124, 60, 256>},
     {FV_HLL2, 124, 28, 128, true, fv::dimsplit_stage_kernel<fv::HLL2, 124, 28, 128>},
     {FV_HLL2, 28, 28, 128, true, fv::dimsplit_stage_kernel<fv::HLL2, 28, 28, 128>},
+    {FV_HLL2, 60, 28, 128, true, fv::dimsplit_stage_kernel<fv::HLL2, 60, 28, 128>},
     {FV_WAF, 124, 60, 256, true, fv::dimsplit_stage_kernel<fv::WAF, 124, 60, 256>},
     {FV_WAF, 124, 28, 128, true, fv::dimsplit_stage_kernel<fv::WAF, 124, 28, 128>},
     {FV_WAF, 28, 28, 128, true, fv::dimsplit_stage_kernel<fv::WAF, 28, 28, 128>},
+    {FV_WAF, 60, 28, 128, true, fv::dimsplit_stage_kernel<fv::WAF, 60, 28, 128>},
     {FV_FORCE, 124, 60, 256, true, fv::dimsplit_stage_kernel<fv::FORCE, 124, 60, 256>},
     {FV_FORCE, 124, 28, 128, true, fv::dimsplit_stage_kernel<fv::FORCE, 124, 28, 128>},
     {FV_FORCE, 28, 28, 128, true, fv::dimsplit_stage_kernel<fv::FORCE, 28, 28, 128>},
+    {FV_FORCE, 60, 28, 128, true, fv::dimsplit_stage_kernel<fv::FORCE, 60, 28, 128>},
     {FV_HLL, 124, 60, 256, true, fv::dimsplit_stage_kernel<fv::HLL, 124, 60, 256>},
     {FV_HLL, 124, 28, 128, true, fv::dimsplit_stage_kernel<fv::HLL, 124, 28, 128>},
     {FV_HLL, 60, 28, 128, true, fv::dimsplit_stage_kernel<fv::HLL, 60, 28, 128>},
