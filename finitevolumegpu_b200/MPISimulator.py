@@ -183,10 +183,14 @@ class MPISimulator(object):
     BaseSimulator.simulate/step (GPUSimulators/Simulator.py:176-228), with the
     time step reduced over all ranks."""
 
-    def __init__(self, sim, grid):
+    def __init__(self, sim, grid, overlap=True):
         self.logger = logging.getLogger(__name__)
         self.sim = sim
         self.grid = grid
+        # exchange the edge rows while the interior of the stripe is computed
+        # (MPISimulator.py:318-331); needs at least three tile rows
+        self.overlap = bool(overlap) and hasattr(sim, "substep_rows") and sim.tile_rows() >= 3
+        self._xstream = None
         self.context = getattr(sim, "context", None)
         self.nx, self.ny, self.dx, self.dy = sim.nx, sim.ny, sim.dx, sim.dy
         self.cfl_scale = sim.cfl_scale
@@ -227,17 +231,39 @@ class MPISimulator(object):
         self.nt += 1
 
     def substep(self, dt, step_number):
-        self.sim.substep(dt, step_number)
-        self.full_exchange()
+        if not self.overlap:
+            self.sim.substep(dt, step_number)
+            self.full_exchange()
+            return
+        # The tile rows at the stripe's edges first; their rows go to the
+        # neighbours on a second stream while the interior rows are computed,
+        # and the next substep waits for both.
+        import torch
+
+        sim = self.sim
+        rows = sim.tile_rows()
+        stream = sim.comm_stream()
+        if self._xstream is None:
+            self._xstream = torch.cuda.Stream(device=stream.device)
+        sim.substep_rows(dt, step_number, 0, 1)
+        sim.substep_rows(dt, step_number, rows - 1, 1)
+        edges_done = torch.cuda.Event()
+        edges_done.record(stream)
+        self._xstream.wait_event(edges_done)
+        self.full_exchange(views=sim.halo_views(pending=True), stream=self._xstream)
+        exchanged = torch.cuda.Event()
+        exchanged.record(self._xstream)
+        sim.substep_rows(dt, step_number, 1, rows - 2, last=True)
+        stream.wait_event(exchanged)
 
     def computeDt(self):
         return self.grid.allreduce_min(np.float32(self.sim.computeDt()))
 
-    def full_exchange(self):
-        views = self.sim.halo_views()
+    def full_exchange(self, views=None, stream=None):
+        views = self.sim.halo_views() if views is None else views
         me = self.grid.rank
         sends, recvs = _exchange_plan(views, self.north, self.south)
-        stream = self.sim.comm_stream()
+        stream = self.sim.comm_stream() if stream is None else stream
         ctx = _stream_context(stream)
         with ctx:
             # a stripe that is its own neighbour (periodic, one rank) copies locally

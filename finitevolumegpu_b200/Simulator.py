@@ -222,20 +222,37 @@ class BaseSimulator(object):
         if self._cur is not None:
             self._cur ^= 1  # every stage launch writes the other buffer
 
+    def substep_rows(self, dt, step_number, row0, nrows, last=False):
+        """One band of tile rows of a substep (fv_sim_substep_rows): bands that
+        cover every tile row once, launched in order, equal substep().  `last`
+        marks the substep's final band, after which the current state is the
+        buffer the substep wrote."""
+        _lib.check(_lib.lib().fv_sim_substep_rows(self._handle, float(np.float32(dt)), int(step_number), int(row0),
+                                                  int(nrows)))
+        if last and self._cur is not None:
+            self._cur ^= 1
+
+    def tile_rows(self):
+        """Number of tile rows of a substep."""
+        r = ctypes.c_int()
+        _lib.check(_lib.lib().fv_sim_tile_rows(self._handle, ctypes.byref(r)))
+        return r.value
+
     def advance(self, n_steps):
         """Run exactly n_steps steps with simulate()'s dt schedule (benchmark helper)."""
         self._cur = None
         _lib.check(_lib.lib().fv_sim_advance(self._handle, int(n_steps)))
 
     # -- device state for row-stripe halo exchange (MPISimulator.py)
-    def halo_views(self):
+    def halo_views(self, pending=False):
         """Zero-copy torch views of the rows a north-south halo exchange moves, in
-        the buffer that holds the current state: a dict with 'south_ghost'
-        (domain rows -2, -1), 'south_send' (rows 0, 1), 'north_send' (rows
-        ny-2, ny-1) and 'north_ghost' (rows ny, ny+1), each a list with one
-        1-D float32 CUDA tensor per variable covering those two full storage
-        rows (ghost columns included).  Work on them must be ordered on
-        comm_stream()."""
+        the buffer that holds the current state (pending=True: the buffer the
+        substep whose bands are being launched writes): a dict with
+        'south_ghost' (domain rows -2, -1), 'south_send' (rows 0, 1),
+        'north_send' (rows ny-2, ny-1) and 'north_ghost' (rows ny, ny+1), each
+        a list with one 1-D float32 CUDA tensor per variable covering those two
+        full storage rows (ghost columns included).  Work on them must be
+        ordered after the stage launches that write them."""
         import torch
 
         if self._state is None or self._cur is None:
@@ -249,8 +266,10 @@ class BaseSimulator(object):
         ny = int(self.ny)
         dev = torch.device("cuda", self.context.device_id)
 
+        buf = self._cur ^ 1 if pending else self._cur
+
         def rows(var, r0):
-            base = addrs[self._cur * 4 + var] + r0 * pitch * 4
+            base = addrs[buf * 4 + var] + r0 * pitch * 4
             return torch.as_tensor(_DeviceRows(base, 2 * pitch), device=dev)
 
         views = {"south_ghost": 0, "south_send": 2, "north_send": ny, "north_ghost": ny + 2}

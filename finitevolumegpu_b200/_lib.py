@@ -68,6 +68,8 @@ _SIGNATURES = {
                        ctypes.POINTER(_P)], _I),
     "fv_sim_destroy": ([_P], _I),
     "fv_sim_substep": ([_P, _F, _I], _I),
+    "fv_sim_substep_rows": ([_P, _F, _I, _I, _I], _I),
+    "fv_sim_tile_rows": ([_P, ctypes.POINTER(_I)], _I),
     "fv_sim_step": ([_P, _F], _I),
     "fv_sim_simulate": ([_P, _D, _F, _I], _I),
     "fv_sim_advance": ([_P, _LL], _I),

@@ -615,8 +615,15 @@ cudaError_t launch_dependent(const void* fn, dim3 grid, dim3 block, void** args,
     return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
-int launch_stage(fv_sim* s, int substep, bool is_last, bool force_cfl, bool explicit_dt, float dt, bool sums) {
+int launch_stage(fv_sim* s, int substep, bool is_last, bool force_cfl, bool explicit_dt, float dt, bool sums,
+                 int row0 = 0, int nrows = -1) {
     alignas(64) StageArgs a = s->args;
+    dim3 grid = s->grid;
+    if (nrows >= 0) {  // a band of tile rows of the substep
+        a.tile_row0 = row0;
+        a.ntiles_total = (int)(s->grid.x * s->grid.y);
+        grid.y = (unsigned)nrows;
+    }
     a.substep = substep;
     a.is_last = is_last ? 1 : 0;
     a.force_cfl = force_cfl ? 1 : 0;
@@ -624,7 +631,7 @@ int launch_stage(fv_sim* s, int substep, bool is_last, bool force_cfl, bool expl
     a.dt_step = dt;
     a.want_sums = sums ? 1 : 0;
     void* kargs[] = {&a};
-    FV_CK(launch_dependent(reinterpret_cast<const void*>(s->ke->fn), s->grid, dim3(s->ke->NT), kargs,
+    FV_CK(launch_dependent(reinterpret_cast<const void*>(s->ke->fn), grid, dim3(s->ke->NT), kargs,
                            entry_smem(*s->ke), s->stream));
     return FV_OK;
 }
@@ -908,6 +915,22 @@ int fv_sim_substep(fv_sim* s, float dt, int step_number) {
     if (step_number < 0 || step_number >= s->num_substeps)
         return fail(FV_ERR_INVALID, "substep %d out of range", step_number);
     return launch_stage(s, step_number, false, true, true, dt, false);
+}
+
+int fv_sim_substep_rows(fv_sim* s, float dt, int step_number, int row0, int nrows) {
+    FV_TRY(check_sim(s));
+    if (step_number < 0 || step_number >= s->num_substeps)
+        return fail(FV_ERR_INVALID, "substep %d out of range", step_number);
+    if (row0 < 0 || nrows < 1 || row0 + nrows > (int)s->grid.y)
+        return fail(FV_ERR_INVALID, "tile rows [%d, %d) outside [0, %d)", row0, row0 + nrows, (int)s->grid.y);
+    return launch_stage(s, step_number, false, true, true, dt, false, row0, nrows);
+}
+
+int fv_sim_tile_rows(fv_sim* s, int* rows) {
+    FV_TRY(check_sim(s));
+    if (!rows) return fail(FV_ERR_INVALID, "null argument");
+    *rows = (int)s->grid.y;
+    return FV_OK;
 }
 
 int fv_sim_step(fv_sim* s, float dt) {

@@ -75,6 +75,9 @@ struct StageArgs {
     float variant_beta;  // parameter of the Osher and Sweby limiters (the variant itself is a kernel template)
     int wait_limit;      // tile-load wait: 0 = kWaitPolls polls (the default, also for zero-filled
                          // arguments), n > 0 = n polls, negative = give up at once (tests)
+    int tile_row0;       // first tile row of this launch (a substep may be split into launches by rows)
+    int ntiles_total;    // tiles of the whole substep, 0 = this launch's grid; the last of them to
+                         // arrive, over all launches, finishes the substep
 };
 
 // Polls of a bounded mbarrier wait before it gives up (each poll may suspend
@@ -245,8 +248,9 @@ __device__ __forceinline__ void stage_epilogue(const StageArgs& A, const StepCtl
     // The tile is written: the next substep's CTAs may launch once every CTA
     // of this grid is here (they wait in grid_dependency_wait for its end).
     grid_launch_dependents();
-    tile_epilogue<NT, NV>(A.ctl, A.block_cfl, A.block_sums, blockIdx.y * gridDim.x + blockIdx.x,
-                          gridDim.x * gridDim.y, A.is_last != 0, A.explicit_dt != 0, s, my_cfl, my_sums, sums);
+    tile_epilogue<NT, NV>(A.ctl, A.block_cfl, A.block_sums, (blockIdx.y + A.tile_row0) * gridDim.x + blockIdx.x,
+                          A.ntiles_total ? A.ntiles_total : gridDim.x * gridDim.y, A.is_last != 0,
+                          A.explicit_dt != 0, s, my_cfl, my_sums, sums);
 }
 
 // ------------------------------------------------------------------ tile load + ghost cells
@@ -792,7 +796,7 @@ __global__ void __launch_bounds__(NT) dimsplit_stage_kernel(const __grid_constan
     J.pitch = A.pitch;
     J.bc = A.bc;
     J.x0 = blockIdx.x * W;
-    J.y0 = blockIdx.y * H;
+    J.y0 = (blockIdx.y + A.tile_row0) * H;
     SplitPar P{A.dx, A.dy, A.g, A.gamma, A.theta, sc.dt * A.dt_scale, A.substep, A.variant_beta};
     process_tile_dimsplit<SCHEME, W, H, NT, false, VAR>(Qs, &bar, 0, true, J, P, sc.do_cfl, sums, &A.ctl->error, my_cfl,
                                                         my_sums, wait_polls(A.wait_limit));
@@ -911,7 +915,7 @@ __global__ void __launch_bounds__(NT) unsplit_stage_kernel(const __grid_constant
     grid_dependency_wait();  // the previous stage's state and control block
     const StepCtl sc = read_step(A);
     if (!sc.active) return;
-    const int x0 = blockIdx.x * W, y0 = blockIdx.y * H;
+    const int x0 = blockIdx.x * W, y0 = (blockIdx.y + A.tile_row0) * H;
     float my_cfl = __int_as_float(0x7f800000);
     double my_sums[3] = {0.0, 0.0, 0.0};
     const bool sums = A.want_sums && A.is_last;

@@ -100,6 +100,16 @@ FV_API int fv_sim_destroy(fv_sim* sim);
  * as the reference classes do.  Always writes the CFL field. */
 FV_API int fv_sim_substep(fv_sim* sim, float dt, int step_number);
 
+/* One band of tile rows [row0, row0 + nrows) of substep `step_number`, for
+ * overlapping a stripe's halo exchange with its interior (the reference's
+ * interior/exterior launches on two streams, MPISimulator.py:318-331,
+ * EE2D_KP07_dimsplit.py:140-266).  A substep launched as bands covering every
+ * tile row once, in order on the simulation's stream, equals fv_sim_substep;
+ * the band that arrives last finishes it.  fv_sim_tile_rows gives the number
+ * of tile rows. */
+FV_API int fv_sim_substep_rows(fv_sim* sim, float dt, int step_number, int row0, int nrows);
+FV_API int fv_sim_tile_rows(fv_sim* sim, int* rows);
+
 /* Replaces BaseSimulator.step(dt) (GPUSimulators/Simulator.py:220-228). */
 FV_API int fv_sim_step(fv_sim* sim, float dt);
 

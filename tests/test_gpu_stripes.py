@@ -83,3 +83,51 @@ def test_one_nccl_rank_periodic_self_exchange(ctx):
             assert np.array_equal(a, b)
     finally:
         dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("scheme", ["KP07_dimsplit", "KP07", "HLL", "EE2D_KP07_dimsplit"])
+def test_substep_bands_equal_substep(ctx, scheme):
+    """A substep launched as bands of tile rows (edges first, then the
+    interior, as MPISimulator overlaps them with the exchange) equals the
+    single launch bit for bit, CFL reduction included."""
+    nx, ny = 150, 230
+    q, dx, dy, g = global_state(scheme, nx, ny, seed=6)
+    a = make(ctx, scheme, q, nx, ny, dx, dy, g, MIXED)
+    b = make(ctx, scheme, q, nx, ny, dx, dy, g, MIXED)
+    rows = b.tile_rows()
+    assert rows >= 3
+    dt = np.float32(a.computeDt() * np.float32(0.45))
+    for _ in range(3):
+        for i in range(a.num_substeps):
+            a.substep(dt, i)
+            b.substep_rows(dt, i, 0, 1)
+            b.substep_rows(dt, i, rows - 1, 1)
+            b.substep_rows(dt, i, 1, rows - 2, last=True)
+    assert a.computeDt() == b.computeDt()
+    for x, y in zip(a.download(), b.download()):
+        assert np.array_equal(x, y)
+
+
+def test_nccl_overlap_equals_plain_exchange(ctx):
+    import torch
+    import torch.distributed as dist
+
+    nx, ny = 160, 200
+    q, dx, dy, g = global_state("KP07_dimsplit", nx, ny, seed=7)
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % free_port(), rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        outs = []
+        for overlap in (False, True):
+            sim = make(ctx, "KP07_dimsplit", q, nx, ny, dx, dy, g, PERIODIC)
+            mpi = MPISimulator(sim, StripeGrid(), overlap=overlap)
+            assert mpi.overlap == overlap
+            mpi.simulate(3.0)
+            outs.append((mpi.download(), mpi.simSteps()))
+        (a, na), (b, nb) = outs
+        assert na == nb
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+    finally:
+        dist.destroy_process_group()
