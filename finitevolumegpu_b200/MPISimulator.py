@@ -189,7 +189,13 @@ class MPISimulator(object):
         self.grid = grid
         # exchange the edge rows while the interior of the stripe is computed
         # (MPISimulator.py:318-331); needs at least three tile rows
-        self.overlap = bool(overlap) and hasattr(sim, "substep_rows") and sim.tile_rows() >= 3
+        self.overlap = False
+        if overlap and hasattr(sim, "substep_rows"):
+            # The exchange sends rows 0, 1 (tile row 0) and ny-2, ny-1, which lie
+            # in tile rows from (ny - 2) // H on: those are the edge bands.
+            rows, h = sim.tile_rows(), sim.tile_info()["tile_h"]
+            self._bottom = (int(sim.ny) - 2) // h
+            self.overlap = self._bottom >= 2 and rows >= 3
         self._xstream = None
         self.context = getattr(sim, "context", None)
         self.nx, self.ny, self.dx, self.dy = sim.nx, sim.ny, sim.dx, sim.dy
@@ -245,15 +251,16 @@ class MPISimulator(object):
         stream = sim.comm_stream()
         if self._xstream is None:
             self._xstream = torch.cuda.Stream(device=stream.device)
+        bottom = self._bottom
         sim.substep_rows(dt, step_number, 0, 1)
-        sim.substep_rows(dt, step_number, rows - 1, 1)
+        sim.substep_rows(dt, step_number, bottom, rows - bottom)
         edges_done = torch.cuda.Event()
         edges_done.record(stream)
         self._xstream.wait_event(edges_done)
         self.full_exchange(views=sim.halo_views(pending=True), stream=self._xstream)
         exchanged = torch.cuda.Event()
         exchanged.record(self._xstream)
-        sim.substep_rows(dt, step_number, 1, rows - 2, last=True)
+        sim.substep_rows(dt, step_number, 1, bottom - 1, last=True)
         stream.wait_event(exchanged)
 
     def computeDt(self):

@@ -108,11 +108,12 @@ def test_substep_bands_equal_substep(ctx, scheme):
         assert np.array_equal(x, y)
 
 
-def test_nccl_overlap_equals_plain_exchange(ctx):
+@pytest.mark.parametrize("ny", [200, 181])  # 181: the last tile row of 60 holds one row
+def test_nccl_overlap_equals_plain_exchange(ctx, ny):
     import torch
     import torch.distributed as dist
 
-    nx, ny = 160, 200
+    nx = 160
     q, dx, dy, g = global_state("KP07_dimsplit", nx, ny, seed=7)
     torch.cuda.set_device(0)
     dist.init_process_group("nccl", init_method="tcp://127.0.0.1:%d" % free_port(), rank=0, world_size=1,
