@@ -123,7 +123,18 @@ class Server(object):
         calling thread queues and admits the next chunk: their state is final
         (later chunks skip them), and their memory returns to the budget once
         released.  Several return threads copy results out in parallel.
+
+        Raises ValueError for a request of a scheme without batched kernels or
+        one that needs more device memory than the whole budget, and
+        MemoryError when the GPU has no room for a request while no other
+        scenario holds device memory (waiting could not help).
         """
+        for r in requests:
+            if r.scheme not in SCHEME_PARAMS:
+                raise ValueError("request %d: no batched kernels for scheme %r" % (r.rid, r.scheme))
+            if state_bytes(r.scheme, r.nx, r.ny) > self.budget:
+                raise ValueError("request %d: a %d x %d grid needs more device memory than the budget of %.3g bytes"
+                                 % (r.rid, r.nx, r.ny, self.budget))
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         running = {}  # (scheme, slot) -> (request, admitted, bytes): on the GPU, not yet at t_end
         results: List[Result] = []
@@ -196,6 +207,9 @@ class Server(object):
                     running[(bk, slot)] = (r, clock() - t0, need)
                 admitting = still
                 if requeue:
+                    if not (running or admitting or outstanding):
+                        raise MemoryError("request %d does not fit on the GPU with no other scenario resident"
+                                          % requeue[0].rid)
                     pending.extendleft(sorted(requeue, key=lambda r: r.arrival, reverse=True))
                 if not (pending or running or outstanding or admitting):
                     break
@@ -237,6 +251,8 @@ class Server(object):
                     except MemoryError:
                         with lock:
                             self.used -= need
+                        if not (running or admitting or outstanding):
+                            raise
                         break
                     pending.popleft()
                     running[(bk, slot)] = (r, clock() - t0, need)

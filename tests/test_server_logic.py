@@ -1,8 +1,9 @@
 """The server's scheduling logic on the CPU, with a stand-in for the GPU batch:
 every request is served exactly once with its own result, the device-memory
 budget is never exceeded, bursts go through the admission threads and single
-arrivals are admitted inline, and an admission that finds the GPU full is
-retried once memory has been released."""
+arrivals are admitted inline, an admission that finds the GPU full is
+retried once memory has been released, and requests that can never fit end
+serve() with an error instead of waiting for ever."""
 
 import threading
 
@@ -126,3 +127,32 @@ def test_full_gpu_admission_is_retried(fake):
     fake.full_once = {3, 7}
     results, _ = Server(None, budget_bytes=1e12, chunk_steps=2, schemes=("KP07_dimsplit",)).serve(reqs)
     assert sorted(r.rid for r in results) == list(range(12))
+
+
+def test_request_larger_than_the_budget_is_refused(fake):
+    reqs = requests(3, 0.0)
+    budget = 0.5 * state_bytes("KP07_dimsplit", 64, 64)
+    with pytest.raises(ValueError, match="request 0"):
+        Server(None, budget_bytes=budget, chunk_steps=1, schemes=("KP07_dimsplit",)).serve(reqs)
+
+
+def test_unknown_scheme_is_refused(fake):
+    reqs = requests(2, 0.0)
+    reqs[1].scheme = "LxF"  # unsplit: no batched kernels
+    with pytest.raises(ValueError, match="request 1"):
+        Server(None, budget_bytes=1e12, chunk_steps=1, schemes=("KP07_dimsplit",)).serve(reqs)
+
+
+@pytest.mark.parametrize("n,spacing", [(1, 0.0), (12, 0.0)])
+def test_gpu_full_with_nothing_resident_raises(fake, monkeypatch, n, spacing):
+    """A MemoryError while no other scenario holds device memory ends serve()
+    instead of retrying for ever: inline admission (one request) and through
+    the admission threads (a burst that all fails)."""
+
+    def add(self, *a, **kw):
+        raise MemoryError("full")
+
+    monkeypatch.setattr(FakeBatch, "add", add)
+    srv = Server(None, budget_bytes=1e12, chunk_steps=1, schemes=("KP07_dimsplit",))
+    with pytest.raises(MemoryError):
+        srv.serve(requests(n, spacing))
