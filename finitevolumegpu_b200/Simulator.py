@@ -93,8 +93,8 @@ class _VariableView(object):
         x, y, nx, ny = (int(v) for v in extent)
         if cpu_data is None:
             cpu_data = np.empty((ny, nx), dtype=np.float32)
-        assert cpu_data.shape == (ny, nx), "cpu_data shape does not match the extent"
-        assert cpu_data.dtype == np.float32 and cpu_data.flags.c_contiguous
+        _lib.require(cpu_data.shape == (ny, nx), "cpu_data shape does not match the extent")
+        _lib.require(cpu_data.dtype == np.float32 and cpu_data.flags.c_contiguous, "cpu_data must be C-ordered float32")
         _lib.check(_lib.lib().fv_sim_download_region(self._sim._handle, self._var, x, y, nx, ny,
                                                      cpu_data.ctypes.data_as(_lib._FP), nx))
         return cpu_data
@@ -106,7 +106,7 @@ class _VariableView(object):
             return self._sim.upload(self._var, cpu_data)
         x, y, nx, ny = (int(v) for v in extent)
         data = np.ascontiguousarray(cpu_data, dtype=np.float32)
-        assert data.shape == (ny, nx), "cpu_data shape does not match the extent"
+        _lib.require(data.shape == (ny, nx), "cpu_data shape does not match the extent")
         _lib.check(_lib.lib().fv_sim_upload_region(self._sim._handle, self._var, x, y, nx, ny,
                                                    data.ctypes.data_as(_lib._FP), nx))
 
@@ -173,13 +173,13 @@ class BaseSimulator(object):
         arrays = []
         for a in variables:
             a = np.asarray(a)
-            assert a.shape == (ny + 2 * gc, nx + 2 * gc) or a.shape == (ny, nx), "Wrong shape of data %s vs %s / %s" % (
-                str(a.shape), str((ny, nx)), str((ny + 2 * gc, nx + 2 * gc)))
-            assert a.itemsize == 4, "Wrong size of data type"
-            assert not np.isfortran(a) or a.ndim < 2 or a.shape[0] == 1, "Wrong datatype (Fortran, expected C)"
+            _lib.require(a.shape == (ny + 2 * gc, nx + 2 * gc) or a.shape == (ny, nx), "Wrong shape of data %s vs %s / %s" % (
+                str(a.shape), str((ny, nx)), str((ny + 2 * gc, nx + 2 * gc))))
+            _lib.require(a.itemsize == 4, "Wrong size of data type")
+            _lib.require(not np.isfortran(a) or a.ndim < 2 or a.shape[0] == 1, "Wrong datatype (Fortran, expected C)")
             arrays.append(np.ascontiguousarray(a, dtype=np.float32))
         shapes = {a.shape for a in arrays}
-        assert len(shapes) == 1, "all variables must have the same shape"
+        _lib.require(len(shapes) == 1, "all variables must have the same shape")
         rows, cols = arrays[0].shape
         tile = -1
         if getattr(self.context, "autotuner", None) is not None:
@@ -293,7 +293,8 @@ class BaseSimulator(object):
         nx, ny = int(self.nx), int(self.ny)
         if cpu_data is None:
             cpu_data = np.empty((ny, nx), dtype=np.float32)
-        assert cpu_data.shape == (ny, nx) and cpu_data.dtype == np.float32 and cpu_data.flags.c_contiguous
+        _lib.require(cpu_data.shape == (ny, nx) and cpu_data.dtype == np.float32 and cpu_data.flags.c_contiguous,
+                     "cpu_data must be a C-ordered float32 array of shape (ny, nx)")
         _lib.check(_lib.lib().fv_sim_download(self._handle, int(var), cpu_data.ctypes.data_as(_lib._FP), nx))
         return cpu_data
 
@@ -309,7 +310,7 @@ class BaseSimulator(object):
     def upload(self, var, data):
         """Replace the interior of variable `var` of the current state."""
         data = np.ascontiguousarray(data, dtype=np.float32)
-        assert data.shape == (int(self.ny), int(self.nx))
+        _lib.require(data.shape == (int(self.ny), int(self.nx)), "data shape does not match the grid")
         _lib.check(_lib.lib().fv_sim_upload(self._handle, int(var), data.ctypes.data_as(_lib._FP), int(self.nx)))
 
     def getOutput(self):

@@ -129,6 +129,14 @@ def lib():
     return _lib
 
 
+def require(cond, msg="invalid argument") -> None:
+    """An argument check that raises the reference's AssertionError and, unlike
+    an assert statement, still runs under ``python -O``: it guards the sizes of
+    host buffers handed to the C library."""
+    if not cond:
+        raise AssertionError(msg)
+
+
 def check(rc: int) -> None:
     """Map a C status code to the reference's Python exception types."""
     if rc == FV_OK:

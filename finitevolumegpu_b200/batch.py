@@ -61,15 +61,16 @@ class Batch(object):
             self._h = None
 
     def add(self, variables, nx, ny, dx, dy, t_end, boundary_conditions=None):
-        """Admit one simulation; returns its slot.  Raises MemoryError when the GPU has no room."""
+        """Admit one simulation; returns its slot.  Raises MemoryError when the
+        GPU has no room and AssertionError for the wrong number or shape of arrays."""
         bc = (boundary_conditions or BoundaryCondition()).asCodedInt()
-        arrays = []
-        for a in variables:
-            a = np.ascontiguousarray(a, dtype=np.float32)
-            assert a.shape in ((ny, nx), (ny + 2 * self.gc, nx + 2 * self.gc)), "Wrong shape of data %s" % (a.shape,)
-            arrays.append(a)
-        assert len(arrays) == self.nv
+        _lib.require(len(variables) == self.nv,
+                     "%s takes %d conserved variables, got %d" % (self.scheme, self.nv, len(variables)))
+        arrays = [np.ascontiguousarray(a, dtype=np.float32) for a in variables]
         rows, cols = arrays[0].shape
+        for a in arrays:
+            _lib.require(a.shape in ((ny, nx), (ny + 2 * self.gc, nx + 2 * self.gc)) and a.shape == (rows, cols),
+                         "Wrong shape of data %s for a %d x %d grid" % (a.shape, nx, ny))
         ptrs = (_lib._FP * self.nv)(*[a.ctypes.data_as(_lib._FP) for a in arrays])
         slot = ctypes.c_int()
         _lib.check(_L().fv_batch_add(self._h, int(nx), int(ny), float(dx), float(dy), int(bc), ptrs, rows, cols,

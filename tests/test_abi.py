@@ -119,3 +119,33 @@ def test_no_cpu_fallback():
     out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=dict(
         os.environ, CUDA_VISIBLE_DEVICES=""))
     assert "raised" in out.stdout, out.stdout + out.stderr
+
+
+def test_shape_checks_survive_python_O():
+    """The checks that guard host buffer sizes are not assert statements: under
+    ``python -O`` a mismatched variable still raises before any C call."""
+    import subprocess
+    import sys
+
+    code = ("import sys; sys.path.insert(0, %r)\n"
+            "import numpy as np\n"
+            "import finitevolumegpu_b200 as fv\n"
+            "class C:\n    handle = None\n    autotuner = None\n    device_name = 'none'\n"
+            "a = np.ones((8, 10), np.float32); b = np.ones((8, 9), np.float32)\n"
+            "try:\n    fv.KP07_dimsplit.KP07_dimsplit(C(), a, b, a, 10, 8, 1.0, 1.0, 9.81)\n"
+            "except AssertionError as e:\n    print('raised', e)\n"
+            "else:\n    print('ok')\n" % ROOT)
+    out = subprocess.run([sys.executable, "-O", "-c", code], capture_output=True, text=True)
+    assert "raised" in out.stdout, out.stdout + out.stderr
+
+
+@pytest.mark.parametrize("n_vars,shape", [(2, (8, 10)), (3, (8, 9))])
+def test_batch_add_rejects_bad_inputs(n_vars, shape):
+    from finitevolumegpu_b200.batch import Batch
+
+    b = Batch.__new__(Batch)  # no device: add() must refuse before reaching the library
+    b.scheme, b.nv, b.gc, b._h, b.shapes = "KP07_dimsplit", 3, 2, None, {}
+    good = np.ones((8, 10), np.float32)
+    arrays = [good] * (n_vars - 1) + [np.ones(shape, np.float32)]
+    with pytest.raises(AssertionError):
+        b.add(arrays, 10, 8, 1.0, 1.0, 1.0)
