@@ -7,14 +7,14 @@ the oracle is held to in test_oracle.py, here run through the CUDA path):
     bounds the FP64 oracle meets;
   * convergence order on a smooth wave (the reference's ConvergenceSmooth1D
     study): about 2 for the second-order schemes, about 1 for the first-order
-    ones, against a 2048-cell run of the same kernel;
+    ones, against an FP64 run of the scheme at 2048 cells;
   * mirror symmetry of a symmetric bump between reflective walls;
   * transpose equivariance of the dimensionally split substeps;
   * conservation of mass with reflective and periodic walls for every scheme.
 
-Thresholds come from the oracle on the same inputs: orders 1.76-2.02
-(second order) and 0.80-1.17 (first order); Stoker L1 errors at 512 cells
-between 3.3e-6 (WAF) and 4.6e-5 (LxF).
+Thresholds come from the oracle on the same inputs: orders between 64 and
+256 cells 1.81-2.02 (second order) and 0.80-1.00 (first order); Stoker L1
+errors at 512 cells between 3.3e-6 (WAF) and 4.6e-5 (LxF).
 """
 
 import numpy as np
@@ -23,6 +23,7 @@ import pytest
 from conftest import bump, dam_break, rel_linf
 
 import finitevolumegpu_b200 as fv
+from oracle.oracle import OracleSim
 from oracle.stoker import stoker
 
 pytestmark = pytest.mark.gpu
@@ -64,18 +65,32 @@ def test_dam_break_converges_to_stoker(ctx, scheme):
 
 @pytest.mark.parametrize("scheme", SWE)
 def test_smooth_convergence_order(ctx, scheme):
+    """Errors of the FP32 kernels at 64, 128 and 256 cells against an FP64 run
+    of the scheme at 2048 cells.  The reference solution is FP64 because FP32
+    itself drifts: the IEEE FP32 oracle ends 1.8e-5 (mean |h|) from FP64 after
+    the 1669 steps of the 2048-cell split run, one-signed, and 1.3e-6 after the
+    418 steps at 512 cells; the GPU kernels drift the same, which would mask
+    the truncation error of the finer grids.  At 256 cells the drift is near
+    3e-7 against errors of 1.8e-5 and more."""
     L, fine = 10.0, 2048
 
-    def run(nx):
+    def setup(nx):
         dx = L / nx
         x = (np.arange(nx) + 0.5) * dx
-        sim = make_sim(ctx, scheme, lines(1.0 + 0.05 * np.exp(-((x - 5.0) / 1.0) ** 2)), nx, 4, dx, dx)
-        sim.simulate(1.0, dt=0.4 * dx / (np.sqrt(9.81 * 1.05) + 0.05))
+        return lines(1.0 + 0.05 * np.exp(-((x - 5.0) / 1.0) ** 2)), dx, 0.4 * dx / (np.sqrt(9.81 * 1.05) + 0.05)
+
+    def run(nx):
+        q, dx, dt = setup(nx)
+        sim = make_sim(ctx, scheme, q, nx, 4, dx, dx)
+        sim.simulate(1.0, dt=dt)
         return sim.download()[0][1].astype(np.float64)
 
-    ref = run(fine)
-    errs = [np.mean(np.abs(run(nx) - ref.reshape(nx, fine // nx).mean(axis=1))) for nx in (64, 128, 256, 512)]
-    orders = [np.log2(errs[i] / errs[i + 1]) for i in range(3)]
+    q, dx, dt = setup(fine)
+    oracle = OracleSim(scheme, q, fine, 4, dx, dx, 9.81, dtype=np.float64)
+    oracle.simulate(1.0, dt=dt)
+    ref = oracle.download()[0][1]
+    errs = [np.mean(np.abs(run(nx) - ref.reshape(nx, fine // nx).mean(axis=1))) for nx in (64, 128, 256)]
+    orders = [np.log2(errs[i] / errs[i + 1]) for i in range(2)]
     if scheme in FIRST_ORDER:
         assert all(0.7 < o < 1.4 for o in orders), (scheme, errs, orders)
     else:
