@@ -16,6 +16,11 @@ reference's files.
 the directory and, for writing, a fresh file name (``name_0000.nc``, …) rather
 than overwriting an existing file.
 
+The module's small host helpers keep the reference's names and behaviour:
+``Timer`` (a logged ``with`` block timer), ``ProgressPrinter`` (the progress
+line ``runSimulation`` logs), ``safeCall``, ``getGitHash`` and
+``getGitStatus``.
+
 ``save_checkpoint`` / ``load_checkpoint`` have no reference counterpart: they
 store a simulator's state with its time-stepping state (t, nt, dt and the last
 CFL minimum) so that a run continued from the checkpoint takes exactly the
@@ -43,12 +48,110 @@ def quantize(data, least_significant_digit):
     return (np.around(scale * np.asarray(data, dtype=np.float64)) / scale).astype(np.float32)
 
 
+def safeCall(cmd):
+    """Output of `cmd` (a list) run in this package's directory, stderr merged
+    into it; a failing command is logged and its CalledProcessError re-raised
+    (GPUSimulators/Common.py:48-66)."""
+    try:
+        return subprocess.check_output(cmd, stderr=subprocess.STDOUT, cwd=os.path.dirname(os.path.abspath(__file__)),
+                                       universal_newlines=True, shell=False)
+    except subprocess.CalledProcessError as e:
+        logging.getLogger(__name__).error("Git failed, \nReturn code: %s\nOutput: %s", e.returncode, e.output)
+        raise
+
+
+def getGitHash():
+    """Commit hash of the checkout holding this package (Common.py:68-69)."""
+    return safeCall(["git", "rev-parse", "HEAD"])
+
+
+def getGitStatus():
+    """Changed tracked files of that checkout (Common.py:71-72)."""
+    return safeCall(["git", "status", "--porcelain", "-uno"])
+
+
 def _git(args):
+    """Like safeCall, but quietly "" where git or a checkout is missing: run
+    metadata must not stop (or log errors for) a simulation that runs from a
+    copy of the package."""
     try:
         return subprocess.check_output(["git"] + args, stderr=subprocess.STDOUT,
                                        cwd=os.path.dirname(os.path.abspath(__file__))).decode().strip()
     except (OSError, subprocess.CalledProcessError):
         return ""
+
+
+class Timer(object):
+    """Wall time of a ``with`` block, logged at `log_level` on exit as
+    "<tag>: <ms> ms"; ``secs`` and ``msecs`` hold it afterwards and
+    ``elapsed()`` reads it while the block runs (Common.py:215-238)."""
+
+    def __init__(self, tag, log_level=logging.DEBUG):
+        self.tag = tag
+        self.log_level = log_level
+        self.logger = logging.getLogger(__name__)
+
+    def __enter__(self):
+        self.start = time.time()
+        return self
+
+    def __exit__(self, *args):
+        self.end = time.time()
+        self.secs = self.end - self.start
+        self.msecs = self.secs * 1000.0
+        self.logger.log(self.log_level, "%s: %f ms", self.tag, self.msecs)
+
+    def elapsed(self):
+        return time.time() - self.start
+
+
+class ProgressPrinter(object):
+    """Progress line for a loop over `total_steps` units (Common.py:436-496).
+
+    ``getPrintString(step)`` returns None until `print_every` seconds have
+    passed since the last line, then a bar with the elapsed, remaining and
+    total time.  The remaining time extrapolates the time per unit, smoothed
+    over the lines printed so far (the newest interval weighs 0.8)."""
+
+    def __init__(self, total_steps, print_every=5):
+        self.logger = logging.getLogger(__name__)
+        self.start = time.time()
+        self.total_steps = total_steps
+        self.print_every = print_every
+        self.next_print_time = print_every
+        self.last_step = 0
+        self.secs_per_iter = None
+
+    def getPrintString(self, step):
+        elapsed = time.time() - self.start
+        if elapsed <= self.next_print_time:
+            return None
+        done = step - self.last_step
+        if done == 0:
+            return None
+        interval = elapsed - (self.next_print_time - self.print_every)
+        rate = interval / done
+        self.secs_per_iter = rate if not self.secs_per_iter else 0.2 * self.secs_per_iter + 0.8 * rate
+        self.last_step = step
+        self.next_print_time = elapsed + self.print_every
+        remaining = (self.total_steps - step) * self.secs_per_iter
+        return "{:s}. Total: {:s}, elapsed: {:s}, remaining: {:s}".format(
+            ProgressPrinter.progressBar(step, self.total_steps), ProgressPrinter.timeString(elapsed + remaining),
+            ProgressPrinter.timeString(elapsed), ProgressPrinter.timeString(remaining))
+
+    @staticmethod
+    def timeString(seconds):
+        """Whole seconds (at least 1) as "1h 2m 3s", zero fields left out."""
+        s = int(max(seconds, 1))
+        h, s = divmod(s, 3600)
+        m, s = divmod(s, 60)
+        return " ".join("%d%s" % (v, unit) for v, unit in ((h, "h"), (m, "m"), (s, "s")) if v)
+
+    @staticmethod
+    def progressBar(step, total_steps, width=30):
+        """"0% [####======] 100%" with `width` cells, '#' for the done fraction."""
+        filled = int(np.round(width * step / total_steps))
+        return "0% [" + "#" * filled + "=" * (width - filled) + "] 100%"
 
 
 def toJson(in_dict):
@@ -111,7 +214,9 @@ def runSimulation(simulator, simulator_args, outfile, save_times, save_var_names
     assert len(save_times) > 0, "Need to specify which times to save"
     timing = {"t_sim_init": 0.0, "t_nc_write": 0.0, "t_full_step": 0.0}
     t0 = time.time()
-    sim = simulator(**simulator_args)
+    with Timer("construct") as t:
+        sim = simulator(**simulator_args)
+    logger.info("Constructed in %s seconds", t.secs)
     with DataDumper(outfile, mode="w") as outdata:
         nc = outdata.ncfile
         nc.created = time.ctime(time.time())
@@ -139,6 +244,7 @@ def runSimulation(simulator, simulator_args, outfile, save_times, save_var_names
         t_steps[0] = save_times[0]
         t_steps[1:] = save_times[1:] - save_times[:-1]
         timing["t_sim_init"] = time.time() - t0
+        progress = ProgressPrinter(save_times[-1], print_every=10)
         for k in range(len(save_times)):
             try:
                 sim.check()
@@ -154,6 +260,9 @@ def runSimulation(simulator, simulator_args, outfile, save_times, save_var_names
             for i, name in enumerate(names):
                 ncvars[name][k, :, :] = quantize(values[i], least_significant_digit)
             timing["t_nc_write"] += time.time() - ts
+            line = progress.getPrintString(save_times[k])
+            if line:
+                logger.debug(line)
         logger.debug("Simulated to t=%f in %d steps", sim.simTime(), sim.simSteps())
         return outdata.filename, timing, None
 

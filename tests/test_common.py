@@ -71,3 +71,55 @@ def test_run_simulation_writes_quantised_frames(tmp_path):
             h, hv = ref.download([0, 2])
             assert np.array_equal(f.variables["h"][k], quantize(h, 3))
             assert np.array_equal(f.variables["hv"][k], quantize(hv, 3))
+
+
+def test_timer_records_and_logs(caplog):
+    import logging
+    import time
+
+    from finitevolumegpu_b200.Common import Timer
+
+    with caplog.at_level(logging.DEBUG, logger="finitevolumegpu_b200.Common"):
+        with Timer("block") as t:
+            time.sleep(0.02)
+            assert t.elapsed() > 0.0
+    assert 0.015 < t.secs < 2.0 and abs(t.msecs - 1000.0 * t.secs) < 1e-9
+    assert any(r.getMessage().startswith("block: ") and r.getMessage().endswith(" ms") for r in caplog.records)
+
+
+def test_progress_printer(monkeypatch):
+    import finitevolumegpu_b200.Common as common
+
+    clock = {"t": 100.0}
+    monkeypatch.setattr(common.time, "time", lambda: clock["t"])
+    p = common.ProgressPrinter(100, print_every=5)
+    clock["t"] = 103.0
+    assert p.getPrintString(10) is None            # before print_every seconds
+    clock["t"] = 110.0
+    line = p.getPrintString(50)                    # 10 s for 50 units: 0.2 s each, 50 left
+    assert line == "0% [" + "#" * 15 + "=" * 15 + "] 100%. Total: 20s, elapsed: 10s, remaining: 10s"
+    clock["t"] = 112.0
+    assert p.getPrintString(60) is None            # the next line is due 5 s after the last
+    clock["t"] = 116.0
+    assert p.getPrintString(50) is None            # no progress since the last line
+    assert common.ProgressPrinter.timeString(3725.9) == "1h 2m 5s"
+    assert common.ProgressPrinter.timeString(0.2) == "1s"
+    assert common.ProgressPrinter.timeString(120) == "2m"
+    assert common.ProgressPrinter.progressBar(0, 10, width=4) == "0% [====] 100%"
+    assert common.ProgressPrinter.progressBar(10, 10, width=4) == "0% [####] 100%"
+
+
+def test_git_helpers():
+    import re
+    import subprocess
+
+    from finitevolumegpu_b200.Common import getGitHash, getGitStatus, safeCall
+
+    try:
+        h = getGitHash()
+    except (OSError, subprocess.CalledProcessError):
+        pytest.skip("package not in a git checkout")
+    assert re.fullmatch(r"[0-9a-f]{40}\n", h)
+    assert isinstance(getGitStatus(), str)
+    with pytest.raises(subprocess.CalledProcessError):
+        safeCall(["git", "rev-parse", "--verify", "no-such-ref-here"])
