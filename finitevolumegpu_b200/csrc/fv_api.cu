@@ -1307,14 +1307,26 @@ int batch_publish(fv_batch* b) {
         int cap = b->work_cap;
         while (cap < n) cap *= 2;
         FV_CK(cudaStreamSynchronize(b->stream));  // the old list may still be read by queued kernels
-        cudaFree(b->d_work);
-        b->d_work = nullptr;
-        for (int k = 0; k < 2; ++k) {
-            cudaFreeHost(b->h_work[k]);
-            b->h_work[k] = nullptr;
+        // The new buffers are allocated before the old ones are released, so a
+        // failed allocation leaves the batch with its previous, consistent list
+        // (and graphs that still point at it); the next run retries the grow.
+        int2* d_new = nullptr;
+        int2* h_new[2] = {nullptr, nullptr};
+        if (cudaMalloc(reinterpret_cast<void**>(&d_new), (size_t)cap * sizeof(int2)) != cudaSuccess ||
+            cudaMallocHost(reinterpret_cast<void**>(&h_new[0]), (size_t)cap * sizeof(int2)) != cudaSuccess ||
+            cudaMallocHost(reinterpret_cast<void**>(&h_new[1]), (size_t)cap * sizeof(int2)) != cudaSuccess) {
+            if (d_new) cudaFree(d_new);
+            for (int k = 0; k < 2; ++k)
+                if (h_new[k]) cudaFreeHost(h_new[k]);
+            cudaGetLastError();  // an out-of-memory error is not sticky; clear it
+            return fail(FV_ERR_NOMEM, "out of memory growing the batch work list to %d tiles", cap);
         }
-        FV_CK(cudaMalloc(reinterpret_cast<void**>(&b->d_work), (size_t)cap * sizeof(int2)));
-        for (int k = 0; k < 2; ++k) FV_CK(cudaMallocHost(reinterpret_cast<void**>(&b->h_work[k]), (size_t)cap * sizeof(int2)));
+        cudaFree(b->d_work);
+        for (int k = 0; k < 2; ++k) cudaFreeHost(b->h_work[k]);
+        b->d_work = d_new;
+        b->h_work[0] = h_new[0];
+        b->h_work[1] = h_new[1];
+        b->bytes += (size_t)(cap - b->work_cap) * sizeof(int2);
         b->work_cap = cap;
         batch_drop_graphs(b);  // the graphs captured the old work-list pointer
     }

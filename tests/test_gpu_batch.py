@@ -82,6 +82,36 @@ def test_batch_matches_oracle(ctx):
         assert rel_linf(a, w) < 2e-5
 
 
+def test_batch_work_list_grows(ctx):
+    """Tiles beyond the initial work list (4096 entries) grow it, the second
+    time after the step graphs were captured on the old list, and every
+    simulation still equals its plain solve."""
+    b = Batch(ctx, "KP07_dimsplit", max_instances=32, tile=0)
+    info = b.info()
+    nx, ny = 1024, 512
+    per = -(-nx // info["tile_w"]) * -(-ny // info["tile_h"])  # 342 tiles of 60 x 28
+    cases = {}
+
+    def add_until(tiles):
+        while len(cases) * per <= tiles:
+            k = len(cases)
+            q, dx, dy, t_end = scenario("KP07_dimsplit", nx, ny, "bump" if k % 2 else "dam", 100 + k)
+            cases[b.add(q, nx, ny, dx, dy, t_end)] = (q, dx, dy, t_end)
+
+    add_until(4096)
+    b.run(2)
+    b.sync()
+    assert b.info()["work_items"] == len(cases) * per > 4096
+    add_until(8192)
+    b.run_to_completion()
+    assert b.info()["work_items"] == len(cases) * per > 8192
+    for slot, (q, dx, dy, t_end) in cases.items():
+        want, nt, _ = plain(ctx, "KP07_dimsplit", q, nx, ny, dx, dy, t_end)
+        assert b.status(slot)["nt"] == nt
+        for a, w in zip(b.download(slot), want):
+            assert np.array_equal(a, w)
+
+
 def test_batch_join_and_leave(ctx):
     """Simulations join and leave between chunks without disturbing the others."""
     b = Batch(ctx, "KP07_dimsplit", max_instances=8)
