@@ -219,12 +219,16 @@ typedef struct fv_batch fv_batch;
 FV_API int fv_batch_create(fv_context* ctx, int scheme, const fv_params* params, int max_instances, fv_batch** out);
 FV_API int fv_batch_destroy(fv_batch* batch);
 /* Admits one simulation (initial state as for fv_sim_create) that runs until
- * its time reaches t_end; returns its slot. */
+ * its time reaches t_end; returns its slot, or FV_ERR_NOMEM when the device
+ * has no room for it (the batch is unchanged). */
 FV_API int fv_batch_add(fv_batch* batch, int nx, int ny, float dx, float dy, int bc, const float* const* host_vars,
                         int host_rows, int host_cols, double t_end, int* slot);
 FV_API int fv_batch_remove(fv_batch* batch, int slot);
 /* Queues n_steps steps for every simulation of the batch (CUDA graphs of the
- * persistent kernel); simulations that reached t_end do nothing. Asynchronous. */
+ * persistent kernel); simulations that reached t_end do nothing. Asynchronous.
+ * Simulations admitted or removed since the last run join or leave the tile
+ * work list first; FV_ERR_NOMEM means the list could not grow, nothing was
+ * queued and the batch is unchanged (a later call retries). */
 FV_API int fv_batch_run(fv_batch* batch, int n_steps);
 /* Waits for queued work and refreshes the host view of every simulation. */
 FV_API int fv_batch_sync(fv_batch* batch);
