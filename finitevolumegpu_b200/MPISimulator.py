@@ -244,14 +244,22 @@ class MPISimulator(object):
         # The tile rows at the stripe's edges first; their rows go to the
         # neighbours on a second stream while the interior rows are computed,
         # and the next substep waits for both.
-        import torch
-
         sim = self.sim
         rows = sim.tile_rows()
         stream = sim.comm_stream()
+        bottom = self._bottom
+        if stream is None:
+            # A host-memory simulator: each call has completed when it returns,
+            # so the same band order runs without streams or events.
+            sim.substep_rows(dt, step_number, 0, 1)
+            sim.substep_rows(dt, step_number, bottom, rows - bottom)
+            self.full_exchange(views=sim.halo_views(pending=True))
+            sim.substep_rows(dt, step_number, 1, bottom - 1, last=True)
+            return
+        import torch
+
         if self._xstream is None:
             self._xstream = torch.cuda.Stream(device=stream.device)
-        bottom = self._bottom
         sim.substep_rows(dt, step_number, 0, 1)
         sim.substep_rows(dt, step_number, bottom, rows - bottom)
         edges_done = torch.cuda.Event()

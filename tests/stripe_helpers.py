@@ -11,7 +11,7 @@ import socket
 
 import numpy as np
 
-from oracle.oracle import OracleSim
+from oracle.oracle import DIMSPLIT_HALF_DT, OracleSim
 
 
 class OracleStripe(OracleSim):
@@ -25,22 +25,60 @@ class OracleStripe(OracleSim):
     def setBoundaryConditions(self, bc):
         self.bc = int(bc.asCodedInt())
 
-    def halo_views(self):
+    def halo_views(self, pending=False):
+        """Views of the current state's edge and ghost rows; with pending=True
+        of the buffer a substep in progress writes (BandedOracleStripe)."""
         import torch
 
         g, ny = self.gc, self.ny
+        bufs = self.u1 if pending else self.u0
 
         def rows(a, r0):
             return torch.from_numpy(a[r0:r0 + g].reshape(-1))
 
-        return {"south_ghost": [rows(a, 0) for a in self.u0], "south_send": [rows(a, g) for a in self.u0],
-                "north_send": [rows(a, ny) for a in self.u0], "north_ghost": [rows(a, ny + g) for a in self.u0]}
+        return {"south_ghost": [rows(a, 0) for a in bufs], "south_send": [rows(a, g) for a in bufs],
+                "north_send": [rows(a, ny) for a in bufs], "north_ghost": [rows(a, ny + g) for a in bufs]}
 
     def comm_stream(self):
         return None
 
     def synchronize(self):
         pass
+
+
+class BandedOracleStripe(OracleStripe):
+    """OracleStripe that also runs a substep in bands of tile rows, as the GPU
+    simulators' substep_rows does, so MPISimulator takes its overlapped
+    schedule (edge bands, exchange into the pending buffer, interior band).
+    A band writes only its rows of the output buffer: the full substep is
+    computed into a copy of that buffer and the band's rows are copied back
+    (the oracle, like the kernels, writes interior cells only).  The buffers
+    swap after the band marked last, whose CFL is the full grid's."""
+
+    TILE_H = 4
+
+    def tile_rows(self):
+        return -(-self.ny // self.TILE_H)
+
+    def tile_info(self):
+        return {"tile_h": self.TILE_H}
+
+    def substep_rows(self, dt, step_number, row0, nrows, last=False):
+        T = self.dtype.type
+        dt = T(dt)
+        kdt = T(dt * T(0.5)) if self.scheme in DIMSPLIT_HALF_DT else dt
+        out = self.u1
+        self.u1 = [a.copy() for a in out]
+        cfl = self._launch(kdt, int(step_number))
+        full, self.u1 = self.u1, out
+        y0 = self.gc + row0 * self.TILE_H
+        y1 = self.gc + min((row0 + nrows) * self.TILE_H, self.ny)
+        for a, f in zip(out, full):
+            a[y0:y1] = f[y0:y1]
+        if last:
+            if self.scheme != "WAF":
+                self.cfl = cfl
+            self.u0, self.u1 = self.u1, self.u0
 
 
 def global_state(scheme, nx, ny, seed=0):
@@ -66,8 +104,9 @@ def free_port():
         return s.getsockname()[1]
 
 
-def gloo_worker(rank, world, port, scheme, nx, ny, bc, t_end, out_path):
-    """One rank of a gloo run: simulate this rank's stripe and gather to rank 0."""
+def gloo_worker(rank, world, port, scheme, nx, ny, bc, t_end, out_path, banded=False):
+    """One rank of a gloo run: simulate this rank's stripe and gather to rank 0
+    (banded: with the overlapped schedule of banded substeps)."""
     import datetime
 
     import torch.distributed as dist
@@ -80,8 +119,11 @@ def gloo_worker(rank, world, port, scheme, nx, ny, bc, t_end, out_path):
         q, dx, dy, g = global_state(scheme, nx, ny)
         y0, rows = stripe_rows(ny, world)[rank]
         local = [a[y0:y0 + rows] for a in q]
-        sim = OracleStripe(scheme, local, nx, rows, dx, dy, g, cfl_scale=0.45, bc=bc)
+        cls = BandedOracleStripe if banded else OracleStripe
+        sim = cls(scheme, local, nx, rows, dx, dy, g, cfl_scale=0.45, bc=bc)
         mpi = MPISimulator(sim, StripeGrid())
+        if mpi.overlap != banded:
+            raise RuntimeError("overlapped schedule %s, expected %s" % (mpi.overlap, banded))
         mpi.simulate(t_end)
         parts = mpi.grid.gather(np.stack(mpi.download()))
         if rank == 0:
@@ -91,10 +133,10 @@ def gloo_worker(rank, world, port, scheme, nx, ny, bc, t_end, out_path):
         dist.destroy_process_group()
 
 
-def run_gloo(world, scheme, nx, ny, bc, t_end, out_path):
+def run_gloo(world, scheme, nx, ny, bc, t_end, out_path, banded=False):
     import torch.multiprocessing as mp
 
     os.environ.setdefault("GLOO_SOCKET_IFNAME", "lo")
-    mp.start_processes(gloo_worker, args=(world, free_port(), scheme, nx, ny, bc, t_end, out_path), nprocs=world,
-                       join=True, start_method="spawn")
+    mp.start_processes(gloo_worker, args=(world, free_port(), scheme, nx, ny, bc, t_end, out_path, banded),
+                       nprocs=world, join=True, start_method="spawn")
     return np.load(out_path)

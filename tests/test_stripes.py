@@ -90,3 +90,21 @@ def test_gloo_ranks_equal_single_domain(tmp_path, world, scheme, bc):
     res = run_gloo(world, scheme, nx, ny, bc, t_end_for(scheme), str(tmp_path / "out.npz"))
     assert int(res["nt"]) == nt and float(res["t"]) == t
     assert np.array_equal(res["state"], want), np.max(np.abs(res["state"] - want))
+
+
+@pytest.mark.parametrize("world,scheme,bc", [
+    (2, "KP07_dimsplit", PERIODIC),               # 21-row stripes: rows ny-2 and ny-1 in different tile rows
+    (3, "KP07_dimsplit", REFLECTIVE),             # 14-row stripes: both in the last tile row
+    (2, "KP07", MIXED),                           # RK2: stage 2 blends into the buffer being written
+    (1, "HLL2", PERIODIC),                        # a stripe that is its own neighbour: local copies
+    (2, "HLL", NS_REFLECTIVE_EW_PERIODIC),        # one ghost row
+])
+def test_gloo_overlapped_schedule_equals_single_domain(tmp_path, world, scheme, bc):
+    """MPISimulator's overlapped substep (edge tile rows, the exchange into the
+    buffer being written, then the interior rows) gives the single-domain run
+    bit for bit: the edge bands hold every row that is sent."""
+    nx, ny = 30, 42
+    want, nt, t = single(scheme, nx, ny, bc, t_end_for(scheme))
+    res = run_gloo(world, scheme, nx, ny, bc, t_end_for(scheme), str(tmp_path / "out.npz"), banded=True)
+    assert int(res["nt"]) == nt and float(res["t"]) == t
+    assert np.array_equal(res["state"], want), np.max(np.abs(res["state"] - want))
