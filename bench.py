@@ -25,6 +25,7 @@ import statistics
 import sys
 import threading
 import time
+import traceback
 
 import numpy as np
 
@@ -141,6 +142,17 @@ def load_profile():
             return json.load(f)
     except (OSError, ValueError):
         return {}
+
+
+def aux_leg(fn, *args, **kwargs):
+    """Runs one of the measurements beside the headline (batched, served, CPU
+    baseline).  A failure is reported in its place in the JSON line, with the
+    traceback on stderr, instead of taking the headline measurement with it."""
+    try:
+        return fn(*args, **kwargs)
+    except Exception as e:
+        traceback.print_exc()
+        return {"error": "%s: %s" % (type(e).__name__, e)}
 
 
 def cpu_baseline_leg(steps=3):
@@ -543,12 +555,12 @@ def run_mine(args, rank, world, local_rank):
         if result is not None:
             result["e2e"] = e2e
     if rank == 0 and world == 1 and not args.no_batched and scheme == SCHEME:
-        result["batched"] = run_batched(ctx)
+        result["batched"] = aux_leg(run_batched, ctx)
     if rank == 0 and world == 1 and not args.no_served and scheme == SCHEME:
-        result["served"] = run_served(ctx, n_req=args.served_requests,
-                                      rates=tuple(float(r) for r in args.served_rates.split(",")))
+        result["served"] = aux_leg(run_served, ctx, n_req=args.served_requests,
+                                   rates=tuple(float(r) for r in args.served_rates.split(",")))
     if rank == 0 and world == 1 and not args.no_cpu_baseline and scheme == SCHEME:
-        result["cpu_baseline"] = cpu_baseline_leg()
+        result["cpu_baseline"] = aux_leg(cpu_baseline_leg)
     return result
 
 

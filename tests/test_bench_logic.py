@@ -1,0 +1,39 @@
+"""bench.py's host logic on the CPU: a failing side measurement does not cost
+the headline line, and the reference arm (the CPU restatement of the
+reference algorithm) keeps the benchmark contract under torchrun: rank 0 alone
+prints one JSON line, every rank exits 0."""
+
+import json
+import os
+import subprocess
+import sys
+
+from conftest import ROOT
+
+import bench
+from stripe_helpers import free_port
+
+
+def test_aux_leg_reports_failures():
+    def failing(n, scale=1):
+        raise RuntimeError("leg %d failed" % (n * scale))
+
+    assert bench.aux_leg(failing, 2, scale=3) == {"error": "RuntimeError: leg 6 failed"}
+    assert bench.aux_leg(lambda a, b=0: {"v": a + b}, 2, b=5) == {"v": 7}
+
+
+def test_reference_arm_under_torchrun():
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
+           "127.0.0.1", "--master-port", str(free_port()), "bench.py", "--impl", "reference", "--gpus", "2",
+           "--steps", "1", "--warmup", "0"]
+    out = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600,
+                         env=dict(os.environ, OMP_NUM_THREADS="4"))
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [line for line in out.stdout.splitlines() if line.startswith("{")]
+    assert len(lines) == 1, out.stdout
+    res = json.loads(lines[0])
+    assert res["impl"] == "reference" and res["n_gpus"] == 2 and res["steps"] == 1
+    assert res["metric"] == "cell-updates/s" and res["higher_is_better"] is True and res["value"] > 0
+    assert res["cpu_baseline"]["value"] == res["value"] and res["cpu_baseline"]["kind"] == "port"
+    assert res["e2e"] == {"value": res["value"], "unit": res["unit"], "h2d_bytes_per_step": 0,
+                          "d2h_bytes_per_step": 0}
