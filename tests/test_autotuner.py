@@ -1,5 +1,6 @@
-"""Host-side parts of the autotuner's reference interface
-(GPUSimulators/Autotuner.py:226-287): the benchmark case and the sanity check."""
+"""Host-side parts of the autotuner: the reference interface's benchmark case
+and sanity check (GPUSimulators/Autotuner.py:226-287), the cache lookup, and
+the agreement of the tuned tile indices with the library's kernel tables."""
 
 import numpy as np
 
@@ -32,3 +33,55 @@ def test_size_classes():
     assert size_class(4096, 4096) == "4^12"
     assert size_class(256, 256) == "4^8"
     assert size_class(4096, 1024) == size_class(2048, 2048) == "4^11"
+
+
+SCHEME_OF = {"KP07_DIMSPLIT": "KP07_dimsplit", "HLL2": "HLL2", "WAF": "WAF", "FORCE": "FORCE", "HLL": "HLL",
+             "EE2D_KP07_DIMSPLIT": "EE2D_KP07_dimsplit", "LXF": "LxF", "KP07": "KP07"}
+
+
+def _table_counts(name):
+    """Entries per scheme of a tile table in fv_api.cu (kTable, kBatchTable)."""
+    import collections
+    import os
+    import re
+
+    from conftest import ROOT
+
+    src = open(os.path.join(ROOT, "finitevolumegpu_b200", "csrc", "fv_api.cu")).read()
+    body = re.search(r"const \w+ %s\[\] = \{(.*?)\n\};" % name, src, re.S).group(1)
+    return collections.Counter(SCHEME_OF[m] for m in re.findall(r"\{FV_(\w+), \d+, \d+, \d+", body))
+
+
+def test_tile_tables_match_the_library():
+    """The tile-configuration counts the tuner sweeps and every cached choice
+    exist in the library's kernel tables (an index past them fails at create)."""
+    import json
+
+    from finitevolumegpu_b200.Autotuner import BATCH_TILE_CONFIGS, DEFAULT_CACHE, TILE_CONFIGS
+
+    stage, batch = _table_counts("kTable"), _table_counts("kBatchTable")
+    assert dict(stage) == TILE_CONFIGS
+    assert dict(batch) == BATCH_TILE_CONFIGS
+    cache = json.load(open(DEFAULT_CACHE))
+    for device, schemes in cache.items():
+        for key, entry in schemes.items():
+            if key.startswith("batch:"):
+                assert 0 <= int(entry["tile"]) < BATCH_TILE_CONFIGS[key[6:]], (device, key)
+            else:
+                for cls, best in entry.items():
+                    assert 0 <= int(best["tile"]) < TILE_CONFIGS[key], (device, key, cls)
+
+
+def test_get_tile_falls_back(tmp_path):
+    import json
+
+    path = tmp_path / "cache.json"
+    json.dump({"Dev": {"HLL": {"4^8": {"tile": 2}, "4^12": {"tile": 1}}, "batch:HLL": {"tile": 3}}}, open(path, "w"))
+    t = Autotuner(cache_file=str(path))
+    assert t.get_tile("HLL", 256, 256, "Dev") == 2
+    assert t.get_tile("HLL", 4096, 4096, "Dev") == 1
+    assert t.get_tile("HLL", 512, 512, "Dev") == 2      # 4^9: nearest tuned class is 4^8
+    assert t.get_tile("HLL", 2048, 2048, "Dev") == 1    # 4^11: nearest tuned class is 4^12
+    assert t.get_tile("WAF", 256, 256, "Dev") == -1     # scheme never tuned: library default
+    assert t.get_tile("HLL", 256, 256, "Other") == -1   # device never tuned
+    assert t.get_batch_tile("HLL", "Dev") == 3 and t.get_batch_tile("WAF", "Dev") == -1
