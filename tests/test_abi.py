@@ -149,3 +149,43 @@ def test_batch_add_rejects_bad_inputs(n_vars, shape):
     arrays = [good] * (n_vars - 1) + [np.ones(shape, np.float32)]
     with pytest.raises(AssertionError):
         b.add(arrays, 10, 8, 1.0, 1.0, 1.0)
+
+
+def _header_prototypes():
+    """{name: (return type, [parameter types])} of every FV_API function."""
+    src = re.sub(r"/\*.*?\*/", " ", open(HEADER).read(), flags=re.S)
+    protos = {}
+    for ret, name, params in re.findall(r"^FV_API\s+([\w\s\*]+?)\s*\b(fv_\w+)\s*\((.*?)\);", src, flags=re.M | re.S):
+        types = []
+        for p in params.split(","):
+            p = " ".join(p.split())
+            if p in ("", "void"):
+                continue
+            ptr = p.count("*")
+            words = [w for w in re.findall(r"[A-Za-z_]\w*", p) if w != "const"]
+            base = " ".join(words[:-1]) if len(words) > 1 else words[0]  # drop the parameter name
+            types.append("ptr" if ptr else base)
+        protos[name] = (("ptr" if "*" in ret else " ".join(ret.split())), types)
+    return protos
+
+
+def _kind(ctype):
+    scalars = {ctypes.c_int: "int", ctypes.c_float: "float", ctypes.c_double: "double",
+               ctypes.c_longlong: "long long", ctypes.c_size_t: "size_t"}
+    if ctype in scalars:
+        return scalars[ctype]
+    if ctype in (ctypes.c_void_p, ctypes.c_char_p) or hasattr(ctype, "_type_") and issubclass(
+            ctype, ctypes._Pointer):
+        return "ptr"
+    return repr(ctype)
+
+
+def test_python_argtypes_match_header_prototypes():
+    """Every ctypes declaration passes as many arguments, of the same kinds, as
+    the C prototype takes: a mismatch would pass garbage through the ABI."""
+    protos = _header_prototypes()
+    assert len(protos) == len(declared_symbols())
+    for name, (ret, params) in protos.items():
+        args, res = _lib._SIGNATURES[name]
+        assert [_kind(a) for a in args] == params, name
+        assert _kind(res) == ret, name
