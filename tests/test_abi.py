@@ -189,3 +189,18 @@ def test_python_argtypes_match_header_prototypes():
         args, res = _lib._SIGNATURES[name]
         assert [_kind(a) for a in args] == params, name
         assert _kind(res) == ret, name
+
+
+def test_python_constants_and_params_match_header():
+    """Status codes, scheme ids and the fv_params layout restated in _lib.py
+    are the header's."""
+    src = re.sub(r"/\*.*?\*/", " ", open(HEADER).read(), flags=re.S)
+    codes = dict((k, int(v)) for k, v in re.findall(r"#define (FV_(?:OK|ERR_\w+))\s+(\d+)", src))
+    assert codes == {k: getattr(_lib, k) for k in codes} and len(codes) == 6
+    enum = dict((k, int(v)) for k, v in re.findall(r"FV_(\w+) = (\d+)", src))
+    ids = {k.upper(): v for k, v in _lib.SCHEME_IDS.items()}
+    assert enum == ids
+    body = re.search(r"typedef struct fv_params \{(.*?)\} fv_params;", src, re.S).group(1)
+    fields = re.findall(r"(float|int)\s+(\w+);", body)
+    ctype = {"float": ctypes.c_float, "int": ctypes.c_int}
+    assert [(n, ctype[t]) for t, n in fields] == list(_lib.fv_params._fields_)
