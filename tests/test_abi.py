@@ -204,3 +204,23 @@ def test_python_constants_and_params_match_header():
     fields = re.findall(r"(float|int)\s+(\w+);", body)
     ctype = {"float": ctypes.c_float, "int": ctypes.c_int}
     assert [(n, ctype[t]) for t, n in fields] == list(_lib.fv_params._fields_)
+
+
+def test_null_handles_are_rejected_before_any_cuda_call():
+    """Every entry point that takes a simulation or batch handle answers a null
+    handle with FV_ERR_INVALID and an error message (checked before any CUDA call, so
+    this runs without a GPU); destroying a null handle is a no-op."""
+    L = _lib.lib()
+    zero = {ctypes.c_int: 0, ctypes.c_float: 0.0, ctypes.c_double: 0.0, ctypes.c_longlong: 0}
+    names = [n for n in _lib._SIGNATURES if n.startswith(("fv_sim_", "fv_batch_"))
+             and not n.endswith(("_create", "_destroy"))]
+    assert len(names) >= 30
+    for name in names:
+        args, _ = _lib._SIGNATURES[name]
+        call = [zero.get(a) for a in args]  # pointers (and the handle) are NULL
+        rc = getattr(L, name)(*call)
+        assert rc == _lib.FV_ERR_INVALID, (name, rc)
+        assert L.fv_last_error().decode(), name  # a message for fv_last_error
+    assert L.fv_sim_destroy(None) == _lib.FV_OK and L.fv_batch_destroy(None) == _lib.FV_OK
+    assert L.fv_context_destroy(None) == _lib.FV_OK
+    assert L.fv_context_device_name(None, None, 0) == _lib.FV_ERR_INVALID
