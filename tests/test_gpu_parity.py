@@ -56,29 +56,36 @@ def test_scheme_vs_oracle(ctx, scheme, bcname):
 @pytest.mark.parametrize("scheme", SWE)
 def test_anisotropic_cells_and_gravity_vs_oracle(ctx, scheme):
     """dx != dy and a gravity other than 9.81: each sweep and flux takes its
-    own cell size, the CFL both.  On this case the oracle's own one-ulp spread
-    is at most that of the dx = dy = 1 case above (and it takes fewer steps),
-    so the bound is the same."""
+    own cell size, the CFL both.  The bound is that of the dx = dy = 1 case
+    above, or three times the oracle's own one-ulp spread on this case where
+    that is larger (it is 2e-7 to 8.3e-6 here, as on the dx = dy = 1 case)."""
     nx, ny = 141, 97
     h, hu, hv = bump(nx, ny)
     dx, dy, g = 0.8, 1.25, 3.7
+
+    def oracle_run(q):
+        o = OracleSim(scheme, q, nx, ny, dx, dy, g, cfl_scale=0.45, bc=MIXED)
+        o.simulate(4.0)
+        return o
+
     sim = make_sim(ctx, scheme, [h, hu, hv], nx, ny, dx=dx, dy=dy, g=g, bc=MIXED, cfl_scale=0.45)
-    ref = OracleSim(scheme, [h, hu, hv], nx, ny, dx, dy, g, cfl_scale=0.45, bc=MIXED)
     sim.simulate(4.0)
-    ref.simulate(4.0)
+    ref = oracle_run([h, hu, hv])
     assert sim.simSteps() == ref.simSteps()
     assert abs(sim.simTime() - ref.simTime()) < 1e-9
-    for a, b in zip(sim.download(), ref.download()):
-        assert rel_linf(a, b) < 2e-5, (scheme, rel_linf(a, b))
+    spread = ulp_sensitivity(lambda q: oracle_run(q).download(), [h, hu, hv])
+    for a, b, (s1, _) in zip(sim.download(), ref.download(), spread):
+        assert rel_linf(a, b) < max(2e-5, 3.0 * s1), (scheme, rel_linf(a, b), s1)
 
 
 @pytest.mark.parametrize("scheme,theta", [(s, t) for s in ("HLL2", "KP07", "KP07_dimsplit") for t in (1.0, 2.0)]
                          + [("EE2D_KP07_dimsplit", 1.0)])
 def test_theta_vs_oracle(ctx, scheme, theta):
     """The minmod parameter at both ends of its range (1: the most limiting,
-    2: the least) instead of the defaults the other cases use.  The oracle's
-    one-ulp spread on these cases is that of the default theta (SWE <= 8e-6,
-    Euler rho_v 2.3e-5 against 2.8e-5), so the bounds are the same."""
+    2: the least) instead of the defaults the other cases use.  The bounds
+    are those of the default-theta cases, or three times the oracle's own
+    one-ulp spread on the case where that is larger (SWE <= 8e-6 and Euler
+    rho_v 2.3e-5 here, against 2.8e-5 at the default theta)."""
     if scheme == "EE2D_KP07_dimsplit":
         nx, ny = 133, 70
         q = kelvin_helmholtz(nx, ny)
@@ -89,13 +96,19 @@ def test_theta_vs_oracle(ctx, scheme, theta):
         q = list(bump(nx, ny))
         kw = dict(dx=1.0, dy=1.0, g=9.81, bc=MIXED)
         t_end, tols = 4.0, (2e-5, 2e-5, 2e-5)
+
+    def oracle_run(q):
+        o = OracleSim(scheme, q, nx, ny, kw["dx"], kw["dy"], kw["g"], theta=theta, cfl_scale=0.45, bc=kw["bc"])
+        o.simulate(t_end)
+        return o
+
     sim = make_sim(ctx, scheme, q, nx, ny, theta=theta, cfl_scale=0.45, **kw)
-    ref = OracleSim(scheme, q, nx, ny, kw["dx"], kw["dy"], kw["g"], theta=theta, cfl_scale=0.45, bc=kw["bc"])
     sim.simulate(t_end)
-    ref.simulate(t_end)
+    ref = oracle_run(q)
     assert sim.simSteps() == ref.simSteps()
-    for a, b, tol in zip(sim.download(), ref.download(), tols):
-        assert rel_linf(a, b) < tol, (scheme, theta, rel_linf(a, b))
+    spread = ulp_sensitivity(lambda q: oracle_run(q).download(), q)
+    for a, b, tol, (s1, _) in zip(sim.download(), ref.download(), tols, spread):
+        assert rel_linf(a, b) < max(tol, 3.0 * s1), (scheme, theta, rel_linf(a, b), s1)
 
 
 @pytest.mark.parametrize("bcname", ["periodic", "reflective"])
