@@ -28,20 +28,28 @@ _libs = {}
 BLOCKS = ((32, 8), (32, 16), (32, 4), (8, 8))
 
 
-def ref_lib_path(scheme: str, block=None) -> str:
+# Builds of the default block besides the reference's own compile options:
+# "nofma" is fast math without FMA contraction (oracle/Makefile REF_NOFMA_LIBS).
+BUILDS = ("nofma",)
+
+
+def ref_lib_path(scheme: str, block=None, build=None) -> str:
+    if build is not None:
+        assert block is None and build in BUILDS, (block, build)
+        return os.path.join(REF_DIR, "libref_%s_%s.so" % (scheme, build))
     if block is None:
         return os.path.join(REF_DIR, "libref_%s.so" % scheme)
     return os.path.join(REF_DIR, "libref_%s_%dx%d.so" % (scheme, block[0], block[1]))
 
 
-def available(scheme: str = "KP07_dimsplit", block=None) -> bool:
-    return os.path.exists(ref_lib_path(scheme, block))
+def available(scheme: str = "KP07_dimsplit", block=None, build=None) -> bool:
+    return os.path.exists(ref_lib_path(scheme, block, build))
 
 
-def ref_lib(scheme: str, block=None):
-    key = (scheme, block)
+def ref_lib(scheme: str, block=None, build=None):
+    key = (scheme, block, build)
     if key not in _libs:
-        L = ctypes.CDLL(ref_lib_path(scheme, block))
+        L = ctypes.CDLL(ref_lib_path(scheme, block, build))
         P = ctypes.c_void_p
         L.ref_last_error.restype = ctypes.c_char_p
         L.ref_malloc.argtypes = [ctypes.POINTER(P), ctypes.c_size_t]
@@ -67,12 +75,13 @@ def _ck(L, rc):
 
 class RefKernelSim(OracleSim):
     """OracleSim's host loop with the reference kernels doing the substeps;
-    `block` = (w, h) picks one of the other block shapes (BLOCKS)."""
+    `block` = (w, h) picks one of the other block shapes (BLOCKS), `build`
+    one of the other builds of the default block (BUILDS)."""
 
-    def __init__(self, scheme, variables, nx, ny, dx, dy, g, block=None, **kw):
+    def __init__(self, scheme, variables, nx, ny, dx, dy, g, block=None, build=None, **kw):
         kw["dtype"] = np.float32
         super().__init__(scheme, variables, nx, ny, dx, dy, g, **kw)
-        self.L = ref_lib(scheme, block)
+        self.L = ref_lib(scheme, block, build)
         L = self.L
         self.bw, self.bh = L.ref_block_width(), L.ref_block_height()
         H, W = self.u0[0].shape

@@ -87,7 +87,9 @@ def cases(ic):
 
 
 if __name__ == "__main__":
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FVGPU_REFERENCE_ROOT", "")
+    if not ref_root:
+        sys.exit("usage: make_ic_golden.py <reference checkout> (or set FVGPU_REFERENCE_ROOT)")
     out = cases(load(ref_root))
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ic_ref.npz")
     np.savez_compressed(dst, **out)
