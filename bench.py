@@ -171,226 +171,217 @@ def cpu_baseline_leg(steps=3):
             "sample": "%d steps of the full 4096x4096 grid, FP64 C restatement (OpenMP, %d threads)" % (steps, cores)}
 
 
-def run_reference(args, rank, world):
-    """The reference algorithm on the host CPU (FP32 oracle), rank 0 only."""
+def run_reference(args, rank, world, budget_s=120.0):
+    """The reference algorithm on the host CPU (FP32 oracle), rank 0 only.
+
+    Each step is one KP07_dimsplit time step of the full 4096 x 4096 grid when
+    the --steps/--warmup run of that fits in about `budget_s` seconds of host
+    time; otherwise of the widest centred stripe that does (measured on one
+    calibration step of the full grid), and config.workload says which."""
     if rank != 0:
         return None
     from oracle.oracle import OracleSim
 
     cores = len(os.sched_getaffinity(0))
-    rows = 256  # bounded sample: a 4096 x 256 stripe of the grid per step
     h, hu, hv, _ = dam_break_4096()
-    r0 = NY // 2 - rows // 2
-    q = [a[r0:r0 + rows].copy() for a in (h, hu, hv)]
-    sim = OracleSim(SCHEME, q, NX, rows, 1.0, 1.0, 9.81, dtype=np.float32, nthreads=cores)
+
+    def make(rows):
+        r0 = NY // 2 - rows // 2
+        q = [a[r0:r0 + rows].copy() for a in (h, hu, hv)]
+        return OracleSim(SCHEME, q, NX, rows, 1.0, 1.0, 9.81, dtype=np.float32, nthreads=cores)
+
+    sim = make(NY)
     dt = sim.computeDt() * 0.9
-    for _ in range(args.warmup):
+    t0 = time.perf_counter()
+    sim.step(dt)  # calibration (and first warm-up) step of the full grid
+    full_s = time.perf_counter() - t0
+    n = max(1, args.steps + args.warmup - 1)
+    rows = NY
+    if n * full_s > budget_s:
+        rows = max(64, min(NY, int(NY * budget_s / (n * full_s)) // 8 * 8))
+        sim = make(rows)
+    for _ in range(args.warmup - 1):
         sim.step(dt)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         sim.step(dt)
     el = time.perf_counter() - t0
     v = NX * rows * args.steps / el
-    sample = "each step: one KP07_dimsplit time step of a 4096x%d stripe of the dam break, FP32, %d threads" % (
-        rows, cores)
+    what = "the full 4096x4096 grid" if rows == NY else "a centred 4096x%d stripe of the 4096x4096 grid" % rows
+    sample = "each step: one KP07_dimsplit time step of %s (dam break), FP32 C restatement, %d threads" % (what, cores)
     return {
         "metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-        "config": {"workload": "KP07_dimsplit 4096x4096 circular dam break (CPU sample 4096x%d)" % rows,
-                   "scheme": SCHEME, "nx": NX, "ny": NY, "parallelism": "host threads"},
+        "config": {"workload": "KP07_dimsplit circular dam break, CPU: %s per step" % what,
+                   "scheme": SCHEME, "nx": NX, "ny": rows, "parallelism": "host threads"},
         "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
 
-def bump_ic(nx, ny, rng):
-    """Gaussian bump: h = 1 + A exp(-r^2/(2 sigma^2)), A ~ U(0.1, 0.5), centre ~ U(0.3, 0.7) x domain, sigma = 20 cells."""
-    A = rng.uniform(0.1, 0.5)
-    cx, cy = rng.uniform(0.3, 0.7) * nx, rng.uniform(0.3, 0.7) * ny
-    x = np.arange(nx, dtype=np.float32) + 0.5
-    y = np.arange(ny, dtype=np.float32) + 0.5
-    h = 1.0 + A * np.exp(-((x[None, :] - cx) ** 2 + (y[:, None] - cy) ** 2) / (2 * 20.0 ** 2))
-    z = np.zeros((ny, nx), np.float32)
-    return [h.astype(np.float32), z, z.copy()]
+def reference_kernels_leg(my_ms_per_step, steps=40, warmup=5):
+    """The reference's own KP07_dimsplit kernel (its CUDA source compiled
+    unmodified for sm_100a) on the same 4096 x 4096 dam break on this GPU,
+    at the fastest of its default block and the other built block shapes:
+    CUDA events around `steps` steps of fixed dt (its kernel launches and
+    buffer swaps), against this library's ms per step."""
+    from oracle import ref_kernels
+
+    h, hu, hv, _ = dam_break_4096()
+    per_block = {}
+    for block in [None] + list(ref_kernels.BLOCKS):
+        if not ref_kernels.available(SCHEME, block):
+            continue
+        ref = ref_kernels.RefKernelSim(SCHEME, [h, hu, hv], NX, NY, 1.0, 1.0, 9.81, block=block)
+        dt = np.float32(ref.computeDt() * np.float32(0.9))
+        ref.time_steps(warmup, dt)
+        per_block["%dx%d" % (ref.bw, ref.bh)] = ref.time_steps(steps, dt)
+        ref.close()
+    best = min(per_block, key=per_block.get)
+    ms = per_block[best]
+    return {"what": "reference KP07DimsplitKernel, CUDA source compiled unmodified for sm_100a, same input and GPU",
+            "ms_per_step": ms, "block": best, "ms_per_step_by_block": per_block,
+            "cell_updates_per_s": NX * NY / (ms * 1e-3), "speedup_of_this_library": ms / my_ms_per_step}
 
 
-def dam_ic(nx, ny, rng):
-    """Circular dam break: h = 1 inside R ~ U(0.1, 0.3) x width of the centre, 0.1 outside."""
-    R = rng.uniform(0.1, 0.3) * nx
-    x = np.arange(nx, dtype=np.float32) + 0.5 - nx / 2.0
-    y = np.arange(ny, dtype=np.float32) + 0.5 - ny / 2.0
-    h = np.where(x[None, :] ** 2 + y[:, None] ** 2 < R * R, 1.0, 0.1).astype(np.float32)
-    z = np.zeros((ny, nx), np.float32)
-    return [h, z, z.copy()]
+class ICFeed(object):
+    """The clients' side of the served stream: initial states generated on
+    `threads` host threads ahead of their requests' admission (requests are
+    numbered in arrival order), at most `ahead` requests past the latest one
+    taken, so that the server's own threads only upload them."""
+
+    def __init__(self, make, count, threads=4, ahead=48):
+        import concurrent.futures
+
+        self.make = make
+        self.cv = threading.Condition()
+        self.taken = -1  # highest request index taken so far
+        self.pool = concurrent.futures.ThreadPoolExecutor(threads, thread_name_prefix="ic-feed")
+        self.futures = {}
+        self.ahead = ahead
+        self.stop = False
+        self.feeder = threading.Thread(target=self._feed, args=(count,), daemon=True)
+        self.feeder.start()
+
+    def _feed(self, count):
+        for i in range(count):
+            with self.cv:
+                while not self.stop and i > self.taken + self.ahead:
+                    self.cv.wait(0.1)
+                if self.stop:
+                    return
+                self.futures[i] = self.pool.submit(self.make, i)
+                self.cv.notify_all()
+
+    def get(self, i):
+        with self.cv:
+            while i not in self.futures and i > self.taken and not self.stop:
+                self.taken = max(self.taken, i - self.ahead)  # let the feeder reach i
+                self.cv.notify_all()
+                self.cv.wait(0.1)
+            fut = self.futures.pop(i, None)
+            self.taken = max(self.taken, i)
+            self.cv.notify_all()
+        # a retried admission (the GPU was full) takes its state a second time
+        return fut.result() if fut is not None else self.make(i)
+
+    def close(self):
+        with self.cv:
+            self.stop = True
+            self.cv.notify_all()
+        self.feeder.join()
+        self.pool.shutdown(wait=True)
 
 
-def kh_ic(nx, ny, rng, gamma=1.4):
-    """Kelvin-Helmholtz: rho = 2, u = +0.5 in the middle half band, rho = 1, u = -0.5 outside, p = 2.5,
-    v = 0.01 sin(4 pi x + phi) with seeded phase."""
-    phi = rng.uniform(0, 2 * np.pi)
-    yy = (np.arange(ny, dtype=np.float32) + 0.5) / ny
-    xx = (np.arange(nx, dtype=np.float32) + 0.5) / nx
-    band = ((yy >= 0.25) & (yy < 0.75))[:, None]
-    rho = np.where(band, 2.0, 1.0) * np.ones((1, nx))
-    u = np.where(band, 0.5, -0.5) * np.ones((1, nx))
-    v = 0.01 * np.sin(4 * np.pi * xx[None, :] + phi) * np.ones((ny, 1))
-    E = 2.5 / (gamma - 1.0) + 0.5 * rho * (u ** 2 + v ** 2)
-    return [a.astype(np.float32) for a in (rho, rho * u, rho * v, E)]
-
-
-def run_batched(ctx, n_inst=512, seed=4, check=4):
-    """Config 4: 512 KP07_dimsplit simulations, sides log-uniform in [64, 1024], bump or dam break,
-    t_end ~ U(5, 50): one batch of the persistent kernel vs the plain simulators one after another."""
-    from finitevolumegpu_b200 import KP07_dimsplit
-    from finitevolumegpu_b200.batch import Batch
-
-    rng = np.random.default_rng(seed)
-    cases = []
-    for i in range(n_inst):
-        nx = int(round(np.exp(rng.uniform(np.log(64), np.log(1024)))))
-        ny = int(round(np.exp(rng.uniform(np.log(64), np.log(1024)))))
-        q = bump_ic(nx, ny, rng) if rng.random() < 0.5 else dam_ic(nx, ny, rng)
-        cases.append((q, nx, ny, float(rng.uniform(5.0, 50.0))))
-    # Warm-up: one untimed admission of the whole workload grows the device
-    # memory pool and the pinned staging ring once, as a long-running service
-    # would have them; the plain path below runs with the same warm pool.
-    import torch
-
-    w = Batch(ctx, "KP07_dimsplit", max_instances=n_inst)
-    for (q, nx, ny, t_end) in cases:
-        w.add(q, nx, ny, 1.0, 1.0, t_end)
-    w.sync()
-    del w
-    # batched: admit all, run to completion, download all
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    b = Batch(ctx, "KP07_dimsplit", max_instances=n_inst)
-    slots = [b.add(q, nx, ny, 1.0, 1.0, t_end) for (q, nx, ny, t_end) in cases]
-    t_add = time.perf_counter()
-    dev_ms = 0.0
-    steps = 0
-    while True:
-        b.sync()
-        dev_ms += b.info()["last_run_ms"] if steps else 0.0
-        if all(b.status(s)["done"] for s in slots):
-            break
-        b.run(16)
-        steps += 16
-    t_run = time.perf_counter()
-    batched_out = b.download_many(slots)
-    nts = [b.status(s)["nt"] for s in slots]
-    t1 = time.perf_counter()
-    info = b.info()
-    del b
-    total = sum(nx * ny * nt for (q, nx, ny, t_end), nt in zip(cases, nts))
-    # plain: one simulator after the other
-    t2 = time.perf_counter()
-    max_diff = 0.0
-    plain_nts = []
-    for i, (q, nx, ny, t_end) in enumerate(cases):
-        sim = KP07_dimsplit.KP07_dimsplit(ctx, q[0], q[1], q[2], nx, ny, 1.0, 1.0, 9.81)
-        sim.simulate(t_end)
-        out = sim.download()
-        plain_nts.append(sim.simSteps())
-        for a, w in zip(out, batched_out[i]):
-            d = float(np.max(np.abs(a - w)))
-            max_diff = max(max_diff, d)
-        del sim
-    t3 = time.perf_counter()
-    # FP64 oracle on the smallest few simulations
-    l1 = 0.0
-    from oracle.oracle import OracleSim
-
-    small = sorted(range(n_inst), key=lambda i: cases[i][1] * cases[i][2])[:check]
-    for i in small:
-        q, nx, ny, t_end = cases[i]
-        o = OracleSim("KP07_dimsplit", q, nx, ny, 1.0, 1.0, 9.81, dtype=np.float64)
-        o.simulate(t_end)
-        for a, w in zip(batched_out[i], o.download()):
-            l1 = max(l1, float(np.sum(np.abs(a - w)) / max(np.sum(np.abs(w)), 1e-30)))
-    return {
-        "workload": "512 KP07_dimsplit simulations, sides log-uniform [64,1024] (seed %d), bump or dam break, "
-                    "t_end ~ U(5,50), each with its own CFL dt" % seed,
-        "cell_updates": total,
-        "batched_cell_updates_per_s": total / (t1 - t0),
-        "batched_device_cell_updates_per_s": total / (dev_ms / 1e3) if dev_ms else None,
-        "plain_cell_updates_per_s": total / (t3 - t2),
-        "speedup_vs_plain": (t3 - t2) / (t1 - t0),
-        "batched_s": {"admit": t_add - t0, "run": t_run - t_add, "download": t1 - t_run, "total": t1 - t0},
-        "plain_s": t3 - t2,
-        "steps_identical": nts == plain_nts,
-        "max_abs_diff_batched_vs_plain": max_diff,
-        "max_rel_l1_vs_fp64_oracle": l1,
-        "oracle_checked": len(small),
-        "tile": {k: info[k] for k in ("tile_w", "tile_h", "threads", "grid")},
-    }
-
-
-def run_served(ctx, n_req=400, rates=(300.0, 3000.0), seed=5, plain_sample=60, warmup_req=64):
+def run_served(ctx, n_req=10000, rates=(300.0, 600.0, 1500.0), seed=5, plain_sample=200, warmup_req=64):
     """Config 5: scenario requests with Poisson arrivals, scheme uniform over {KP07_dimsplit, HLL, EE2D},
     sides log-uniform [128, 2048], t_end ~ U(1, 20), served with continuous batching under a 120 GB budget.
-    The same scenarios are served at each arrival rate of the sweep (the last one saturates the server);
-    a short warm-up serve first pays the one-time costs (memory pool and pinned staging growth)."""
+    The same scenarios are served at each arrival rate of the sweep (the last one saturates the server).
+    Initial states are made from per-request seeds by client threads just ahead of admission, and each
+    result is reduced on the server's return threads to its FP64 per-variable sums (the first
+    `plain_sample` keep their arrays), so host memory stays bounded; the sums must agree across the
+    rates (each result is independent of what else was on the GPU).  A short warm-up serve first pays
+    the one-time costs (memory pool and pinned staging growth)."""
     from finitevolumegpu_b200 import SCHEMES, BoundaryCondition
     from finitevolumegpu_b200.server import Request, Server
 
     rng = np.random.default_rng(seed)
     schemes = ["KP07_dimsplit", "HLL", "EE2D_KP07_dimsplit"]
     periodic = BoundaryCondition(BoundaryCondition.getTypes(0x02020202))
-    scen = []
+    specs = []
     for i in range(n_req):
         s = schemes[int(rng.integers(0, 3))]
         nx = int(round(np.exp(rng.uniform(np.log(128), np.log(2048)))))
         ny = int(round(np.exp(rng.uniform(np.log(128), np.log(2048)))))
-        if s == "EE2D_KP07_dimsplit":
-            q, bc = kh_ic(nx, ny, rng), periodic  # unit cells: the Kelvin-Helmholtz family scaled to the grid
-        else:
-            q, bc = (bump_ic(nx, ny, rng) if rng.random() < 0.5 else dam_ic(nx, ny, rng)), None
-        scen.append((s, q, nx, ny, float(rng.uniform(1.0, 20.0)), bc))
+        kind = "kh" if s == "EE2D_KP07_dimsplit" else ("bump" if rng.random() < 0.5 else "dam")
+        specs.append((s, nx, ny, kind, float(rng.uniform(1.0, 20.0)), int(rng.integers(0, 2 ** 31))))
     gaps = np.random.default_rng(seed + 1).exponential(1.0, n_req)
 
-    def requests(rate, count=n_req):
-        t = np.cumsum(gaps[:count]) / rate
-        return [Request(i, s, q, nx, ny, 1.0, 1.0, te, arrival=float(t[i]), boundary_conditions=bc)
-                for i, (s, q, nx, ny, te, bc) in enumerate(scen[:count])]
+    def make_ic(i):
+        s, nx, ny, kind, _, icseed = specs[i]
+        r = np.random.default_rng(icseed)
+        # unit cells; the Euler requests are the Kelvin-Helmholtz family scaled to the grid
+        return {"kh": kh_ic, "bump": bump_ic, "dam": dam_ic}[kind](nx, ny, r)
 
-    Server(ctx, budget_bytes=120e9, chunk_steps=8).serve(requests(1e9, warmup_req))
-    sweep, results = [], None
+    def keep(req, state):
+        if req.rid < plain_sample:
+            return state
+        return tuple(float(a.sum(dtype=np.float64)) for a in state)
+
+    def serve(rate, count=n_req):
+        t = np.cumsum(gaps[:count]) / rate
+        feed = ICFeed(make_ic, count)
+        try:
+            reqs = [Request(i, s, (lambda i=i: feed.get(i)), nx, ny, 1.0, 1.0, te, arrival=float(t[i]),
+                            boundary_conditions=periodic if s == "EE2D_KP07_dimsplit" else None)
+                    for i, (s, nx, ny, _, te, _) in enumerate(specs[:count])]
+            return Server(ctx, budget_bytes=120e9, chunk_steps=8).serve(reqs, result_fn=keep)
+        finally:
+            feed.close()
+
+    serve(1e9, warmup_req)
+    sweep, sums, results = [], [], None
     for rate in rates:
-        results, st = Server(ctx, budget_bytes=120e9, chunk_steps=8).serve(requests(rate))
+        results, st = serve(rate)
         st["arrival_rate_per_s"] = rate
         sweep.append(st)
+        sums.append({r.rid: (r.state if r.rid >= plain_sample else
+                             tuple(float(a.sum(dtype=np.float64)) for a in r.state))
+                     for r in results if r.status == "done"})
     stats = dict(sweep[-1])
     # plain one-at-a-time path on a sample of the same requests
     by_id = {r.rid: r for r in results}
     t0 = time.perf_counter()
     cells = 0
     same = True
-    for i, (s, q, nx, ny, te, bc) in enumerate(scen[:plain_sample]):
+    for i in range(min(plain_sample, n_req)):
+        s, nx, ny, _, te, _ = specs[i]
+        q = make_ic(i)
         cls = SCHEMES[s]
-        kw = {} if bc is None else {"boundary_conditions": bc}
         if s == "EE2D_KP07_dimsplit":
-            sim = cls(ctx, *q, nx, ny, 1.0, 1.0, 0.0, 1.4, **kw)
+            sim = cls(ctx, *q, nx, ny, 1.0, 1.0, 0.0, 1.4, boundary_conditions=periodic)
         else:
-            sim = cls(ctx, *q, nx, ny, 1.0, 1.0, 9.81, **kw)
+            sim = cls(ctx, *q, nx, ny, 1.0, 1.0, 9.81)
         sim.simulate(te)
         out = sim.download()
         cells += nx * ny * sim.simSteps()
-        same = same and all(np.array_equal(a, w) for a, w in zip(out, by_id[i].state))
+        same = same and by_id[i].status == "done" and all(np.array_equal(a, w) for a, w in zip(out, by_id[i].state))
         del sim
     plain_rate = cells / (time.perf_counter() - t0)
     stats.update({
         "workload": "%d requests, Poisson arrivals (seed %d) swept over %s per s, schemes KP07_dimsplit/HLL/EE2D, "
                     "sides log-uniform [128,2048], t_end ~ U(1,20), 120 GB budget; top-level figures at the last "
                     "rate" % (n_req, seed, "/".join("%.0f" % r for r in rates)),
-        "sweep": [{k: v for k, v in st.items() if k in ("arrival_rate_per_s", "cell_updates_per_s", "p50_latency_s",
-                                                        "p99_latency_s", "mean_latency_s", "elapsed_s",
-                                                        "host_seconds")} for st in sweep],
+        "sweep": [{k: v for k, v in st.items() if k in ("arrival_rate_per_s", "requests", "rejected", "failed",
+                                                        "cell_updates_per_s", "p50_latency_s", "p99_latency_s",
+                                                        "mean_latency_s", "elapsed_s", "host_seconds")}
+                  for st in sweep],
         "plain_one_at_a_time_cell_updates_per_s": plain_rate,
-        "plain_sample_requests": plain_sample,
+        "plain_sample_requests": min(plain_sample, n_req),
         "speedup_vs_plain": stats["cell_updates_per_s"] / plain_rate,
         "results_identical_to_plain": same,
+        "results_identical_across_rates": all(d == sums[0] for d in sums[1:]) and len(sums[0]) == n_req,
     })
     return stats
 
@@ -426,6 +417,10 @@ def run_mine(args, rank, world, local_rank):
 
     dist = world > 1
     ctx = CudaContext.CudaContext(device=local_rank, autotuning=True)
+    if args.tile is not None:  # one tile configuration instead of the autotuner's choice (profiling)
+        from finitevolumegpu_b200.Autotuner import _Fixed
+
+        ctx.autotuner = _Fixed(args.tile)
     scheme = args.scheme
     sim, nx, ny, q0, desc = make_scheme_sim(ctx, scheme, rank)
     sim.advance(args.warmup)
@@ -561,6 +556,8 @@ def run_mine(args, rank, world, local_rank):
                                    rates=tuple(float(r) for r in args.served_rates.split(",")))
     if rank == 0 and world == 1 and not args.no_cpu_baseline and scheme == SCHEME:
         result["cpu_baseline"] = aux_leg(cpu_baseline_leg)
+    if rank == 0 and world == 1 and not args.no_reference_kernels and scheme == SCHEME and NX == 4096:
+        result["reference_kernels_gpu"] = aux_leg(reference_kernels_leg, dev_ms_per_step)
     return result
 
 
@@ -574,12 +571,17 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the 512-simulation batched workload")
     ap.add_argument("--no-served", action="store_true", help="skip the served request stream")
-    ap.add_argument("--served-requests", type=int, default=400)
-    ap.add_argument("--served-rates", default="300,3000",
+    ap.add_argument("--no-reference-kernels", action="store_true",
+                    help="skip timing the reference's own kernel on the same GPU")
+    ap.add_argument("--served-requests", type=int, default=10000)
+    ap.add_argument("--served-rates", default="300,600,1500",
                     help="Poisson arrival rates (requests/s) of the served sweep, comma separated; the last one "
                          "should saturate the server")
     ap.add_argument("--size", type=int, default=4096, help="grid side (the benchmark workload is 4096)")
     ap.add_argument("--scheme", default=SCHEME, help="scheme of the single-simulation timing (default KP07_dimsplit)")
+    ap.add_argument("--tile", type=int, default=None,
+                    help="tile configuration of the timed simulation (index into the scheme's kernel table; "
+                         "default: the autotuner's)")
     args = ap.parse_args()
     global NX, NY
     NX = NY = args.size

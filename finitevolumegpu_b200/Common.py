@@ -207,13 +207,19 @@ def runSimulation(simulator, simulator_args, outfile, save_times, save_var_names
                   least_significant_digit=3):
     """Run `simulator(**simulator_args)` and store `save_var_names` at each of
     `save_times` (None entries skip that variable) in a new NetCDF file.
-    Returns (file name, host timings); the third value of the reference (MPI
-    profiling) is None for a single simulator."""
+
+    Returns (file name, host timings, the simulator's profiling_data_mpi) as
+    the reference does (GPUSimulators/Common.py:98-105, :208).  The timings are
+    {"start": {stage: s}, "end": {stage: s}} with end - start the time spent in
+    each stage ("t_sim_init", "t_nc_write", "t_full_step"): host clock stamps
+    added up before and after each visit, as the reference adds them.  The
+    third value is None for a simulator without MPI profiling."""
     logger = logging.getLogger(__name__)
     save_times = np.asarray(save_times, dtype=np.float64)
     assert len(save_times) > 0, "Need to specify which times to save"
-    timing = {"t_sim_init": 0.0, "t_nc_write": 0.0, "t_full_step": 0.0}
-    t0 = time.time()
+    stages = ("t_sim_init", "t_nc_write", "t_full_step")
+    timing = {"start": {k: 0.0 for k in stages}, "end": {k: 0.0 for k in stages}}
+    timing["start"]["t_sim_init"] = time.time()
     with Timer("construct") as t:
         sim = simulator(**simulator_args)
     logger.info("Constructed in %s seconds", t.secs)
@@ -243,28 +249,28 @@ def runSimulation(simulator, simulator_args, outfile, save_times, save_var_names
         t_steps = np.empty_like(save_times)
         t_steps[0] = save_times[0]
         t_steps[1:] = save_times[1:] - save_times[:-1]
-        timing["t_sim_init"] = time.time() - t0
+        timing["end"]["t_sim_init"] = time.time()
         progress = ProgressPrinter(save_times[-1], print_every=10)
         for k in range(len(save_times)):
             try:
                 sim.check()
             except AssertionError as e:
                 logger.error("Error after %d steps (t=%f): %s", sim.simSteps(), sim.simTime(), str(e))
-                return outdata.filename, timing, None
-            ts = time.time()
+                return outdata.filename, timing, getattr(sim, "profiling_data_mpi", None)
+            timing["start"]["t_full_step"] += time.time()
             if t_steps[k] > 0.0:
                 sim.simulate(t_steps[k], dt)
-            timing["t_full_step"] += time.time() - ts
-            ts = time.time()
+            timing["end"]["t_full_step"] += time.time()
+            timing["start"]["t_nc_write"] += time.time()
             values = sim.download(download_vars)
             for i, name in enumerate(names):
                 ncvars[name][k, :, :] = quantize(values[i], least_significant_digit)
-            timing["t_nc_write"] += time.time() - ts
+            timing["end"]["t_nc_write"] += time.time()
             line = progress.getPrintString(save_times[k])
             if line:
                 logger.debug(line)
         logger.debug("Simulated to t=%f in %d steps", sim.simTime(), sim.simSteps())
-        return outdata.filename, timing, None
+        return outdata.filename, timing, getattr(sim, "profiling_data_mpi", None)
 
 
 # Constructor keyword arguments of each scheme beyond (context, fields, nx, ny, dx, dy, g).

@@ -38,6 +38,7 @@ cfl_scale, num_substeps``, ``substep(dt, step_number)``, ``computeDt()``,
 from __future__ import annotations
 
 import logging
+import time
 
 import numpy as np
 
@@ -175,6 +176,69 @@ def _exchange_plan(views, north, south):
     return sends, recvs
 
 
+class HaloProfile(object):
+    """The reference's ``profiling_data_mpi`` (GPUSimulators/MPISimulator.py:210-221):
+    {"start": {stage: s}, "end": {stage: s}, "n_time_steps": n}, read by its
+    drivers as end - start per stage (mpiTesting.py:171-177).
+
+    The reference adds host time stamps; here each stage's duration is timed
+    with CUDA events on the stream the stage runs on (host clock for
+    host-memory simulators) and added to "end", "start" staying 0, so
+    end - start is the same total.  Stages: "t_mpi_step" (the stage kernels of
+    a substep), "t_mpi_halo_exchange" (a whole exchange) and
+    "t_mpi_halo_exchange_sendreceive" (its point-to-point messages).  The
+    exchange moves rows between device buffers directly, with no host staging,
+    so "t_mpi_halo_exchange_download" and "..._upload" stay 0.
+    "n_time_steps" counts substeps, as the reference's does (:338).  Event
+    pairs are read back lazily, when the dictionary is read."""
+
+    STAGES = ("t_mpi_halo_exchange", "t_mpi_halo_exchange_download", "t_mpi_halo_exchange_upload",
+              "t_mpi_halo_exchange_sendreceive", "t_mpi_step")
+    MAX_PENDING = 512  # event pairs kept before the oldest are read back
+
+    def __init__(self):
+        self.data = {"start": {k: 0 for k in self.STAGES}, "end": {k: 0 for k in self.STAGES}, "n_time_steps": 0}
+        self._pending = []  # (stage, start event, end event)
+        self._free = []
+
+    def _event(self):
+        if self._free:
+            return self._free.pop()
+        import torch
+
+        return torch.cuda.Event(enable_timing=True)
+
+    def begin(self, stream):
+        """A token marking the start of a stage on `stream` (None: host clock)."""
+        if stream is None:
+            return time.perf_counter()
+        ev = self._event()
+        ev.record(stream)
+        return ev
+
+    def end(self, stage, token, stream):
+        if stream is None:
+            self.data["end"][stage] += time.perf_counter() - token
+            return
+        ev = self._event()
+        ev.record(stream)
+        self._pending.append((stage, token, ev))
+        if len(self._pending) > self.MAX_PENDING:
+            self._resolve(len(self._pending) // 2)
+
+    def _resolve(self, n=None):
+        n = len(self._pending) if n is None else n
+        done, self._pending = self._pending[:n], self._pending[n:]
+        for stage, e0, e1 in done:
+            e1.synchronize()
+            self.data["end"][stage] += e0.elapsed_time(e1) / 1000.0
+            self._free += [e0, e1]
+
+    def read(self):
+        self._resolve()
+        return self.data
+
+
 class MPISimulator(object):
     """One stripe of a decomposed simulation (GPUSimulators/MPISimulator.py:205-480).
 
@@ -187,6 +251,7 @@ class MPISimulator(object):
         self.logger = logging.getLogger(__name__)
         self.sim = sim
         self.grid = grid
+        self._profile = HaloProfile()
         # exchange the edge rows while the interior of the stripe is computed
         # (MPISimulator.py:318-331); needs at least three tile rows
         self.overlap = False
@@ -236,9 +301,19 @@ class MPISimulator(object):
         self.t = float(self.t) + float(np.float32(dt))
         self.nt += 1
 
+    @property
+    def profiling_data_mpi(self):
+        """Accumulated stage times and substep count (see HaloProfile)."""
+        return self._profile.read()
+
     def substep(self, dt, step_number):
+        prof = self._profile
+        prof.data["n_time_steps"] += 1
         if not self.overlap:
+            stream = self.sim.comm_stream()
+            tok = prof.begin(stream)
             self.sim.substep(dt, step_number)
+            prof.end("t_mpi_step", tok, stream)
             self.full_exchange()
             return
         # The tile rows at the stripe's edges first; their rows go to the
@@ -248,6 +323,7 @@ class MPISimulator(object):
         rows = sim.tile_rows()
         stream = sim.comm_stream()
         bottom = self._bottom
+        tok = prof.begin(stream)
         if stream is None:
             # A host-memory simulator: each call has completed when it returns,
             # so the same band order runs without streams or events.
@@ -255,6 +331,7 @@ class MPISimulator(object):
             sim.substep_rows(dt, step_number, bottom, rows - bottom)
             self.full_exchange(views=sim.halo_views(pending=True))
             sim.substep_rows(dt, step_number, 1, bottom - 1, last=True)
+            prof.end("t_mpi_step", tok, stream)
             return
         import torch
 
@@ -269,6 +346,7 @@ class MPISimulator(object):
         exchanged = torch.cuda.Event()
         exchanged.record(self._xstream)
         sim.substep_rows(dt, step_number, 1, bottom - 1, last=True)
+        prof.end("t_mpi_step", tok, stream)  # the stage kernels of all bands
         stream.wait_event(exchanged)
 
     def computeDt(self):
@@ -280,7 +358,9 @@ class MPISimulator(object):
         sends, recvs = _exchange_plan(views, self.north, self.south)
         stream = self.sim.comm_stream() if stream is None else stream
         ctx = _stream_context(stream)
+        prof = getattr(self, "_profile", None)
         with ctx:
+            t_all = prof.begin(stream) if prof else None
             # a stripe that is its own neighbour (periodic, one rank) copies locally
             nv = len(views["north_send"])
             if self.south == me:
@@ -289,7 +369,12 @@ class MPISimulator(object):
             if self.north == me:
                 for v in range(nv):
                     views["north_ghost"][v].copy_(views["south_send"][v])
-            self.grid.exchange([s for s in sends if s[0] != me], [r for r in recvs if r[0] != me])
+            t_msg = prof.begin(stream) if prof else None
+            with _nvtx("fv halo exchange"):
+                self.grid.exchange([s for s in sends if s[0] != me], [r for r in recvs if r[0] != me])
+            if prof:
+                prof.end("t_mpi_halo_exchange_sendreceive", t_msg, stream)
+                prof.end("t_mpi_halo_exchange", t_all, stream)
 
     def download(self, variables=None):
         return self.sim.download(variables) if variables is not None else self.sim.download()
@@ -319,6 +404,20 @@ class MPISimulator(object):
         i, j = self.grid.getCoordinate()
         x0, y0 = i * width, j * height
         return [x0, x0 + width, y0, y0 + height]
+
+
+def _nvtx(name):
+    """An NVTX range on a profiler's timeline (a no-op without CUDA)."""
+    import contextlib
+
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            return torch.cuda.nvtx.range(name)
+    except Exception:
+        pass
+    return contextlib.nullcontext()
 
 
 def _stream_context(stream):

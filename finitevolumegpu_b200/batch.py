@@ -93,7 +93,9 @@ class Batch(object):
         t, nt, dt, done = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_float(), ctypes.c_int()
         _lib.check(_L().fv_batch_status(self._h, int(slot), ctypes.byref(t), ctypes.byref(nt), ctypes.byref(dt),
                                         ctypes.byref(done)))
-        return {"t": t.value, "nt": nt.value, "dt": dt.value, "done": bool(done.value)}
+        # done: reached t_end or failed; failed: a step left a non-finite value or
+        # a non-positive depth (density), or t/dt is not a number
+        return {"t": t.value, "nt": nt.value, "dt": dt.value, "done": bool(done.value), "failed": done.value == 2}
 
     def download(self, slot):
         ny, nx = self.shapes[slot]

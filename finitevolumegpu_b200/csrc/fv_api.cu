@@ -10,6 +10,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <condition_variable>
@@ -100,6 +101,16 @@ const KEntry kTable[] = {
     {FV_KP07, 120, 60, 128, false, fv::unsplit_stage_kernel<fv::KP07, 120, 60, 128>},
     {FV_KP07, 120, 60, 256, false, fv::unsplit_stage_kernel<fv::KP07, 120, 60, 256>},
     {FV_KP07, 60, 28, 128, false, fv::unsplit_stage_kernel<fv::KP07, 60, 28, 128>},
+    // two lines per thread in packed FP32 (same cells, bit for bit)
+    {FV_KP07_DIMSPLIT, 124, 28, 64, true, fv::dimsplit_stage_kernel<fv::KP07_DIMSPLIT, 124, 28, 64, 0, 2>},
+    {FV_KP07_DIMSPLIT, 124, 60, 128, true, fv::dimsplit_stage_kernel<fv::KP07_DIMSPLIT, 124, 60, 128, 0, 2>},
+    {FV_KP07_DIMSPLIT, 60, 28, 64, true, fv::dimsplit_stage_kernel<fv::KP07_DIMSPLIT, 60, 28, 64, 0, 2>},
+    {FV_HLL2, 124, 28, 64, true, fv::dimsplit_stage_kernel<fv::HLL2, 124, 28, 64, 0, 2>},
+    {FV_HLL2, 124, 60, 128, true, fv::dimsplit_stage_kernel<fv::HLL2, 124, 60, 128, 0, 2>},
+    {FV_HLL2, 60, 28, 64, true, fv::dimsplit_stage_kernel<fv::HLL2, 60, 28, 64, 0, 2>},
+    {FV_EE2D_KP07_DIMSPLIT, 124, 28, 64, true, fv::dimsplit_stage_kernel<fv::EE2D, 124, 28, 64, 0, 2>},
+    {FV_EE2D_KP07_DIMSPLIT, 124, 60, 128, true, fv::dimsplit_stage_kernel<fv::EE2D, 124, 60, 128, 0, 2>},
+    {FV_EE2D_KP07_DIMSPLIT, 60, 28, 64, true, fv::dimsplit_stage_kernel<fv::EE2D, 60, 28, 64, 0, 2>},
 };
 constexpr int kNumEntries = sizeof(kTable) / sizeof(kTable[0]);
 
@@ -598,6 +609,16 @@ int write_ctl(fv_sim* s) {
     return FV_OK;
 }
 
+// An NVTX range over a host-side scope (stage launches, graph replays, batch
+// runs and syncs), visible on a profiler's timeline; without a profiler
+// attached the push and pop return at once.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
 // Stage kernels are launched with programmatic stream serialization: the next
 // substep's CTAs may launch while this one's last CTAs run, and wait in the
 // kernel (grid_dependency_wait) for its completion before reading anything.
@@ -617,6 +638,7 @@ cudaError_t launch_dependent(const void* fn, dim3 grid, dim3 block, void** args,
 
 int launch_stage(fv_sim* s, int substep, bool is_last, bool force_cfl, bool explicit_dt, float dt, bool sums,
                  int row0 = 0, int nrows = -1) {
+    NvtxRange range(nrows >= 0 ? "fv stage launch (band)" : "fv stage launch");
     alignas(64) StageArgs a = s->args;
     dim3 grid = s->grid;
     if (nrows >= 0) {  // a band of tile rows of the substep
@@ -660,6 +682,7 @@ int build_graph(fv_sim* s, int nsteps, cudaGraphExec_t* out) {
 }
 
 int run_steps(fv_sim* s, long long k) {
+    NvtxRange range("fv step graph replays");
     if (!s->graph1) FV_TRY(build_graph(s, 1, &s->graph1));
     if (!s->graph16) FV_TRY(build_graph(s, 16, &s->graph16));
     while (k >= 16) {
@@ -941,6 +964,7 @@ int fv_sim_step(fv_sim* s, float dt) {
 }
 
 int fv_sim_simulate(fv_sim* s, double t, float dt, int use_dt) {
+    NvtxRange range("fv_sim_simulate");
     FV_TRY(check_sim(s));
     FV_TRY(read_ctl(s));
     SimCtl& c = *s->ctl_h;
@@ -1257,6 +1281,17 @@ void batch_drop_graphs(fv_batch* b) {
     if (b->graph1) cudaGraphExecDestroy(b->graph1);
     if (b->graph16) cudaGraphExecDestroy(b->graph16);
     b->graph1 = b->graph16 = nullptr;
+}
+
+// 0 running, 1 reached t_end (simulate()'s stopping rule), 2 failed: a step
+// left a non-finite value or a non-positive depth (density), t or dt is not a
+// number, or dt is not positive before t_end.
+int batch_done_state(const SimCtl& c) {
+    if (c.bad || std::isnan(c.t) || std::isnan(c.dt)) return 2;
+    if (c.t < c.t_end && !(c.dt > 0.0f)) return 2;  // cannot advance (simulate() would stop here)
+    const double rem = c.t_end - c.t;
+    const float cur = (float)((rem < (double)c.dt) ? rem : (double)c.dt);
+    return (!(c.t < c.t_end) || cur <= 0.0f) ? 1 : 0;
 }
 
 int batch_launch_step(fv_batch* b) {
@@ -1599,6 +1634,7 @@ int fv_batch_remove(fv_batch* b, int slot) {
 }
 
 int fv_batch_run(fv_batch* b, int n_steps) {
+    NvtxRange range("fv batch run (graph replays)");
     FV_TRY(check_batch(b));
     if (n_steps < 0) return fail(FV_ERR_INVALID, "negative step count");
     std::lock_guard<std::mutex> lock(b->mu);
@@ -1623,6 +1659,7 @@ int fv_batch_run(fv_batch* b, int n_steps) {
 }
 
 int fv_batch_sync(fv_batch* b) {
+    NvtxRange range("fv batch sync");
     FV_TRY(check_batch(b));
     {
         std::lock_guard<std::mutex> lock(b->mu);
@@ -1635,10 +1672,7 @@ int fv_batch_sync(fv_batch* b) {
     std::lock_guard<std::mutex> lock(b->mu);
     for (int s = 0; s < b->max_inst; ++s) {
         if (!b->used[s] || !b->registered[s]) continue;
-        const SimCtl& c = b->h_ctl[s];
-        const double rem = c.t_end - c.t;
-        const float cur = (float)((rem < (double)c.dt) ? rem : (double)c.dt);
-        b->done_at_sync[s] = (!(c.t < c.t_end) || cur <= 0.0f) ? 1 : 0;
+        b->done_at_sync[s] = batch_done_state(b->h_ctl[s]);
     }
     float ms = 0.0f;
     if (cudaEventElapsedTime(&ms, b->ev0, b->ev1) == cudaSuccess) b->last_ms = ms;
@@ -1655,11 +1689,7 @@ int fv_batch_status(fv_batch* b, int slot, double* t, long long* nt, float* dt, 
     if (t) *t = c.t;
     if (nt) *nt = c.nt;
     if (dt) *dt = c.dt;
-    if (done) {
-        const double rem = c.t_end - c.t;
-        const float cur = (float)((rem < (double)c.dt) ? rem : (double)c.dt);
-        *done = (!(c.t < c.t_end) || cur <= 0.0f) ? 1 : 0;
-    }
+    if (done) *done = batch_done_state(c);
     return FV_OK;
 }
 

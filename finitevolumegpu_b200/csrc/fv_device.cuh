@@ -121,6 +121,99 @@ __device__ __forceinline__ float ffma(float a, float b, float c) {
     return d;
 }
 
+// ------------------------------------------------------------------ two lanes per thread
+
+// Two independent FP32 values, one from each of two lines a thread walks side
+// by side.  Add, subtract, multiply and FMA on a pair are one packed
+// round-to-nearest instruction (add/sub/mul/fma.rn.ftz.f32x2, sm_100), whose
+// lanes round exactly as the scalar instructions above do, so a pair holds the
+// same bits as two scalar computations.  Everything else (min/max, division,
+// square root, comparisons) runs lane by lane with the scalar operations.
+struct __align__(8) f2 {
+    float x, y;
+};
+
+__device__ __forceinline__ uint64_t& u64(f2& a) { return reinterpret_cast<uint64_t&>(a); }
+__device__ __forceinline__ const uint64_t& u64(const f2& a) { return reinterpret_cast<const uint64_t&>(a); }
+
+__device__ __forceinline__ f2 fadd(f2 a, f2 b) {
+    f2 d;
+    asm("add.rn.ftz.f32x2 %0, %1, %2;" : "=l"(u64(d)) : "l"(u64(a)), "l"(u64(b)));
+    return d;
+}
+__device__ __forceinline__ f2 fsub(f2 a, f2 b) {
+    f2 d;
+    asm("sub.rn.ftz.f32x2 %0, %1, %2;" : "=l"(u64(d)) : "l"(u64(a)), "l"(u64(b)));
+    return d;
+}
+__device__ __forceinline__ f2 fmul(f2 a, f2 b) {
+    f2 d;
+    asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(u64(d)) : "l"(u64(a)), "l"(u64(b)));
+    return d;
+}
+__device__ __forceinline__ f2 ffma(f2 a, f2 b, f2 c) {
+    f2 d;
+    asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(u64(d)) : "l"(u64(a)), "l"(u64(b)), "l"(u64(c)));
+    return d;
+}
+
+// A scalar constant in the number type of a computation (both lanes for f2).
+template <class N> __device__ __forceinline__ N splat(float a);
+template <> __device__ __forceinline__ float splat<float>(float a) { return a; }
+template <> __device__ __forceinline__ f2 splat<f2>(float a) { return f2{a, a}; }
+
+// Lane-wise operations, scalar or pair.
+__device__ __forceinline__ float vneg(float a) { return -a; }
+__device__ __forceinline__ f2 vneg(f2 a) { return f2{-a.x, -a.y}; }
+__device__ __forceinline__ float vdiv(float a, float b) { return a / b; }  // fast-math division
+__device__ __forceinline__ f2 vdiv(f2 a, f2 b) { return f2{a.x / b.x, a.y / b.y}; }
+__device__ __forceinline__ float vrcp(float a) { return 1.0f / a; }
+__device__ __forceinline__ f2 vrcp(f2 a) { return f2{1.0f / a.x, 1.0f / a.y}; }
+__device__ __forceinline__ float vsqrt(float a) { return sqrtf(a); }
+__device__ __forceinline__ f2 vsqrt(f2 a) { return f2{sqrtf(a.x), sqrtf(a.y)}; }
+__device__ __forceinline__ float vmin(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ f2 vmin(f2 a, f2 b) { return f2{fminf(a.x, b.x), fminf(a.y, b.y)}; }
+__device__ __forceinline__ float vmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ f2 vmax(f2 a, f2 b) { return f2{fmaxf(a.x, b.x), fmaxf(a.y, b.y)}; }
+
+// Three-input minimum (NaN-dropping) and maximum (NaN-propagating): one
+// instruction each on sm_100, and exactly min(min(a, b), c) and
+// max.NaN(max.NaN(a, b), c).
+__device__ __forceinline__ float vmin3(float a, float b, float c) {
+    float d;
+    asm("min.ftz.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+__device__ __forceinline__ float vmax3_nan(float a, float b, float c) {
+    float d;
+    asm("max.ftz.NaN.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+__device__ __forceinline__ float vmax3(float a, float b, float c) {
+    float d;
+    asm("max.ftz.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+__device__ __forceinline__ f2 vmin3(f2 a, f2 b, f2 c) { return f2{vmin3(a.x, b.x, c.x), vmin3(a.y, b.y, c.y)}; }
+__device__ __forceinline__ f2 vmax3_nan(f2 a, f2 b, f2 c) {
+    return f2{vmax3_nan(a.x, b.x, c.x), vmax3_nan(a.y, b.y, c.y)};
+}
+__device__ __forceinline__ f2 vmax3(f2 a, f2 b, f2 c) { return f2{vmax3(a.x, b.x, c.x), vmax3(a.y, b.y, c.y)}; }
+
+// Lane-wise selects: a > b ? t : f, and s >= 0 ? t : f, s <= 0 ? t : f.
+__device__ __forceinline__ float vsel_gt(float a, float b, float t, float f) { return (a > b) ? t : f; }
+__device__ __forceinline__ f2 vsel_gt(f2 a, f2 b, f2 t, f2 f) {
+    return f2{(a.x > b.x) ? t.x : f.x, (a.y > b.y) ? t.y : f.y};
+}
+__device__ __forceinline__ float vsel_ge0(float s, float t, float f) { return (s >= 0.0f) ? t : f; }
+__device__ __forceinline__ f2 vsel_ge0(f2 s, f2 t, f2 f) {
+    return f2{(s.x >= 0.0f) ? t.x : f.x, (s.y >= 0.0f) ? t.y : f.y};
+}
+__device__ __forceinline__ float vsel_le0(float s, float t, float f) { return (s <= 0.0f) ? t : f; }
+__device__ __forceinline__ f2 vsel_le0(f2 s, f2 t, f2 f) {
+    return f2{(s.x <= 0.0f) ? t.x : f.x, (s.y <= 0.0f) ? t.y : f.y};
+}
+
 // ------------------------------------------------------------------ limiters
 
 // Generalised minmod slope (GPUSimulators/cuda/limiters.h:31-41).  The
@@ -145,11 +238,14 @@ __device__ __forceinline__ float fmax_nan(float a, float b) {
     asm("max.NaN.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
     return r;
 }
+__device__ __forceinline__ float vmax_nan(float a, float b) { return fmax_nan(a, b); }
+__device__ __forceinline__ f2 vmax_nan(f2 a, f2 b) { return f2{fmax_nan(a.x, b.x), fmax_nan(a.y, b.y)}; }
 
-__device__ __forceinline__ float minmod3(float b, float c, float f) {
-    const float lo = fminf(fminf(b, c), f);
-    const float hi = fmax_nan(fmax_nan(b, c), f);
-    return fmax_nan(lo, fminf(hi, 0.0f));
+template <class N>
+__device__ __forceinline__ N minmod3(N b, N c, N f) {
+    const N lo = vmin3(b, c, f);
+    const N hi = vmax3_nan(b, c, f);
+    return vmax_nan(lo, vmin(hi, splat<N>(0.0f)));
 }
 
 __device__ __forceinline__ float minmod_slope(float left, float center, float right, float theta) {
@@ -196,59 +292,64 @@ __device__ __forceinline__ float desingularize(float x, float eps) {
 
 // A state at a cell face together with its physical flux
 // (GPUSimulators/cuda/SWECommon.h:29-37), velocity and gravity-wave speed.
-struct SweFace {
-    float q[3];
-    float f[3];
-    float u, c;
+// N is float, or f2 for two lines walked side by side.
+template <class N>
+struct SweFaceT {
+    N q[3];
+    N f[3];
+    N u, c;
 };
+using SweFace = SweFaceT<float>;
 
-__device__ __forceinline__ SweFace swe_face(float h, float hu, float hv, float g, float half_g) {
-    SweFace s;
+template <class N>
+__device__ __forceinline__ SweFaceT<N> swe_face(N h, N hu, N hv, N g, N half_g) {
+    SweFaceT<N> s;
     s.q[0] = h;
     s.q[1] = hu;
     s.q[2] = hv;
-    const float rh = 1.0f / h;
+    const N rh = vrcp(h);
     s.u = fmul(hu, rh);
     s.f[0] = hu;
     s.f[1] = ffma(hu, s.u, fmul(fmul(half_g, h), h));
     s.f[2] = fmul(hv, s.u);
-    s.c = sqrtf(fmul(g, h));
+    s.c = vsqrt(fmul(g, h));
     return s;
 }
 
 // Central-upwind flux (GPUSimulators/cuda/SWECommon.h:228-241); m is the left
 // (minus) state, p the right (plus) state.
-__device__ __forceinline__ void swe_central_upwind(const SweFace& m, const SweFace& p, float out[3]) {
-    const float am = fminf(fminf(fsub(m.u, m.c), fsub(p.u, p.c)), 0.0f);
-    const float ap = fmaxf(fmaxf(fadd(m.u, m.c), fadd(p.u, p.c)), 0.0f);
-    const float inv = 1.0f / fsub(ap, am);
-    const float apam = fmul(ap, am);
+template <class N>
+__device__ __forceinline__ void swe_central_upwind(const SweFaceT<N>& m, const SweFaceT<N>& p, N out[3]) {
+    const N am = vmin3(fsub(m.u, m.c), fsub(p.u, p.c), splat<N>(0.0f));
+    const N ap = vmax3(fadd(m.u, m.c), fadd(p.u, p.c), splat<N>(0.0f));
+    const N inv = vrcp(fsub(ap, am));
+    const N apam = fmul(ap, am);
+    const N nam = vneg(am);
 #pragma unroll
     for (int v = 0; v < 3; ++v)
-        out[v] = fmul(ffma(apam, fsub(p.q[v], m.q[v]), ffma(ap, m.f[v], fmul(-am, p.f[v]))), inv);
+        out[v] = fmul(ffma(apam, fsub(p.q[v], m.q[v]), ffma(ap, m.f[v], fmul(nam, p.f[v]))), inv);
 }
 
-// HLL flux (GPUSimulators/cuda/SWECommon.h:274-313).
-__device__ __forceinline__ void swe_hll(const SweFace& l, const SweFace& r, float out[3]) {
-    const float h_l = l.q[0], h_r = r.q[0];
-    const float hsum = fadd(h_l, h_r);
-    const float h_dag = fsub(fmul(0.5f, hsum), fmul(fmul(0.25f, fsub(r.u, l.u)), hsum) / fadd(l.c, r.c));
-    const float q_l = (h_dag > h_l) ? sqrtf(fmul(0.5f, fmul(fadd(h_dag, h_l), h_dag) / fmul(h_l, h_l))) : 1.0f;
-    const float q_r = (h_dag > h_r) ? sqrtf(fmul(0.5f, fmul(fadd(h_dag, h_r), h_dag) / fmul(h_r, h_r))) : 1.0f;
-    const float S_l = ffma(-l.c, q_l, l.u);
-    const float S_r = ffma(r.c, q_r, r.u);
-    if (S_l >= 0.0f) {
+// HLL flux (GPUSimulators/cuda/SWECommon.h:274-313).  The three cases (all
+// waves to the right, all to the left, the star region) are lane-wise
+// selects, so one formula serves scalars and pairs.
+template <class N>
+__device__ __forceinline__ void swe_hll(const SweFaceT<N>& l, const SweFaceT<N>& r, N out[3]) {
+    const N h_l = l.q[0], h_r = r.q[0];
+    const N one = splat<N>(1.0f), half = splat<N>(0.5f);
+    const N hsum = fadd(h_l, h_r);
+    const N h_dag = fsub(fmul(half, hsum), vdiv(fmul(fmul(splat<N>(0.25f), fsub(r.u, l.u)), hsum), fadd(l.c, r.c)));
+    const N q_l = vsel_gt(h_dag, h_l, vsqrt(fmul(half, vdiv(fmul(fadd(h_dag, h_l), h_dag), fmul(h_l, h_l)))), one);
+    const N q_r = vsel_gt(h_dag, h_r, vsqrt(fmul(half, vdiv(fmul(fadd(h_dag, h_r), h_dag), fmul(h_r, h_r)))), one);
+    const N S_l = ffma(vneg(l.c), q_l, l.u);
+    const N S_r = ffma(r.c, q_r, r.u);
+    const N inv = vrcp(fsub(S_r, S_l));
+    const N srsl = fmul(S_r, S_l);
+    const N nsl = vneg(S_l);
 #pragma unroll
-        for (int v = 0; v < 3; ++v) out[v] = l.f[v];
-    } else if (S_r <= 0.0f) {
-#pragma unroll
-        for (int v = 0; v < 3; ++v) out[v] = r.f[v];
-    } else {
-        const float inv = 1.0f / fsub(S_r, S_l);
-        const float srsl = fmul(S_r, S_l);
-#pragma unroll
-        for (int v = 0; v < 3; ++v)
-            out[v] = fmul(ffma(srsl, fsub(r.q[v], l.q[v]), ffma(S_r, l.f[v], fmul(-S_l, r.f[v]))), inv);
+    for (int v = 0; v < 3; ++v) {
+        const N star = fmul(ffma(srsl, fsub(r.q[v], l.q[v]), ffma(S_r, l.f[v], fmul(nsl, r.f[v]))), inv);
+        out[v] = vsel_ge0(S_l, l.f[v], vsel_le0(S_r, r.f[v], star));
     }
 }
 
@@ -266,87 +367,91 @@ __device__ __forceinline__ void swe_hll(const SweFace& l, const SweFace& r, floa
 // theta*f), since scaling by 2 commutes with rounding, and the face values
 // q0 -+ s2/4 equal q0 -+ s/2 bit for bit.  This saves the multiply of the
 // central difference.
-__device__ __forceinline__ void swe_muscl_hancock(const float (&qm)[3], const float (&q0)[3], const float (&qp)[3],
-                                                  float (&bd)[3], float theta2, float g, float half_g, float k2,
-                                                  SweFace& w, SweFace& e) {
-    float W[3], E[3];
+template <class N>
+__device__ __forceinline__ void swe_muscl_hancock(const N (&qm)[3], const N (&q0)[3], const N (&qp)[3], N (&bd)[3],
+                                                  N theta2, N g, N half_g, N k2, SweFaceT<N>& w, SweFaceT<N>& e) {
+    N W[3], E[3];
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
-        const float f = fmul(fsub(qp[v], q0[v]), theta2);
-        const float s2 = minmod3(bd[v], fsub(qp[v], qm[v]), f);
+        const N f = fmul(fsub(qp[v], q0[v]), theta2);
+        const N s2 = minmod3(bd[v], fsub(qp[v], qm[v]), f);
         bd[v] = f;
-        W[v] = ffma(-0.25f, s2, q0[v]);
-        E[v] = ffma(0.25f, s2, q0[v]);
+        W[v] = ffma(splat<N>(-0.25f), s2, q0[v]);
+        E[v] = ffma(splat<N>(0.25f), s2, q0[v]);
     }
-    const float uw = W[1] / W[0];
-    const float ue = E[1] / E[0];
-    float D[3];
+    const N uw = vdiv(W[1], W[0]);
+    const N ue = vdiv(E[1], E[0]);
+    N D[3];
     D[0] = fsub(W[1], E[1]);
     D[1] = fsub(ffma(W[1], uw, fmul(fmul(half_g, W[0]), W[0])), ffma(E[1], ue, fmul(fmul(half_g, E[0]), E[0])));
-    D[2] = ffma(W[2], uw, fmul(-E[2], ue));
+    D[2] = ffma(W[2], uw, fmul(vneg(E[2]), ue));
     w = swe_face(ffma(k2, D[0], W[0]), ffma(k2, D[1], W[1]), ffma(k2, D[2], W[2]), g, half_g);
     e = swe_face(ffma(k2, D[0], E[0]), ffma(k2, D[1], E[1]), ffma(k2, D[2], E[2]), g, half_g);
 }
 
 // ------------------------------------------------------------------ Euler
 
-struct EulerFace {
-    float q[4];
-    float f[4];
-    float u, c;
+template <class N>
+struct EulerFaceT {
+    N q[4];
+    N f[4];
+    N u, c;
 };
+using EulerFace = EulerFaceT<float>;
 
 // Face state with pressure (GPUSimulators/cuda/EulerCommon.h:83-90), flux
 // (EulerCommon.h:93-109) and sound speed sqrt(gamma*P/rho) (EulerCommon.h:130-131, :176).
-__device__ __forceinline__ EulerFace euler_face(float rho, float ru, float rv, float E, float gamma) {
-    EulerFace s;
+// gm1 = gamma - 1.
+template <class N>
+__device__ __forceinline__ EulerFaceT<N> euler_face(N rho, N ru, N rv, N E, N gamma, N gm1) {
+    EulerFaceT<N> s;
     s.q[0] = rho;
     s.q[1] = ru;
     s.q[2] = rv;
     s.q[3] = E;
-    const float rr = 1.0f / rho;
-    const float P = fmul(gamma - 1.0f, ffma(fmul(-0.5f, ffma(ru, ru, fmul(rv, rv))), rr, E));
+    const N rr = vrcp(rho);
+    const N P = fmul(gm1, ffma(fmul(splat<N>(-0.5f), ffma(ru, ru, fmul(rv, rv))), rr, E));
     s.u = fmul(ru, rr);
     s.f[0] = ru;
     s.f[1] = ffma(ru, s.u, P);
     s.f[2] = fmul(rv, s.u);
     s.f[3] = fmul(s.u, fadd(E, P));
-    s.c = sqrtf(fmul(fmul(gamma, P), rr));
+    s.c = vsqrt(fmul(fmul(gamma, P), rr));
     return s;
 }
 
 // GPUSimulators/cuda/EulerCommon.h:171-187
-__device__ __forceinline__ void euler_central_upwind(const EulerFace& m, const EulerFace& p, float out[4]) {
-    const float am = fminf(fminf(fsub(m.u, m.c), fsub(p.u, p.c)), 0.0f);
-    const float ap = fmaxf(fmaxf(fadd(m.u, m.c), fadd(p.u, p.c)), 0.0f);
-    const float inv = 1.0f / fsub(ap, am);
-    const float apam = fmul(ap, am);
+template <class N>
+__device__ __forceinline__ void euler_central_upwind(const EulerFaceT<N>& m, const EulerFaceT<N>& p, N out[4]) {
+    const N am = vmin3(fsub(m.u, m.c), fsub(p.u, p.c), splat<N>(0.0f));
+    const N ap = vmax3(fadd(m.u, m.c), fadd(p.u, p.c), splat<N>(0.0f));
+    const N inv = vrcp(fsub(ap, am));
+    const N apam = fmul(ap, am);
+    const N nam = vneg(am);
 #pragma unroll
     for (int v = 0; v < 4; ++v)
-        out[v] = fmul(ffma(apam, fsub(p.q[v], m.q[v]), ffma(ap, m.f[v], fmul(-am, p.f[v]))), inv);
+        out[v] = fmul(ffma(apam, fsub(p.q[v], m.q[v]), ffma(ap, m.f[v], fmul(nam, p.f[v]))), inv);
 }
 
-// GPUSimulators/cuda/EulerCommon.h:117-160
-__device__ __forceinline__ void euler_hll(const EulerFace& l, const EulerFace& r, float out[4]) {
-    const float h_l = l.q[0], h_r = r.q[0];
-    const float hsum = fadd(h_l, h_r);
-    const float h_dag = fsub(fmul(0.5f, hsum), fmul(fmul(0.25f, fsub(r.u, l.u)), hsum) / fadd(l.c, r.c));
-    const float q_l = (h_dag > h_l) ? sqrtf(fmul(0.5f, fmul(fadd(h_dag, h_l), h_dag) / fmul(h_l, h_l))) : 1.0f;
-    const float q_r = (h_dag > h_r) ? sqrtf(fmul(0.5f, fmul(fadd(h_dag, h_r), h_dag) / fmul(h_r, h_r))) : 1.0f;
-    const float S_l = ffma(-l.c, q_l, l.u);
-    const float S_r = ffma(r.c, q_r, r.u);
-    if (S_l >= 0.0f) {
+// GPUSimulators/cuda/EulerCommon.h:117-160; the cases are lane-wise selects
+// as in swe_hll.
+template <class N>
+__device__ __forceinline__ void euler_hll(const EulerFaceT<N>& l, const EulerFaceT<N>& r, N out[4]) {
+    const N h_l = l.q[0], h_r = r.q[0];
+    const N one = splat<N>(1.0f), half = splat<N>(0.5f);
+    const N hsum = fadd(h_l, h_r);
+    const N h_dag = fsub(fmul(half, hsum), vdiv(fmul(fmul(splat<N>(0.25f), fsub(r.u, l.u)), hsum), fadd(l.c, r.c)));
+    const N q_l = vsel_gt(h_dag, h_l, vsqrt(fmul(half, vdiv(fmul(fadd(h_dag, h_l), h_dag), fmul(h_l, h_l)))), one);
+    const N q_r = vsel_gt(h_dag, h_r, vsqrt(fmul(half, vdiv(fmul(fadd(h_dag, h_r), h_dag), fmul(h_r, h_r)))), one);
+    const N S_l = ffma(vneg(l.c), q_l, l.u);
+    const N S_r = ffma(r.c, q_r, r.u);
+    const N inv = vrcp(fsub(S_r, S_l));
+    const N srsl = fmul(S_r, S_l);
+    const N nsl = vneg(S_l);
 #pragma unroll
-        for (int v = 0; v < 4; ++v) out[v] = l.f[v];
-    } else if (S_r <= 0.0f) {
-#pragma unroll
-        for (int v = 0; v < 4; ++v) out[v] = r.f[v];
-    } else {
-        const float inv = 1.0f / fsub(S_r, S_l);
-        const float srsl = fmul(S_r, S_l);
-#pragma unroll
-        for (int v = 0; v < 4; ++v)
-            out[v] = fmul(ffma(srsl, fsub(r.q[v], l.q[v]), ffma(S_r, l.f[v], fmul(-S_l, r.f[v]))), inv);
+    for (int v = 0; v < 4; ++v) {
+        const N star = fmul(ffma(srsl, fsub(r.q[v], l.q[v]), ffma(S_r, l.f[v], fmul(nsl, r.f[v]))), inv);
+        out[v] = vsel_ge0(S_l, l.f[v], vsel_le0(S_r, r.f[v], star));
     }
 }
 
@@ -356,27 +461,28 @@ __device__ __forceinline__ void euler_hll(const EulerFace& l, const EulerFace& r
 // the predictor flux uses gamma in place of P; that is reproduced here.
 // bd: theta2*(q0 - qm) on entry, theta2*(qp - q0) on return, theta2 = 2*theta,
 // and the slope at twice its size (as in swe_muscl_hancock).
-__device__ __forceinline__ void euler_muscl_hancock(const float (&qm)[4], const float (&q0)[4], const float (&qp)[4],
-                                                    float (&bd)[4], float theta2, float gamma, float k2, EulerFace& w,
-                                                    EulerFace& e) {
-    float W[4], E[4];
+template <class N>
+__device__ __forceinline__ void euler_muscl_hancock(const N (&qm)[4], const N (&q0)[4], const N (&qp)[4], N (&bd)[4],
+                                                    N theta2, N gamma, N gm1, N k2, EulerFaceT<N>& w,
+                                                    EulerFaceT<N>& e) {
+    N W[4], E[4];
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-        const float f = fmul(fsub(qp[v], q0[v]), theta2);
-        const float s2 = minmod3(bd[v], fsub(qp[v], qm[v]), f);
+        const N f = fmul(fsub(qp[v], q0[v]), theta2);
+        const N s2 = minmod3(bd[v], fsub(qp[v], qm[v]), f);
         bd[v] = f;
-        W[v] = ffma(-0.25f, s2, q0[v]);
-        E[v] = ffma(0.25f, s2, q0[v]);
+        W[v] = ffma(splat<N>(-0.25f), s2, q0[v]);
+        E[v] = ffma(splat<N>(0.25f), s2, q0[v]);
     }
-    const float uw = W[1] / W[0];
-    const float ue = E[1] / E[0];
-    float D[4];
+    const N uw = vdiv(W[1], W[0]);
+    const N ue = vdiv(E[1], E[0]);
+    N D[4];
     D[0] = fsub(W[1], E[1]);
     D[1] = fsub(ffma(W[1], uw, gamma), ffma(E[1], ue, gamma));
-    D[2] = ffma(W[2], uw, fmul(-E[2], ue));
-    D[3] = ffma(uw, fadd(W[3], gamma), fmul(-ue, fadd(E[3], gamma)));
-    w = euler_face(ffma(k2, D[0], W[0]), ffma(k2, D[1], W[1]), ffma(k2, D[2], W[2]), ffma(k2, D[3], W[3]), gamma);
-    e = euler_face(ffma(k2, D[0], E[0]), ffma(k2, D[1], E[1]), ffma(k2, D[2], E[2]), ffma(k2, D[3], E[3]), gamma);
+    D[2] = ffma(W[2], uw, fmul(vneg(E[2]), ue));
+    D[3] = ffma(uw, fadd(W[3], gamma), fmul(vneg(ue), fadd(E[3], gamma)));
+    w = euler_face(ffma(k2, D[0], W[0]), ffma(k2, D[1], W[1]), ffma(k2, D[2], W[2]), ffma(k2, D[3], W[3]), gamma, gm1);
+    e = euler_face(ffma(k2, D[0], E[0]), ffma(k2, D[1], E[1]), ffma(k2, D[2], E[2]), ffma(k2, D[3], E[3]), gamma, gm1);
 }
 
 // ------------------------------------------------------------------ WAF

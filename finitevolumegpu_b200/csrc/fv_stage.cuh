@@ -51,6 +51,8 @@ struct alignas(16) SimCtl {
     unsigned int arrive;  // CTA arrival counter for the last-CTA epilogue
     int error;         // nonzero once a bounded wait gave up
     double sums[4];    // FP64 sums of the interior of u0 after the last step that asked for them
+    int bad;           // batched simulations: a step left a non-finite value or a non-positive depth
+                       // (density); the simulation then stops (t_end is set to t)
 };
 
 // Launch arguments (passed as a __grid_constant__ parameter; the tensor maps
@@ -235,6 +237,7 @@ __device__ void tile_epilogue(SimCtl* ctl, float* block_cfl, double* block_sums,
             c->t = s.t_new;
             c->nt = c->nt + 1;
             if (!explicit_dt && c->update_dt && (c->nt % 100 == 0)) c->dt = (c->cfl_min * c->factor) * c->cfl_scale;
+            if (c->bad) c->t_end = c->t;  // a failed simulation takes no further steps
         }
         c->arrive = 0u;
         __threadfence();
@@ -404,30 +407,64 @@ __device__ __forceinline__ void st_cell(float* line, int k, int step, const floa
     for (int v = 0; v < NV; ++v) p[vslot<SWAP>(v) * PS] = q[v];
 }
 
-// Physics policies for the MUSCL-Hancock walker.
+// Two lines walked side by side: the second line starts d2 floats after the
+// first; lane x of a pair is the first line, lane y the second.
+template <int NV, bool SWAP, int PS>
+__device__ __forceinline__ void ld_cell(const float* line, int k, int step, int d2, f2 (&q)[NV]) {
+    const float* p = line + k * step;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) q[v] = f2{p[vslot<SWAP>(v) * PS], p[vslot<SWAP>(v) * PS + d2]};
+}
+
+template <int NV, bool SWAP, int PS>
+__device__ __forceinline__ void st_cell(float* line, int k, int step, int d2, const f2 (&q)[NV]) {
+    float* p = line + k * step;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        p[vslot<SWAP>(v) * PS] = q[v].x;
+        p[vslot<SWAP>(v) * PS + d2] = q[v].y;
+    }
+}
+
+template <int NV, bool SWAP, int PS>
+__device__ __forceinline__ void ld_cell(const float* line, int k, int step, int, float (&q)[NV]) {
+    ld_cell<NV, SWAP, PS>(line, k, step, q);
+}
+
+template <int NV, bool SWAP, int PS>
+__device__ __forceinline__ void st_cell(float* line, int k, int step, int, const float (&q)[NV]) {
+    st_cell<NV, SWAP, PS>(line, k, step, q);
+}
+
+// Physics policies for the MUSCL-Hancock walker; N is float (one line per
+// thread) or f2 (two lines per thread).
+template <class N>
 struct SwePhys {
     static constexpr int NV = 3;
-    using Face = SweFace;
-    float theta2, g, half_g, k2;  // theta2 = 2 * theta (swe_muscl_hancock)
-    __device__ __forceinline__ void recon(const float (&qm)[3], const float (&q0)[3], const float (&qp)[3],
-                                          float (&bd)[3], Face& w, Face& e) const {
+    using Num = N;
+    using Face = SweFaceT<N>;
+    N theta2, g, half_g, k2;  // theta2 = 2 * theta (swe_muscl_hancock)
+    __device__ __forceinline__ void recon(const N (&qm)[3], const N (&q0)[3], const N (&qp)[3], N (&bd)[3], Face& w,
+                                          Face& e) const {
         swe_muscl_hancock(qm, q0, qp, bd, theta2, g, half_g, k2, w, e);
     }
-    template <bool HLLF> __device__ __forceinline__ static void flux(const Face& l, const Face& r, float (&F)[3]) {
+    template <bool HLLF> __device__ __forceinline__ static void flux(const Face& l, const Face& r, N (&F)[3]) {
         if (HLLF) swe_hll(l, r, F);
         else swe_central_upwind(l, r, F);
     }
 };
 
+template <class N>
 struct EulerPhys {
     static constexpr int NV = 4;
-    using Face = EulerFace;
-    float theta2, gamma, k2;  // theta2 = 2 * theta
-    __device__ __forceinline__ void recon(const float (&qm)[4], const float (&q0)[4], const float (&qp)[4],
-                                          float (&bd)[4], Face& w, Face& e) const {
-        euler_muscl_hancock(qm, q0, qp, bd, theta2, gamma, k2, w, e);
+    using Num = N;
+    using Face = EulerFaceT<N>;
+    N theta2, gamma, gm1, k2;  // theta2 = 2 * theta, gm1 = gamma - 1
+    __device__ __forceinline__ void recon(const N (&qm)[4], const N (&q0)[4], const N (&qp)[4], N (&bd)[4], Face& w,
+                                          Face& e) const {
+        euler_muscl_hancock(qm, q0, qp, bd, theta2, gamma, gm1, k2, w, e);
     }
-    template <bool HLLF> __device__ __forceinline__ static void flux(const Face& l, const Face& r, float (&F)[4]) {
+    template <bool HLLF> __device__ __forceinline__ static void flux(const Face& l, const Face& r, N (&F)[4]) {
         if (HLLF) euler_hll(l, r, F);
         else euler_central_upwind(l, r, F);
     }
@@ -435,11 +472,11 @@ struct EulerPhys {
 
 // One MUSCL-Hancock window step at cell c: shift in Q[c+1], reconstruct c,
 // flux at c-1/2, update cell c-1 (GPUSimulators/cuda/common.h:444-475).
-template <class Phys, bool HLLF, bool SWAP, int PS>
-__device__ __forceinline__ void mh_step(float* line, int step, int c, float (&qm)[Phys::NV], float (&q0)[Phys::NV],
-                                        float (&qp)[Phys::NV], const float (&qn)[Phys::NV], float (&bd)[Phys::NV],
-                                        typename Phys::Face& eL, float (&Fprev)[Phys::NV], const Phys& P,
-                                        float kdx, bool update) {
+template <class Phys, bool HLLF, bool SWAP, int PS, class N = typename Phys::Num>
+__device__ __forceinline__ void mh_step(float* line, int step, int d2, int c, N (&qm)[Phys::NV], N (&q0)[Phys::NV],
+                                        N (&qp)[Phys::NV], const N (&qn)[Phys::NV], N (&bd)[Phys::NV],
+                                        typename Phys::Face& eL, N (&Fprev)[Phys::NV], const Phys& P, N kdx,
+                                        bool update) {
     constexpr int NV = Phys::NV;
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
@@ -449,34 +486,35 @@ __device__ __forceinline__ void mh_step(float* line, int step, int c, float (&qm
     }
     typename Phys::Face w, e;
     P.recon(qm, q0, qp, bd, w, e);
-    float F[NV];
+    N F[NV];
     Phys::template flux<HLLF>(eL, w, F);
     if (update) {
-        float out[NV];
+        N out[NV];
 #pragma unroll
         for (int v = 0; v < NV; ++v) out[v] = ffma(fsub(Fprev[v], F[v]), kdx, qm[v]);
-        st_cell<NV, SWAP, PS>(line, c - 1, step, out);
+        st_cell<NV, SWAP, PS>(line, c - 1, step, d2, out);
     }
 #pragma unroll
     for (int v = 0; v < NV; ++v) Fprev[v] = F[v];
     eL = e;
 }
 
-// Updates cells [a, b) of a line in place.  pre holds Q[a-2], Q[a-1], Q[b], Q[b+1].
-template <class Phys, bool HLLF, bool SWAP, int PS>
-__device__ __forceinline__ void walk_mh(float* line, int step, int a, int b, const float (&pre)[4][Phys::NV],
-                                        const Phys& P, float kdx) {
+// Updates cells [a, b) of a line (of two lines, d2 floats apart, for f2) in
+// place.  pre holds Q[a-2], Q[a-1], Q[b], Q[b+1].
+template <class Phys, bool HLLF, bool SWAP, int PS, class N = typename Phys::Num>
+__device__ __forceinline__ void walk_mh(float* line, int step, int d2, int a, int b, const N (&pre)[4][Phys::NV],
+                                        const Phys& P, N kdx) {
     constexpr int NV = Phys::NV;
-    float qm[NV], q0[NV], qp[NV], qn[NV], Fprev[NV], bd[NV];
+    N qm[NV], q0[NV], qp[NV], qn[NV], Fprev[NV], bd[NV];
     typename Phys::Face eL;
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
         q0[v] = pre[0][v];
         qp[v] = pre[1][v];
-        Fprev[v] = 0.0f;
+        Fprev[v] = splat<N>(0.0f);
     }
     // c = a-1: reconstruct only
-    ld_cell<NV, SWAP, PS>(line, a, step, qn);
+    ld_cell<NV, SWAP, PS>(line, a, step, d2, qn);
     {
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
@@ -489,17 +527,17 @@ __device__ __forceinline__ void walk_mh(float* line, int step, int a, int b, con
         P.recon(qm, q0, qp, bd, w, eL);
     }
     // c = a: first face, no update
-    ld_cell<NV, SWAP, PS>(line, a + 1, step, qn);
-    mh_step<Phys, HLLF, SWAP, PS>(line, step, a, qm, q0, qp, qn, bd, eL, Fprev, P, kdx, false);
+    ld_cell<NV, SWAP, PS>(line, a + 1, step, d2, qn);
+    mh_step<Phys, HLLF, SWAP, PS>(line, step, d2, a, qm, q0, qp, qn, bd, eL, Fprev, P, kdx, false);
     // unrolled by the window's length, so the rotation of the three-cell
     // window becomes register renaming instead of moves
 #pragma unroll 3
     for (int c = a + 1; c < b - 1; ++c) {
-        ld_cell<NV, SWAP, PS>(line, c + 1, step, qn);
-        mh_step<Phys, HLLF, SWAP, PS>(line, step, c, qm, q0, qp, qn, bd, eL, Fprev, P, kdx, true);
+        ld_cell<NV, SWAP, PS>(line, c + 1, step, d2, qn);
+        mh_step<Phys, HLLF, SWAP, PS>(line, step, d2, c, qm, q0, qp, qn, bd, eL, Fprev, P, kdx, true);
     }
-    mh_step<Phys, HLLF, SWAP, PS>(line, step, b - 1, qm, q0, qp, pre[2], bd, eL, Fprev, P, kdx, true);
-    mh_step<Phys, HLLF, SWAP, PS>(line, step, b, qm, q0, qp, pre[3], bd, eL, Fprev, P, kdx, true);
+    mh_step<Phys, HLLF, SWAP, PS>(line, step, d2, b - 1, qm, q0, qp, pre[2], bd, eL, Fprev, P, kdx, true);
+    mh_step<Phys, HLLF, SWAP, PS>(line, step, d2, b, qm, q0, qp, pre[3], bd, eL, Fprev, P, kdx, true);
 }
 
 // Two-point flux walker (FORCE, HLL: GPUSimulators/cuda/SWE2D_FORCE.cu:29-81,
@@ -607,12 +645,12 @@ __device__ __forceinline__ void walk_line(float* line, int step, int a, int b, c
                                           const SweepPar& p) {
     const float kdx = p.kdt / p.dxx;
     if constexpr (SCHEME == KP07_DIMSPLIT || SCHEME == HLL2) {
-        const SwePhys P{2.0f * p.theta, p.g, p.half_g, p.kdt / (2.0f * p.dxx)};
-        walk_mh<SwePhys, SCHEME == HLL2, SWAP, PS>(line, step, a, b, pre, P, kdx);
+        const SwePhys<float> P{2.0f * p.theta, p.g, p.half_g, p.kdt / (2.0f * p.dxx)};
+        walk_mh<SwePhys<float>, SCHEME == HLL2, SWAP, PS>(line, step, 0, a, b, pre, P, kdx);
     } else if constexpr (SCHEME == EE2D) {
-        const EulerPhys P{2.0f * p.theta, p.gamma, p.kdt / (2.0f * p.dxx)};
+        const EulerPhys<float> P{2.0f * p.theta, p.gamma, p.gamma - 1.0f, p.kdt / (2.0f * p.dxx)};
         // x sweeps use HLL, y sweeps central-upwind (GPUSimulators/cuda/EE2D_KP07_dimsplit.cu:62, :106)
-        walk_mh<EulerPhys, !SWAP, SWAP, PS>(line, step, a, b, pre, P, kdx);
+        walk_mh<EulerPhys<float>, !SWAP, SWAP, PS>(line, step, 0, a, b, pre, P, kdx);
     } else if constexpr (SCHEME == WAF) {
         walk_waf<SWAP, PS, VAR>(line, step, a, b, pre, p.g, p.half_g, p.inv_g, kdx, kdx, p.beta);
     } else {
@@ -621,47 +659,94 @@ __device__ __forceinline__ void walk_line(float* line, int step, int a, int b, c
     }
 }
 
+// Two lines, d2 floats apart, walked side by side in packed arithmetic
+// (the MUSCL-Hancock schemes).  Each cell gets the same bits as walk_line.
+template <int SCHEME, bool SWAP, int PS>
+__device__ __forceinline__ void walk_line2(float* line, int step, int d2, int a, int b,
+                                           const f2 (&pre)[4][(SCHEME == EE2D) ? 4 : 3], const SweepPar& p) {
+    static_assert(SCHEME == KP07_DIMSPLIT || SCHEME == HLL2 || SCHEME == EE2D, "packed walkers: MUSCL-Hancock only");
+    const f2 kdx = splat<f2>(p.kdt / p.dxx);
+    if constexpr (SCHEME == EE2D) {
+        const EulerPhys<f2> P{splat<f2>(2.0f * p.theta), splat<f2>(p.gamma), splat<f2>(p.gamma - 1.0f),
+                              splat<f2>(p.kdt / (2.0f * p.dxx))};
+        walk_mh<EulerPhys<f2>, !SWAP, SWAP, PS>(line, step, d2, a, b, pre, P, kdx);
+    } else {
+        const SwePhys<f2> P{splat<f2>(2.0f * p.theta), splat<f2>(p.g), splat<f2>(p.half_g),
+                            splat<f2>(p.kdt / (2.0f * p.dxx))};
+        walk_mh<SwePhys<f2>, SCHEME == HLL2, SWAP, PS>(line, step, d2, a, b, pre, P, kdx);
+    }
+}
+
 // x sweep over tile rows [t0, t1): interior columns updated in place.
-template <int SCHEME, int NV, int W, int H, int NT, int VAR>
+// LPT = 2: a thread walks rows t and t + (t1 - t0)/2 side by side.
+template <int SCHEME, int NV, int W, int H, int NT, int VAR, int LPT>
 __device__ __forceinline__ void sweep_x(float* Qs, int t0, int t1, const SweepPar& p) {
     constexpr int SP = W + 8, PS = SP * (H + 4), NSEG = 4, R = W / NSEG;
     const int item = threadIdx.x;
-    const bool has = item < (t1 - t0) * NSEG;
+    const int nlines = (t1 - t0) / LPT;
+    const bool has = item < nlines * NSEG;
     const int t = t0 + item / NSEG, seg = item % NSEG;
     const int a = 4 + seg * R, b = a + R;
     float* line = Qs + t * SP;
-    float pre[4][NV];
-    if (has) {
-        ld_cell<NV, false, PS>(line, a - 2, 1, pre[0]);
-        ld_cell<NV, false, PS>(line, a - 1, 1, pre[1]);
-        ld_cell<NV, false, PS>(line, b, 1, pre[2]);
-        ld_cell<NV, false, PS>(line, b + 1, 1, pre[3]);
+    if constexpr (LPT == 1) {
+        float pre[4][NV];
+        if (has) {
+            ld_cell<NV, false, PS>(line, a - 2, 1, pre[0]);
+            ld_cell<NV, false, PS>(line, a - 1, 1, pre[1]);
+            ld_cell<NV, false, PS>(line, b, 1, pre[2]);
+            ld_cell<NV, false, PS>(line, b + 1, 1, pre[3]);
+        }
+        __syncthreads();
+        if (has) walk_line<SCHEME, false, PS, VAR>(line, 1, a, b, pre, p);
+    } else {
+        const int d2 = nlines * SP;
+        f2 pre[4][NV];
+        if (has) {
+            ld_cell<NV, false, PS>(line, a - 2, 1, d2, pre[0]);
+            ld_cell<NV, false, PS>(line, a - 1, 1, d2, pre[1]);
+            ld_cell<NV, false, PS>(line, b, 1, d2, pre[2]);
+            ld_cell<NV, false, PS>(line, b + 1, 1, d2, pre[3]);
+        }
+        __syncthreads();
+        if (has) walk_line2<SCHEME, false, PS>(line, 1, d2, a, b, pre, p);
     }
-    __syncthreads();
-    if (has) walk_line<SCHEME, false, PS, VAR>(line, 1, a, b, pre, p);
     __syncthreads();
 }
 
 // y sweep over tile columns [s0, s1): interior rows updated in place.
-template <int SCHEME, int NV, int W, int H, int NT, int VAR>
+// LPT = 2: a thread walks columns s and s + (s1 - s0)/2 side by side.
+template <int SCHEME, int NV, int W, int H, int NT, int VAR, int LPT>
 __device__ __forceinline__ void sweep_y(float* Qs, int s0, int s1, const SweepPar& p) {
     constexpr int SP = W + 8, PS = SP * (H + 4);
-    constexpr int NSEG = NT / (W + 4), R = H / NSEG;
-    const int ncols = s1 - s0;
+    constexpr int NSEG = NT * LPT / (W + 4), R = H / NSEG;
+    const int ncols = (s1 - s0) / LPT;
     const int item = threadIdx.x;
     const bool has = item < ncols * NSEG;
     const int s = s0 + item % ncols, seg = item / ncols;
     const int a = 2 + seg * R, b = a + R;
     float* line = Qs + s;
-    float pre[4][NV];
-    if (has) {
-        ld_cell<NV, true, PS>(line, a - 2, SP, pre[0]);
-        ld_cell<NV, true, PS>(line, a - 1, SP, pre[1]);
-        ld_cell<NV, true, PS>(line, b, SP, pre[2]);
-        ld_cell<NV, true, PS>(line, b + 1, SP, pre[3]);
+    if constexpr (LPT == 1) {
+        float pre[4][NV];
+        if (has) {
+            ld_cell<NV, true, PS>(line, a - 2, SP, pre[0]);
+            ld_cell<NV, true, PS>(line, a - 1, SP, pre[1]);
+            ld_cell<NV, true, PS>(line, b, SP, pre[2]);
+            ld_cell<NV, true, PS>(line, b + 1, SP, pre[3]);
+        }
+        __syncthreads();
+        if (has) walk_line<SCHEME, true, PS, VAR>(line, SP, a, b, pre, p);
+    } else {
+        const int d2 = ncols;
+        f2 pre[4][NV];
+        if (has) {
+            ld_cell<NV, true, PS>(line, a - 2, SP, d2, pre[0]);
+            ld_cell<NV, true, PS>(line, a - 1, SP, d2, pre[1]);
+            ld_cell<NV, true, PS>(line, b, SP, d2, pre[2]);
+            ld_cell<NV, true, PS>(line, b + 1, SP, d2, pre[3]);
+        }
+        __syncthreads();
+        if (has) walk_line2<SCHEME, true, PS>(line, SP, d2, a, b, pre, p);
     }
-    __syncthreads();
-    if (has) walk_line<SCHEME, true, PS, VAR>(line, SP, a, b, pre, p);
     __syncthreads();
 }
 
@@ -679,16 +764,21 @@ struct SplitPar {
 // (FORCE, HLL, HLL2, WAF, KP07_dimsplit, EE2D).  Accumulates the tile's CFL
 // minimum and FP64 sums into the per-thread values.  Returns false if the tile
 // load gave up (nothing was written).
-template <int SCHEME, int W, int H, int NT, bool GLOBAL_TMAP = false, int VAR = 0>
+// HEALTH (batched kernels): with `health` set, *unhealthy becomes true if any
+// written cell holds a non-finite value or a non-positive depth (density).
+template <int SCHEME, int W, int H, int NT, bool GLOBAL_TMAP = false, int VAR = 0, int LPT = 1, bool HEALTH = false>
 __device__ bool process_tile_dimsplit(float* Qs, uint64_t* bar, uint32_t phase, bool init_bar, const TileJob& J,
                                       const SplitPar& P, bool do_cfl, bool sums, int* err, float& my_cfl,
-                                      double (&my_sums)[(SCHEME == EE2D) ? 4 : 3], uint32_t polls = kWaitPolls) {
+                                      double (&my_sums)[(SCHEME == EE2D) ? 4 : 3], uint32_t polls = kWaitPolls,
+                                      bool health = false, bool* unhealthy = nullptr) {
     constexpr int NV = (SCHEME == EE2D) ? 4 : 3;
     constexpr int G = (SCHEME == FORCE || SCHEME == HLL) ? 1 : 2;
     constexpr int SP = W + 8, TR = H + 4, PS = SP * TR;
     static_assert(W % 4 == 0 && (W / 4) % 2 == 1, "row segments must be odd for conflict-free x sweeps");
-    static_assert(TR * 4 <= NT, "one x-sweep segment per thread");
-    static_assert(NT % (W + 4) == 0 && H % (NT / (W + 4)) == 0, "y-sweep segments must tile the block");
+    static_assert(TR * 4 <= NT * LPT, "one x-sweep segment (LPT lines) per thread");
+    static_assert((NT * LPT) % (W + 4) == 0 && H % ((NT * LPT) / (W + 4)) == 0, "y-sweep segments must tile the block");
+    static_assert(LPT == 1 || (LPT == 2 && H % 2 == 0 && (SCHEME == KP07_DIMSPLIT || SCHEME == HLL2 || SCHEME == EE2D)),
+                  "two lines per thread: MUSCL-Hancock schemes with an even number of tile rows");
     if (!load_tile<NV, SP, TR, GLOBAL_TMAP>(Qs, J.tmap, J.x0, J.y0, bar, phase, init_bar, err, polls)) return false;
     const int x0 = J.x0, y0 = J.y0;
     if (x0 == 0 || x0 + W + 2 > J.nx || y0 == 0 || y0 + H + 2 > J.ny) apply_boundary<NV, W, H, NT>(Qs, J);
@@ -704,14 +794,14 @@ __device__ bool process_tile_dimsplit(float* Qs, uint64_t* bar, uint32_t phase, 
     const bool x_first = (SCHEME == FORCE || SCHEME == HLL) ? true : (P.substep == 0);
     if (x_first) {
         p.dxx = P.dx;
-        sweep_x<SCHEME, NV, W, H, NT, VAR>(Qs, 2 - G, H + 2 + G, p);
+        sweep_x<SCHEME, NV, W, H, NT, VAR, LPT>(Qs, 2 - G, H + 2 + G, p);
         p.dxx = P.dy;
-        sweep_y<SCHEME, NV, W, H, NT, VAR>(Qs, 4, W + 4, p);
+        sweep_y<SCHEME, NV, W, H, NT, VAR, LPT>(Qs, 4, W + 4, p);
     } else {
         p.dxx = P.dy;
-        sweep_y<SCHEME, NV, W, H, NT, VAR>(Qs, 4 - G, W + 4 + G, p);
+        sweep_y<SCHEME, NV, W, H, NT, VAR, LPT>(Qs, 4 - G, W + 4 + G, p);
         p.dxx = P.dx;
-        sweep_x<SCHEME, NV, W, H, NT, VAR>(Qs, 2, H + 2, p);
+        sweep_x<SCHEME, NV, W, H, NT, VAR, LPT>(Qs, 2, H + 2, p);
     }
 
     // copy-out of the interior (+ gravity source, CFL, sums)
@@ -751,6 +841,20 @@ __device__ bool process_tile_dimsplit(float* Qs, uint64_t* bar, uint32_t phase, 
                 for (int j = 0; j < nvalid; ++j) J.out[v][gi + j] = e[j];
             }
         }
+        if constexpr (HEALTH) {
+            if (health) {
+                bool bad = false;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    if (j < nvalid) {
+                        bad |= !((&val[0].x)[j] > 0.0f);
+#pragma unroll
+                        for (int v = 1; v < NV; ++v) bad |= !(fabsf((&val[v].x)[j]) < __int_as_float(0x7f800000));
+                    }
+                }
+                if (bad) *unhealthy = true;
+            }
+        }
         if (do_cfl || sums) {
             const float* h = &val[0].x;
             const float* hu = &val[1].x;
@@ -770,7 +874,7 @@ __device__ bool process_tile_dimsplit(float* Qs, uint64_t* bar, uint32_t phase, 
     return true;
 }
 
-template <int SCHEME, int W, int H, int NT, int VAR = 0>
+template <int SCHEME, int W, int H, int NT, int VAR = 0, int LPT = 1>
 __global__ void __launch_bounds__(NT) dimsplit_stage_kernel(const __grid_constant__ StageArgs A) {
     constexpr int NV = (SCHEME == EE2D) ? 4 : 3;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -798,8 +902,8 @@ __global__ void __launch_bounds__(NT) dimsplit_stage_kernel(const __grid_constan
     J.x0 = blockIdx.x * W;
     J.y0 = (blockIdx.y + A.tile_row0) * H;
     SplitPar P{A.dx, A.dy, A.g, A.gamma, A.theta, sc.dt * A.dt_scale, A.substep, A.variant_beta};
-    process_tile_dimsplit<SCHEME, W, H, NT, false, VAR>(Qs, &bar, 0, true, J, P, sc.do_cfl, sums, &A.ctl->error, my_cfl,
-                                                        my_sums, wait_polls(A.wait_limit));
+    process_tile_dimsplit<SCHEME, W, H, NT, false, VAR, LPT>(Qs, &bar, 0, true, J, P, sc.do_cfl, sums, &A.ctl->error,
+                                                             my_cfl, my_sums, wait_polls(A.wait_limit));
     stage_epilogue<NT, NV>(A, sc, my_cfl, my_sums, sums);
 }
 
@@ -835,7 +939,7 @@ struct BatchArgs {
 // control block exactly as the single-simulation kernel does.  Simulations
 // that reached t_end are skipped.  The work list lives in device memory, so
 // one captured CUDA graph serves any batch composition.
-template <int SCHEME, int W, int H, int NT, int VAR = 0>
+template <int SCHEME, int W, int H, int NT, int VAR = 0, int LPT = 1>
 __global__ void __launch_bounds__(NT) batched_stage_kernel(const __grid_constant__ BatchArgs B) {
     constexpr int NV = (SCHEME == EE2D) ? 4 : 3;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -868,8 +972,12 @@ __global__ void __launch_bounds__(NT) batched_stage_kernel(const __grid_constant
         J.x0 = (job.y - ty * I.tiles_x) * W;
         J.y0 = ty * H;
         SplitPar P{I.dx, I.dy, I.g, I.gamma, I.theta, sc.dt * I.dt_scale, B.substep, I.variant_beta};
-        process_tile_dimsplit<SCHEME, W, H, NT, true, VAR>(Qs, &bar, phase, init, J, P, sc.do_cfl, sums, B.err, my_cfl,
-                                                      my_sums);
+        bool unhealthy = false;
+        process_tile_dimsplit<SCHEME, W, H, NT, true, VAR, LPT, true>(Qs, &bar, phase, init, J, P, sc.do_cfl, sums,
+                                                                      B.err, my_cfl, my_sums, kWaitPolls,
+                                                                      B.is_last != 0, &unhealthy);
+        // ordered before this tile's arrival (tile_epilogue fences before it counts)
+        if (__syncthreads_or(unhealthy) && threadIdx.x == 0) atomicOr(&I.ctl->bad, 1);
         init = false;
         phase ^= 1u;
         tile_epilogue<NT, NV>(I.ctl, I.block_cfl, I.block_sums, job.y, I.ntiles, B.is_last != 0, false, sc, my_cfl,

@@ -18,14 +18,19 @@
 //     results; calls on one stream are ordered and safe;
 //   * the first call on a device looks up the array's device address
 //     (cudaGetSymbolAddress) and sets the kernel's shared-memory limit, with
-//     that device current; make that first call before any stream capture.
-
+//     that device current; make that first call before any stream capture;
+//   * a tile load that gives up (the kernel's bounded wait) leaves a sticky
+//     error flag in the array; the next call on the device reads it first
+//     (waiting for its stream), clears it and returns FV_ERR_DEVICE without
+//     launching, since the previous output is incomplete.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <cstddef>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -101,7 +106,38 @@ int device_setup(unsigned char** scratch) {
     return FV_OK;
 }
 
+// Poll limit of the kernel's tile-load wait (StageArgs::wait_limit): 0, the
+// default, is the library's limit.  FVGPU_NOALLOC_WAIT_POLLS, read once per
+// process, overrides it; tests set it negative so that every tile load gives
+// up at once and the error report can be checked without a GPU fault.
+int noalloc_wait_limit() {
+    static const int limit = [] {
+        const char* e = getenv("FVGPU_NOALLOC_WAIT_POLLS");
+        return e ? atoi(e) : 0;
+    }();
+    return limit;
+}
+
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// Whether two planes of `n` floats share any element.
+bool overlaps(const float* a, const float* b, size_t n) {
+    const uintptr_t x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+    const uintptr_t bytes = n * sizeof(float);
+    return x < y + bytes && y < x + bytes;
+}
+
+// Wall codes the kernel implements: Dirichlet, periodic, reflective.
+int check_bc(int bc) {
+    if (bc & (int)0xF0F0F0F0u) return noalloc_fail(FV_ERR_INVALID, "unknown bits in the boundary-condition code");
+    for (int side = 0; side < 4; ++side) {
+        const int t = (bc >> (8 * side)) & 0xF;
+        if (t == fv::BC_NEUMANN) return noalloc_fail(FV_ERR_UNSUPPORTED, "Neumann boundary condition not supported");
+        if (t != fv::BC_DIRICHLET && t != fv::BC_PERIODIC && t != fv::BC_REFLECTIVE)
+            return noalloc_fail(FV_ERR_INVALID, "boundary-condition code of a side is not 0, 1, 2 or 3");
+    }
+    return FV_OK;
+}
 
 }  // namespace
 
@@ -117,9 +153,8 @@ int fv_kp07_dimsplit_substep_noalloc(const float* const* in, float* const* out, 
     if (nx < 1 || ny < 1) return noalloc_fail(FV_ERR_INVALID, "grid must be at least 1 x 1");
     if (pitch % 4 != 0 || pitch < nx + 8)
         return noalloc_fail(FV_ERR_INVALID, "pitch must be a multiple of 4 floats and at least nx + 8");
-    for (int side = 0; side < 4; ++side)
-        if (((bc >> (8 * side)) & 0xF) == fv::BC_NEUMANN)
-            return noalloc_fail(FV_ERR_UNSUPPORTED, "Neumann boundary condition not supported");
+    int rc = check_bc(bc);
+    if (rc != FV_OK) return rc;
     const dim3 grid((nx + kW - 1) / kW, (ny + kH - 1) / kH);
     if ((long long)grid.x * grid.y > kMaxTiles) {
         char msg[160];
@@ -127,12 +162,34 @@ int fv_kp07_dimsplit_substep_noalloc(const float* const* in, float* const* out, 
                  nx, ny, (long long)grid.x * grid.y, kMaxTiles);
         return noalloc_fail(FV_ERR_INVALID, msg);
     }
+    // The kernel reads halo cells of `in` that neighbouring CTAs may already
+    // have written in `out`: the output planes must share no element with any
+    // input plane or with each other.
+    const size_t plane = (size_t)(ny + 4) * (size_t)pitch;
+    for (int v = 0; v < 3; ++v)
+        for (int w = 0; w < 3; ++w)
+            if (overlaps(in[v], out[w], plane) || (w != v && overlaps(out[v], out[w], plane)))
+                return noalloc_fail(FV_ERR_INVALID, "output planes must not overlap the input planes or each other");
     unsigned char* scratch = nullptr;
-    int rc = device_setup(&scratch);
+    rc = device_setup(&scratch);
     if (rc != FV_OK) return rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     fv::SimCtl* ctl = reinterpret_cast<fv::SimCtl*>(scratch);
     float* block_cfl = reinterpret_cast<float*>(scratch + kCtlBytes);
+
+    // The error flag of the previous call: a tile load of it that gave up
+    // left part of its output unwritten.  Reading it waits for this stream.
+    int prev_error = 0;
+    if (cudaMemcpyAsync(&prev_error, &ctl->error, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return noalloc_fail(FV_ERR_CUDA, "reading the static control block's error flag failed");
+    if (prev_error) {
+        if (cudaMemsetAsync(&ctl->error, 0, sizeof(int), s) != cudaSuccess)
+            return noalloc_fail(FV_ERR_CUDA, "clearing the static control block's error flag failed");
+        return noalloc_fail(FV_ERR_DEVICE,
+                            "a tile load of the previous allocation-free substep on this device gave up: its output "
+                            "is incomplete (the flag is now cleared)");
+    }
 
     alignas(64) fv::StageArgs a;
     memset(&a, 0, sizeof(a));
@@ -168,10 +225,15 @@ int fv_kp07_dimsplit_substep_noalloc(const float* const* in, float* const* out, 
     a.explicit_dt = 1;
     a.dt_step = dt;
     a.want_sums = 0;
+    a.wait_limit = noalloc_wait_limit();
 
-    // The control block must start at zero: buffer parity 0 (read `in`, write
-    // `out`), arrival counter 0, no error.
-    if (cudaMemsetAsync(ctl, 0, sizeof(fv::SimCtl), s) != cudaSuccess)
+    // The control block must start at zero up to the error flag: buffer
+    // parity 0 (read `in`, write `out`), arrival counter 0.  The error flag
+    // (zero here) stays as this call's kernel leaves it, for the next call.
+    static_assert(offsetof(fv::SimCtl, error) > offsetof(fv::SimCtl, arrive) &&
+                      offsetof(fv::SimCtl, error) > offsetof(fv::SimCtl, cur),
+                  "the cleared prefix of the control block covers the buffer parity and the arrival counter");
+    if (cudaMemsetAsync(ctl, 0, offsetof(fv::SimCtl, error), s) != cudaSuccess)
         return noalloc_fail(FV_ERR_CUDA, "clearing the static control block failed");
     void* kargs[] = {&a};
     cudaError_t e = cudaLaunchKernel(reinterpret_cast<const void*>(kKernel), grid, dim3(kNT), kargs, kSmem, s);

@@ -14,6 +14,16 @@ Arrived requests are uploaded by admission threads and finished scenarios
 are downloaded and released by return threads, so host-to-device uploads of
 new requests, device-to-host reads of results and the queuing of the next
 chunk overlap.
+
+Failures stay with their request.  A request that cannot run (a scheme
+without batched kernels, a grid larger than the whole budget, the wrong
+number or shape of arrays, a GPU with no room even when nothing else is
+resident) comes back with status "rejected" and its reason; a scenario whose
+state goes bad on the GPU (a non-finite value or a non-positive depth after
+a step, or a non-finite time step, e.g. from a corrupted initial state; the
+counterpart of the reference's check(), GPUSimulators/Common.py:772-780)
+stops there, its slot and memory are released, and it comes back with status
+"failed".  The other scenarios run on unchanged.
 """
 
 from __future__ import annotations
@@ -46,7 +56,7 @@ SCHEME_PARAMS = {
 class Request:
     rid: int
     scheme: str
-    variables: list
+    variables: object  # list of host arrays, or a callable returning them (called at admission)
     nx: int
     ny: int
     dx: float
@@ -67,12 +77,14 @@ class Request:
 class Result:
     rid: int
     scheme: str
-    state: list
+    state: object  # the downloaded arrays (or what serve()'s result_fn made of them); None unless done
     steps: int
     t: float
     arrival: float
-    admitted: float
+    admitted: Optional[float]
     finished: float
+    status: str = "done"  # "done", "failed" (its state went bad on the GPU) or "rejected" (could not run)
+    error: Optional[str] = None
 
     @property
     def latency(self):
@@ -111,7 +123,7 @@ class Server(object):
                                           max_instances=self.max_instances)
         return b
 
-    def serve(self, requests: List[Request], clock=time.perf_counter):
+    def serve(self, requests: List[Request], clock=time.perf_counter, result_fn=None):
         """Serve `requests` (arrival times relative to the call) until all are done.
 
         The calling thread queues the next chunk of steps for every batch with
@@ -124,25 +136,34 @@ class Server(object):
         (later chunks skip them), and their memory returns to the budget once
         released.  Several return threads copy results out in parallel.
 
-        Raises ValueError for a request of a scheme without batched kernels or
-        one that needs more device memory than the whole budget, and
-        MemoryError when the GPU has no room for a request while no other
-        scenario holds device memory (waiting could not help).
+        Every request comes back as one Result: "done" with its state
+        (``result_fn(request, arrays)`` if given, on a return thread, e.g. to
+        keep a checksum instead of the arrays), or "rejected" / "failed" with
+        the reason (see the module docstring).  Returns (results, stats);
+        the stats count and time the done requests.
         """
-        for r in requests:
-            if r.scheme not in SCHEME_PARAMS:
-                raise ValueError("request %d: no batched kernels for scheme %r" % (r.rid, r.scheme))
-            if state_bytes(r.scheme, r.nx, r.ny) > self.budget:
-                raise ValueError("request %d: a %d x %d grid needs more device memory than the budget of %.3g bytes"
-                                 % (r.rid, r.nx, r.ny, self.budget))
-        pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
-        running = {}  # (scheme, slot) -> (request, admitted, bytes): on the GPU, not yet at t_end
+        pending = collections.deque()
+        running = {}  # (batch key, slot) -> (request, admitted, bytes): on the GPU, not yet at t_end
         results: List[Result] = []
         lock = threading.Lock()
         returns = queue.Queue()
         shared = {"cells": 0, "outstanding": 0, "error": None}
         timers = collections.Counter()
         t0 = clock()
+
+        def finish(r, status, error, admitted=None, steps=0, t=0.0):
+            with lock:
+                results.append(Result(r.rid, r.scheme, None, steps, t, r.arrival, admitted, clock() - t0, status,
+                                      error))
+
+        for r in sorted(requests, key=lambda r: r.arrival):
+            if r.scheme not in SCHEME_PARAMS:
+                finish(r, "rejected", "no batched kernels for scheme %r" % (r.scheme,))
+            elif state_bytes(r.scheme, r.nx, r.ny) > self.budget:
+                finish(r, "rejected", "a %d x %d grid needs more device memory than the budget of %.3g bytes"
+                       % (r.nx, r.ny, self.budget))
+            else:
+                pending.append(r)
 
         def return_finished():
             while True:
@@ -157,6 +178,8 @@ class Server(object):
                     st = b.status(slot)
                     state = b.download(slot)
                     b.remove(slot)
+                    if result_fn is not None:
+                        state = result_fn(r, state)
                 except Exception as e:  # reported by serve()
                     with lock:
                         shared["error"] = e
@@ -171,11 +194,16 @@ class Server(object):
                     timers["return"] += clock() - ta
 
         def admit(b, r):
+            """Uploads one request; its slot, or raises (MemoryError: no room now;
+            AssertionError / ValueError / TypeError: the request is malformed)."""
             ta = clock()
-            slot = b.add(r.variables, r.nx, r.ny, r.dx, r.dy, r.t_end, r.boundary_conditions)
+            variables = r.variables() if callable(r.variables) else r.variables
+            slot = b.add(variables, r.nx, r.ny, r.dx, r.dy, r.t_end, r.boundary_conditions)
             with lock:
                 timers["admit_upload"] += clock() - ta
             return slot
+
+        malformed = (AssertionError, ValueError, TypeError, IndexError)
 
         workers = [threading.Thread(target=return_finished, name="fvgpu-return-%d" % k, daemon=True)
                    for k in range(self.return_threads)]
@@ -204,13 +232,19 @@ class Server(object):
                             self.used -= need
                         requeue.append(r)
                         continue
+                    except malformed as e:
+                        with lock:
+                            self.used -= need
+                        finish(r, "rejected", "%s: %s" % (type(e).__name__, e))
+                        continue
                     running[(bk, slot)] = (r, clock() - t0, need)
                 admitting = still
                 if requeue:
                     if not (running or admitting or outstanding):
-                        raise MemoryError("request %d does not fit on the GPU with no other scenario resident"
-                                          % requeue[0].rid)
-                    pending.extendleft(sorted(requeue, key=lambda r: r.arrival, reverse=True))
+                        for r in requeue:  # waiting cannot help: nothing else holds device memory
+                            finish(r, "rejected", "does not fit on the GPU with no other scenario resident")
+                    else:
+                        pending.extendleft(sorted(requeue, key=lambda r: r.arrival, reverse=True))
                 if not (pending or running or outstanding or admitting):
                     break
                 # 1. queue the next chunk
@@ -246,27 +280,44 @@ class Server(object):
                         admitting.append((pool.submit(admit, self._batch(bk), r), r, bk, need))
                         continue
                     try:
-                        slot = self._batch(bk).add(r.variables, r.nx, r.ny, r.dx, r.dy, r.t_end,
-                                                   r.boundary_conditions)
+                        slot = admit(self._batch(bk), r)
                     except MemoryError:
                         with lock:
                             self.used -= need
                         if not (running or admitting or outstanding):
-                            raise
+                            pending.popleft()
+                            finish(r, "rejected", "does not fit on the GPU with no other scenario resident")
+                            continue
                         break
+                    except malformed as e:
+                        with lock:
+                            self.used -= need
+                        pending.popleft()
+                        finish(r, "rejected", "%s: %s" % (type(e).__name__, e))
+                        continue
                     pending.popleft()
                     running[(bk, slot)] = (r, clock() - t0, need)
                 timers["admit"] += clock() - ta
-                # 3. wait for the chunk; hand the scenarios at t_end to the return thread
+                # 3. wait for the chunk; hand the scenarios at t_end to the return
+                #    threads and release the ones that failed
                 ta = clock()
                 for s in active:
                     self.batches[s].sync()
                 for key in [k for k in running if k[0] in active]:
-                    if self.batches[key[0]].status(key[1])["done"]:
-                        r, admitted, need = running.pop(key)
+                    st = self.batches[key[0]].status(key[1])
+                    if not st["done"]:
+                        continue
+                    r, admitted, need = running.pop(key)
+                    if st["failed"]:
+                        self.batches[key[0]].remove(key[1])
                         with lock:
-                            shared["outstanding"] += 1
-                        returns.put((key, r, admitted, need))
+                            self.used -= need
+                        finish(r, "failed", "non-finite value or non-positive depth after step %d (t=%g)"
+                               % (st["nt"], st["t"]), admitted, st["nt"], st["t"])
+                        continue
+                    with lock:
+                        shared["outstanding"] += 1
+                    returns.put((key, r, admitted, need))
                 timers["wait"] += clock() - ta
                 if not active:
                     # nothing on the GPU: wait for the next arrival, an upload or returns to free memory
@@ -282,9 +333,12 @@ class Server(object):
             raise shared["error"]
         cells = shared["cells"]
         elapsed = clock() - t0
-        lat = np.array([r.latency for r in results]) if results else np.zeros(1)
+        done = [r for r in results if r.status == "done"]
+        lat = np.array([r.latency for r in done]) if done else np.zeros(1)
         stats = {
-            "requests": len(results),
+            "requests": len(done),
+            "rejected": sum(r.status == "rejected" for r in results),
+            "failed": sum(r.status == "failed" for r in results),
             "elapsed_s": elapsed,
             "cell_updates": cells,
             "cell_updates_per_s": cells / max(elapsed - (busy_since or 0.0), 1e-9),

@@ -232,7 +232,14 @@ FV_API int fv_batch_remove(fv_batch* batch, int slot);
 FV_API int fv_batch_run(fv_batch* batch, int n_steps);
 /* Waits for queued work and refreshes the host view of every simulation. */
 FV_API int fv_batch_sync(fv_batch* batch);
-/* t, nt, dt and whether the simulation reached t_end, as of the last sync. */
+/* t, nt, dt and the simulation's state as of the last sync: done = 0 still
+ * running, 1 reached t_end, 2 failed (a step left a non-finite value or a
+ * non-positive depth or density, t or dt is not a number, e.g. from a
+ * non-finite initial state, or dt is not positive before t_end): a failed
+ * simulation takes no further steps and
+ * its state is undefined; the other simulations of the batch are unaffected.
+ * The reference's counterpart is check()'s NaN test (GPUSimulators/Common.py:772-780,
+ * called from Simulator.simulate, GPUSimulators/Simulator.py:210-217). */
 FV_API int fv_batch_status(fv_batch* batch, int slot, double* t, long long* nt, float* dt, int* done);
 FV_API int fv_batch_download(fv_batch* batch, int slot, int var, float* host, int host_pitch);
 /* Device bytes held, simulations in the batch, work-list length, device time
@@ -241,21 +248,29 @@ FV_API int fv_batch_info(fv_batch* batch, size_t* device_bytes, int* active, int
 /* Tile shape, threads per CTA and persistent grid size of the batch's kernel. */
 FV_API int fv_batch_tile(fv_batch* batch, int* tile_w, int* tile_h, int* threads, int* grid);
 
-/* One KP07_dimsplit substep (GPUSimulators/cuda/SWE2D_KP07_dimsplit.cu semantics)
- * that allocates no memory: for callers that may not call cudaMalloc, such as
- * applications that own all device memory through their own pool, or loops
- * that must not pay allocation latency or risk running out of memory mid-run.
- * No counterpart in the reference.
+/* One KP07_dimsplit substep that allocates no memory, for callers that may
+ * not call cudaMalloc: applications that own all device memory through their
+ * own pool, or loops that must not pay allocation latency or risk running out
+ * of memory mid-run.  No counterpart in the reference.
  * in/out: 3 device pointers (h, hu, hv), each (ny+4) x pitch floats, element
  * (y, x) at [(y+2)*pitch + x+4], 16-byte aligned, pitch a multiple of 4 and
- * >= nx+8; dt is the kernel dt (half the step dt, as KP07_dimsplit.py:109
- * passes); step selects the sweep order; cfl_min (device float*, may be NULL)
- * receives min over cells of min(dx/(|u|+sqrt(gh)), dy/(|v|+sqrt(gh))).
+ * >= nx+8; no output plane may overlap an input plane or another output
+ * plane (FV_ERR_INVALID).  dt is the kernel dt (half the step dt of a split
+ * step); step selects the sweep order (0: x then y); bc is the boundary codec
+ * of fv_sim_create with each side Dirichlet, periodic or reflective (Neumann:
+ * FV_ERR_UNSUPPORTED, other codes FV_ERR_INVALID); cfl_min (device float*,
+ * may be NULL) receives min over cells of min(dx/(|u|+sqrt(gh)),
+ * dy/(|v|+sqrt(gh))).
  * Scratch is a static device array of about 33 KB per GPU, limiting a call to
  * 8192 tiles of 124 x 60 cells (FV_ERR_INVALID beyond).  Calls that overlap on
  * the GPU share that array and race.  The first call on a device performs its
  * set-up (symbol lookup, kernel attribute); make it before any stream capture.
- * Asynchronous on `stream` (a cudaStream_t, or NULL). */
+ * Each call first waits for `stream` and reads the error flag the previous
+ * call may have left: if a tile load of that call gave up, its output is
+ * incomplete, and this call clears the flag and returns FV_ERR_DEVICE without
+ * launching.  Otherwise asynchronous on `stream` (a cudaStream_t, or NULL).
+ * Test hook: FVGPU_NOALLOC_WAIT_POLLS (read once per process) sets the tile
+ * load's poll limit; a negative value makes every tile load give up at once. */
 FV_API int fv_kp07_dimsplit_substep_noalloc(const float* const* in, float* const* out, int pitch, int nx, int ny,
                                             float dx, float dy, float dt, float g, float theta, int step, int bc,
                                             float* cfl_min, void* stream);

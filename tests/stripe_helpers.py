@@ -45,6 +45,10 @@ class OracleStripe(OracleSim):
     def synchronize(self):
         pass
 
+    def check(self):
+        for a in self.u0:
+            assert np.all(np.isfinite(a[self.gc:self.gc + self.ny, self.gc:self.gc + self.nx])), "NaN in state"
+
 
 class BandedOracleStripe(OracleStripe):
     """OracleStripe that also runs a substep in bands of tile rows, as the GPU
@@ -140,3 +144,57 @@ def run_gloo(world, scheme, nx, ny, bc, t_end, out_path, banded=False):
     mp.start_processes(gloo_worker, args=(world, free_port(), scheme, nx, ny, bc, t_end, out_path, banded),
                        nprocs=world, join=True, start_method="spawn")
     return np.load(out_path)
+
+
+def profiling_worker(rank, world, port, out_path):
+    """One rank of a gloo run of Common.runSimulation over an MPISimulator,
+    with the reference driver's profile aggregation (mpiTesting.py:171-177)
+    applied to the returned dictionaries on rank 0."""
+    import datetime
+    import json
+
+    import torch.distributed as dist
+
+    from finitevolumegpu_b200.Common import runSimulation
+    from finitevolumegpu_b200.MPISimulator import MPISimulator, StripeGrid, stripe_rows
+
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        nx, ny = 40, 24
+        q, dx, dy, g = global_state("KP07_dimsplit", nx, ny)
+        y0, rows = stripe_rows(ny, world)[rank]
+        grid = StripeGrid()
+
+        def gen_sim(nx, ny, dx, dy, g, h0, hu0, hv0):
+            sim = BandedOracleStripe("KP07_dimsplit", [h0, hu0, hv0], nx, ny, dx, dy, g, cfl_scale=0.45,
+                                     bc=0x03030303)
+            return MPISimulator(sim, grid)
+
+        args = {"nx": nx, "ny": rows, "dx": dx, "dy": dy, "g": g,
+                "h0": q[0][y0:y0 + rows], "hu0": q[1][y0:y0 + rows], "hv0": q[2][y0:y0 + rows]}
+        outfile, sim_runner_profiling_data, sim_profiling_data = runSimulation(
+            gen_sim, args, out_path + ".%d.nc" % rank, [0.0, 1.0, 2.0], ["h", "hu", "hv"])
+        profiling_data = {}
+        for stage in sim_runner_profiling_data["start"].keys():
+            profiling_data[stage] = sim_runner_profiling_data["end"][stage] - sim_runner_profiling_data["start"][stage]
+        for stage in sim_profiling_data["start"].keys():
+            profiling_data[stage] = sim_profiling_data["end"][stage] - sim_profiling_data["start"][stage]
+        profiling_data["n_time_steps"] = sim_profiling_data["n_time_steps"]
+        if rank == 0:
+            with open(out_path, "w") as f:
+                json.dump(profiling_data, f)
+    finally:
+        dist.destroy_process_group()
+
+
+def run_profiling_gloo(world, out_path):
+    import json
+
+    import torch.multiprocessing as mp
+
+    os.environ.setdefault("GLOO_SOCKET_IFNAME", "lo")
+    mp.start_processes(profiling_worker, args=(world, free_port(), out_path), nprocs=world, join=True,
+                       start_method="spawn")
+    with open(out_path) as f:
+        return json.load(f)

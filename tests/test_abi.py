@@ -224,3 +224,32 @@ def test_null_handles_are_rejected_before_any_cuda_call():
     assert L.fv_sim_destroy(None) == _lib.FV_OK and L.fv_batch_destroy(None) == _lib.FV_OK
     assert L.fv_context_destroy(None) == _lib.FV_OK
     assert L.fv_context_device_name(None, None, 0) == _lib.FV_ERR_INVALID
+
+
+def test_noalloc_argument_checks_come_before_any_cuda_call():
+    """The allocation-free substep refuses unknown wall codes, Neumann walls and
+    output planes that overlap an input plane or each other before it touches
+    the GPU (the addresses below are never dereferenced)."""
+    L = _lib.lib()
+    FP = _lib._FP
+    nx, ny = 100, 50
+    pitch = nx + 8
+    plane = (ny + 4) * pitch * 4
+
+    def planes(base):
+        return (FP * 3)(*[ctypes.cast(base + k * plane, FP) for k in range(3)])
+
+    ins, outs = planes(1 << 32), planes((1 << 32) + 3 * plane)
+
+    def call(i, o, bc=0x03030303):
+        return L.fv_kp07_dimsplit_substep_noalloc(i, o, pitch, nx, ny, 1.0, 1.0, 0.01, 9.81, 1.3, 0, bc, None, None)
+
+    for bc in (0x03030304, 0x0F000000, 0x03030313):
+        assert call(ins, outs, bc) == _lib.FV_ERR_INVALID, hex(bc)
+    assert call(ins, outs, 0x01030303) == _lib.FV_ERR_UNSUPPORTED
+    assert call(ins, ins) == _lib.FV_ERR_INVALID
+    assert "overlap" in L.fv_last_error().decode()
+    shifted = (FP * 3)(*[ctypes.cast((1 << 32) + 3 * plane - 16, FP), outs[1], outs[2]])
+    assert call(ins, shifted) == _lib.FV_ERR_INVALID  # last 16 bytes of the third input plane
+    same = (FP * 3)(outs[0], outs[0], outs[2])
+    assert call(ins, same) == _lib.FV_ERR_INVALID

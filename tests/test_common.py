@@ -60,7 +60,9 @@ def test_run_simulation_writes_quantised_frames(tmp_path):
     times = np.array([0.0, 0.5, 1.25])
     fname, timing, mpi = runSimulation(FakeSim, {"nx": 12, "ny": 9, "dx": 1.0, "dy": 1.0}, str(tmp_path / "o.nc"),
                                        times, ["h", None, "hv"])
-    assert mpi is None and set(timing) == {"t_sim_init", "t_nc_write", "t_full_step"}
+    assert mpi is None and set(timing) == {"start", "end"}
+    for stage in ("t_sim_init", "t_nc_write", "t_full_step"):
+        assert timing["end"][stage] - timing["start"][stage] >= 0.0
     ref = FakeSim(12, 9)
     with netcdf_file(fname, "r", mmap=False) as f:
         assert np.allclose(f.variables["time"][:], times)

@@ -170,3 +170,67 @@ def test_server_respects_memory_budget(ctx):
     assert stats["requests"] == 6
     admitted = sorted(r.admitted for r in results)
     assert admitted[-1] > admitted[0]  # later requests waited for memory
+
+
+def test_batch_failed_simulations_stop_and_the_others_match_plain(ctx):
+    """Corrupted initial states fail alone: a NaN depth makes the initial time
+    step NaN (control-block check); a NaN in hv alone leaves the time step
+    finite (the reference's min over axes drops it), so the stage kernel's
+    per-step health check must catch it.  Both stop, the other simulations
+    of the batch equal their plain runs bit for bit."""
+    b = Batch(ctx, "KP07_dimsplit", max_instances=8)
+    cases = {}
+    bad = {}
+    for k, (nx, ny) in enumerate([(97, 150), (130, 131), (64, 64), (250, 120)]):
+        q, dx, dy, t_end = scenario("KP07_dimsplit", nx, ny, "bump" if k % 2 else "dam", 40 + k)
+        if k == 1:
+            q = [a.copy() for a in q]
+            q[0][ny // 2, nx // 3] = np.nan
+        if k == 2:
+            q = [a.copy() for a in q]
+            q[2][5, 7] = np.nan
+        slot = b.add(q, nx, ny, dx, dy, t_end)
+        (bad if k in (1, 2) else cases)[slot] = (q, nx, ny, dx, dy, t_end)
+    b.run_to_completion()
+    for slot in bad:
+        st = b.status(slot)
+        assert st["done"] and st["failed"], st
+        assert st["nt"] <= 1  # stopped at once
+    for slot, (q, nx, ny, dx, dy, t_end) in cases.items():
+        st = b.status(slot)
+        assert st["done"] and not st["failed"]
+        want, nt, t = plain(ctx, "KP07_dimsplit", q, nx, ny, dx, dy, t_end)
+        assert st["nt"] == nt and st["t"] == t
+        for a, w in zip(b.download(slot), want):
+            assert np.array_equal(a, w)
+
+
+def test_server_isolates_bad_requests(ctx):
+    """A corrupted initial state comes back failed, a wrong shape rejected, an
+    unknown scheme rejected; every other request equals its solo run."""
+    reqs = []
+    for i in range(9):
+        s = ("KP07_dimsplit", "HLL")[i % 2]
+        nx, ny = 60 + 13 * i, 90 - 5 * i
+        q, dx, dy, t_end = scenario(s, nx, ny, "bump" if i % 3 else "dam", 300 + i)
+        reqs.append(Request(i, s, q, nx, ny, dx, dy, t_end, arrival=0.001 * i))
+    reqs[2].variables = [a.copy() for a in reqs[2].variables]
+    reqs[2].variables[1][3, 4] = np.inf  # corrupted momentum
+    reqs[5].variables = [a[:-1] for a in reqs[5].variables]  # one row short
+    reqs[7].scheme = "KP07"  # unsplit: not served
+    results, stats = Server(ctx, budget_bytes=2e9, chunk_steps=4, max_instances=32).serve(reqs)
+    by = {r.rid: r for r in results}
+    assert len(results) == 9
+    assert by[2].status == "failed" and by[2].state is None
+    assert by[5].status == "rejected" and "shape" in by[5].error
+    assert by[7].status == "rejected"
+    assert stats["requests"] == 6 and stats["failed"] == 1 and stats["rejected"] == 2
+    for r in reqs:
+        if r.rid in (2, 5, 7):
+            continue
+        res = by[r.rid]
+        assert res.status == "done"
+        want, nt, t = plain(ctx, r.scheme, r.variables, r.nx, r.ny, r.dx, r.dy, r.t_end)
+        assert res.steps == nt and res.t == t
+        for a, w in zip(res.state, want):
+            assert np.array_equal(a, w), (r.rid, rel_linf(a, w))

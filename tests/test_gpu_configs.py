@@ -6,6 +6,17 @@
   1000 steps.  Compared with the reference's own kernels after 100 steps
   (relative L-inf <= 1e-5) and with the FP64 oracle after 1000 steps
   (relative L1 <= 1e-4); FP64 mass sum conserved to FP32 round-off.
+* Config 2: the seven SWE schemes on the 4096 x 4096 seeded circular dam
+  break (h = 1 inside R ~ U(0.1, 0.3) x width, 0.1 outside), reflective
+  walls, cfl_scale 0.9, 200 steps, against the reference's own kernels on
+  the same inputs: relative L1 <= 1e-4 per conserved variable, and relative
+  L-inf within 1e-5 or twice the distance between two valid builds of the
+  reference (at a dam break WAF and KP07 amplify single roundings to 1e-3).
+  FORCE goes unstable at this step size in the reference (dt is refreshed
+  only every 100 steps while the flow speeds up), and cells become NaN here
+  as there: the cells whose finiteness differs from the reference's may be
+  no more than between the reference's two builds, and the cells finite in
+  both are compared.
 * Config 3: EE2D_KP07_dimsplit Kelvin-Helmholtz, gamma = 1.4, periodic:
   at 4096 x 2048 for 500 steps the FP64 sums of rho, rho*u, rho*v and E stay
   at their initial values to FP32 round-off; the relative L1/L-inf error
@@ -95,6 +106,60 @@ def test_config1_kp07_dimsplit_256(ctx):
             "mass_rel_change": abs(m1 - m0) / m0})
     assert max(l1) <= 1e-4, l1
     assert abs(m1 - m0) / m0 <= 1e-6
+
+
+def config2_dam_break(n=4096, seed=0):
+    rng = np.random.default_rng(seed)
+    R = rng.uniform(0.1, 0.3) * n
+    y, x = np.mgrid[0:n, 0:n] + 0.5
+    h = np.where(np.hypot(x - n / 2.0, y - n / 2.0) < R, 1.0, 0.1).astype(np.float32)
+    z = np.zeros_like(h)
+    return [h, z, z.copy()]
+
+
+@pytest.fixture(scope="module")
+def config2_state():
+    return config2_dam_break()
+
+
+@pytest.mark.parametrize("scheme", ["LxF", "FORCE", "HLL", "HLL2", "WAF", "KP07", "KP07_dimsplit"])
+def test_config2_vs_reference_kernels(ctx, config2_state, scheme):
+    n, steps = 4096, 200
+    q = config2_state
+
+    def run_ref(build):
+        ref = ref_kernels.RefKernelSim(scheme, q, n, n, 1.0, 1.0, 9.81, cfl_scale=0.9, build=build)
+        advance_host(ref, steps)
+        out = ref.download()
+        ref.close()
+        return out
+
+    want = run_ref(None)
+    other = run_ref("nofma")
+    sim = fv.SCHEMES[scheme](ctx, *q, n, n, 1.0, 1.0, 9.81, cfl_scale=0.9)
+    sim.advance(steps)
+    got = sim.download()
+    del sim
+    l1, linf, floor, finite = [], [], [], []
+    for a, b, c in zip(got, want, other):
+        fa, fb, fc = np.isfinite(a), np.isfinite(b), np.isfinite(c)
+        # cells whose finiteness differs from the reference's: no more than
+        # between the reference's two builds (plus 1e-4 of the cells)
+        assert (fa != fb).mean() <= (fc != fb).mean() + 1e-4, (scheme, (fa != fb).mean(), (fc != fb).mean())
+        finite.append(float(fb.mean()))
+        m, mc = fa & fb, fb & fc
+        if not m.any():
+            l1.append(0.0), linf.append(0.0), floor.append(0.0)
+            continue
+        l1.append(rel_l1(a[m], b[m]))
+        linf.append(rel_linf(a[m], b[m]))
+        floor.append(rel_linf(c[mc], b[mc]) if mc.any() else 0.0)
+    record({"config": 2, "scheme": scheme, "n": n, "steps": steps, "rel_l1_vs_reference_kernels": l1,
+            "rel_linf_vs_reference_kernels": linf, "reference_build_to_build_rel_linf": floor,
+            "finite_fraction": finite})
+    for v in range(3):
+        assert l1[v] <= 1e-4, (scheme, v, l1)
+        assert linf[v] <= max(1e-5, 2.0 * floor[v]), (scheme, v, linf, floor)
 
 
 def test_config3_ee2d_conservation_full_size(ctx):

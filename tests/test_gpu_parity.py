@@ -165,35 +165,53 @@ def test_dam_break_vs_oracle(ctx, scheme):
         assert rel_l1(a, b) < 1e-5
 
 
+def _run_reference(make, n_steps, build=None):
+    """n_steps of simulate()'s dt schedule through the reference's kernels."""
+    ref = make(build)
+    for _ in range(n_steps):
+        if ref.nt % 100 == 0:
+            ref.dt = np.float32(ref.computeDt() * np.float32(ref.cfl_scale))
+        ref.step(ref.dt)
+    out = ref.download()
+    ref.close()
+    return out
+
+
 @pytest.mark.parametrize("scheme", SWE + ["EE2D_KP07_dimsplit"])
 def test_vs_reference_kernels(ctx, scheme):
-    """Same inputs through the reference's own kernels (built unmodified for sm_100a)."""
-    assert ref_kernels.available(scheme), "oracle/_ref is not built"
+    """Same inputs through the reference's own kernels (built unmodified for
+    sm_100a), 100 steps: relative L-inf <= 1e-5 per conserved variable, or,
+    where the reference disagrees with itself by more, the distance between
+    two valid builds of the reference (its compile options, and the same
+    without FMA contraction).  That floor is measured here on the same
+    inputs: on WAF's hv (1.2e-5), EE2D's rho_v (3.5e-5, the 1 % perturbation)
+    and KP07_dimsplit's hv (1.1e-5) it is above 1e-5, i.e. 1e-5 is below the
+    rounding freedom the reference's own source leaves."""
+    assert ref_kernels.available(scheme) and ref_kernels.available(scheme, build="nofma"), "oracle/_ref is not built"
     if scheme == "EE2D_KP07_dimsplit":
         nx, ny = 160, 96
         q = kelvin_helmholtz(nx, ny)
         kw = dict(dx=1.0 / nx, dy=1.0 / ny, g=0.0, bc=PERIODIC)
         sim = make_sim(ctx, scheme, q, nx, ny, cfl_scale=0.45, **kw)
-        ref = ref_kernels.RefKernelSim(scheme, q, nx, ny, kw["dx"], kw["dy"], 0.0, gamma=1.4, cfl_scale=0.45,
-                                       bc=PERIODIC)
+
+        def make(build):
+            return ref_kernels.RefKernelSim(scheme, q, nx, ny, kw["dx"], kw["dy"], 0.0, gamma=1.4, cfl_scale=0.45,
+                                            bc=PERIODIC, build=build)
     else:
         nx, ny = 256, 256
         q = bump(nx, ny)
         sim = make_sim(ctx, scheme, list(q), nx, ny, cfl_scale=0.45)
-        ref = ref_kernels.RefKernelSim(scheme, list(q), nx, ny, 1.0, 1.0, 9.81, cfl_scale=0.45)
-    # exactly 100 steps with simulate()'s dt schedule on both sides
-    for _ in range(100):
-        if ref.nt % 100 == 0:
-            ref.dt = np.float32(ref.computeDt() * np.float32(ref.cfl_scale))
-        ref.step(ref.dt)
+
+        def make(build):
+            return ref_kernels.RefKernelSim(scheme, list(q), nx, ny, 1.0, 1.0, 9.81, cfl_scale=0.45, build=build)
+    # exactly 100 steps with simulate()'s dt schedule on all sides
+    ref = _run_reference(make, 100)
+    ref2 = _run_reference(make, 100, build="nofma")
     sim.advance(100)
     assert sim.simSteps() == 100
-    # Noise floor: the IEEE FP32 oracle is up to 1.2e-5 (WAF) from the
-    # fast-math reference kernels after these 100 steps, and 3.7e-5 on rho_v of
-    # the Kelvin-Helmholtz case, whose magnitude is 1/50 of rho_u.
-    tol = {"WAF": 2e-5, "EE2D_KP07_dimsplit": 5e-5}.get(scheme, 1e-5)
-    for a, b in zip(sim.download(), ref.download()):
-        assert rel_linf(a, b) < tol, (scheme, rel_linf(a, b))
+    for v, (a, b, c) in enumerate(zip(sim.download(), ref, ref2)):
+        floor = rel_linf(c, b)
+        assert rel_linf(a, b) <= max(1e-5, floor), (scheme, v, rel_linf(a, b), floor)
 
 
 @pytest.mark.parametrize("scheme", SWE + ["EE2D_KP07_dimsplit"])

@@ -126,6 +126,11 @@ def test_nccl_overlap_equals_plain_exchange(ctx, ny):
             assert mpi.overlap == overlap
             mpi.simulate(3.0)
             outs.append((mpi.download(), mpi.simSteps()))
+            # the reference's profiling dictionary, timed with CUDA events
+            prof = mpi.profiling_data_mpi
+            assert prof["n_time_steps"] == 2 * mpi.simSteps()
+            assert prof["end"]["t_mpi_step"] - prof["start"]["t_mpi_step"] > 0.0
+            assert prof["end"]["t_mpi_halo_exchange"] >= prof["end"]["t_mpi_halo_exchange_sendreceive"] >= 0.0
         (a, na), (b, nb) = outs
         assert na == nb
         for x, y in zip(a, b):

@@ -108,3 +108,20 @@ def test_gloo_overlapped_schedule_equals_single_domain(tmp_path, world, scheme, 
     res = run_gloo(world, scheme, nx, ny, bc, t_end_for(scheme), str(tmp_path / "out.npz"), banded=True)
     assert int(res["nt"]) == nt and float(res["t"]) == t
     assert np.array_equal(res["state"], want), np.max(np.abs(res["state"] - want))
+
+
+def test_run_simulation_returns_reference_profiling(tmp_path):
+    """runSimulation over an MPISimulator returns the reference's profiling
+    dictionaries, and the reference driver's aggregation (end - start per
+    stage, n_time_steps) runs on them: two gloo ranks, overlapped schedule."""
+    from stripe_helpers import run_profiling_gloo
+
+    prof = run_profiling_gloo(2, str(tmp_path / "prof.json"))
+    for stage in ("t_sim_init", "t_nc_write", "t_full_step", "t_mpi_step", "t_mpi_halo_exchange",
+                  "t_mpi_halo_exchange_sendreceive", "t_mpi_halo_exchange_download", "t_mpi_halo_exchange_upload"):
+        assert stage in prof and prof[stage] >= 0.0, (stage, prof)
+    assert prof["t_mpi_step"] > 0.0 and prof["t_mpi_halo_exchange_sendreceive"] > 0.0
+    assert prof["t_mpi_halo_exchange"] >= prof["t_mpi_halo_exchange_sendreceive"]
+    assert prof["t_mpi_halo_exchange_download"] == 0 and prof["t_mpi_halo_exchange_upload"] == 0
+    # two substeps per KP07_dimsplit step; at least the 2-second run's steps
+    assert prof["n_time_steps"] >= 2 and prof["n_time_steps"] % 2 == 0
