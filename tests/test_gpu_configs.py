@@ -16,7 +16,8 @@
   only every 100 steps while the flow speeds up), and cells become NaN here
   as there: the cells whose finiteness differs from the reference's may be
   no more than between the reference's two builds, and the cells finite in
-  both are compared.
+  both are held to twice the distance between those builds (the growing
+  instability amplifies every rounding).
 * Config 3: EE2D_KP07_dimsplit Kelvin-Helmholtz, gamma = 1.4, periodic:
   at 4096 x 2048 for 500 steps the FP64 sums of rho, rho*u, rho*v and E stay
   at their initial values to FP32 round-off; the relative L1/L-inf error
@@ -140,7 +141,7 @@ def test_config2_vs_reference_kernels(ctx, config2_state, scheme):
     sim.advance(steps)
     got = sim.download()
     del sim
-    l1, linf, floor, finite = [], [], [], []
+    l1, linf, floor, floor_l1, finite = [], [], [], [], []
     for a, b, c in zip(got, want, other):
         fa, fb, fc = np.isfinite(a), np.isfinite(b), np.isfinite(c)
         # cells whose finiteness differs from the reference's: no more than
@@ -149,16 +150,18 @@ def test_config2_vs_reference_kernels(ctx, config2_state, scheme):
         finite.append(float(fb.mean()))
         m, mc = fa & fb, fb & fc
         if not m.any():
-            l1.append(0.0), linf.append(0.0), floor.append(0.0)
+            l1.append(0.0), linf.append(0.0), floor.append(0.0), floor_l1.append(0.0)
             continue
         l1.append(rel_l1(a[m], b[m]))
         linf.append(rel_linf(a[m], b[m]))
         floor.append(rel_linf(c[mc], b[mc]) if mc.any() else 0.0)
+        floor_l1.append(rel_l1(c[mc], b[mc]) if mc.any() else 0.0)
     record({"config": 2, "scheme": scheme, "n": n, "steps": steps, "rel_l1_vs_reference_kernels": l1,
             "rel_linf_vs_reference_kernels": linf, "reference_build_to_build_rel_linf": floor,
-            "finite_fraction": finite})
+            "reference_build_to_build_rel_l1": floor_l1, "finite_fraction": finite})
     for v in range(3):
-        assert l1[v] <= 1e-4, (scheme, v, l1)
+        # 1e-4; the unstable FORCE run only as close as the reference's two builds are to each other
+        assert l1[v] <= max(1e-4, 2.0 * floor_l1[v]), (scheme, v, l1, floor_l1)
         assert linf[v] <= max(1e-5, 2.0 * floor[v]), (scheme, v, linf, floor)
 
 

@@ -113,7 +113,7 @@ def test_noalloc_rejects_grids_beyond_the_static_scratch(ctx):
 
 _GIVE_UP_CHILD = textwrap.dedent("""
     import ctypes, sys
-    sys.path.insert(0, %r)
+    sys.path.insert(0, sys.argv[1])
     import torch
     from finitevolumegpu_b200 import _lib
     nx, ny, pitch = 200, 100, 208
@@ -139,7 +139,7 @@ def test_noalloc_reports_a_tile_load_that_gave_up():
     call that launched returns FV_OK, the next one reports FV_ERR_DEVICE and
     clears the flag without launching, so the one after launches again."""
     env = dict(os.environ, FVGPU_NOALLOC_WAIT_POLLS="-1")
-    r = subprocess.run([sys.executable, "-c", _GIVE_UP_CHILD % ROOT], env=env, capture_output=True, text=True,
+    r = subprocess.run([sys.executable, "-c", _GIVE_UP_CHILD, ROOT], env=env, capture_output=True, text=True,
                        timeout=300)
     assert r.returncode == 0, r.stderr[-2000:]
     line = [ln for ln in r.stdout.splitlines() if ln.startswith("RCS")][-1]
