@@ -37,3 +37,34 @@ def test_reference_arm_under_torchrun():
     assert res["cpu_baseline"]["value"] == res["value"] and res["cpu_baseline"]["kind"] == "port"
     assert res["e2e"] == {"value": res["value"], "unit": res["unit"], "h2d_bytes_per_step": 0,
                           "d2h_bytes_per_step": 0}
+
+
+def test_bench_legs_and_initial_states():
+    """Every leg the GPU arm runs is defined, and the seeded initial states
+    have the requested shapes (bench.py's host side, no GPU)."""
+    import numpy as np
+
+    for name in ("run_mine", "run_reference", "run_batched", "run_served", "cpu_baseline_leg",
+                 "reference_kernels_leg", "make_scheme_sim", "ICFeed"):
+        assert callable(getattr(bench, name)), name
+    rng = np.random.default_rng(0)
+    for make, nv in ((bench.bump_ic, 3), (bench.dam_ic, 3), (bench.kh_ic, 4)):
+        q = make(37, 21, rng)
+        assert len(q) == nv and all(a.shape == (21, 37) and a.dtype == np.float32 for a in q)
+        assert np.all(q[0] > 0)
+
+
+def test_ic_feed_serves_requests_in_order_with_skips_and_retries():
+    made = []
+
+    def make(i):
+        made.append(i)
+        return i * 10
+
+    feed = bench.ICFeed(make, 100, threads=3, ahead=4)
+    try:
+        got = [feed.get(i) for i in range(100) if i % 7 != 3]  # some requests are never admitted
+        assert got == [i * 10 for i in range(100) if i % 7 != 3]
+        assert feed.get(17) == 170  # a retried admission regenerates its state
+    finally:
+        feed.close()
