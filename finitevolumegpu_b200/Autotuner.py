@@ -32,12 +32,12 @@ import numpy as np
 
 # Number of tile configurations per scheme in libfvgpu's kernel table.
 TILE_CONFIGS = {
-    "KP07_dimsplit": 7,
-    "HLL2": 7,
-    "WAF": 4,
+    "KP07_dimsplit": 9,
+    "HLL2": 9,
+    "WAF": 9,
     "FORCE": 4,
     "HLL": 4,
-    "EE2D_KP07_dimsplit": 7,
+    "EE2D_KP07_dimsplit": 8,
     "LxF": 4,
     "KP07": 4,
 }

@@ -14,6 +14,7 @@ same as that of a plain simulator run alone.
 from __future__ import annotations
 
 import ctypes
+import threading
 
 import numpy as np
 
@@ -53,6 +54,9 @@ class Batch(object):
                                         ctypes.byref(h)))
         self._h = h
         self.shapes = {}
+        # slot -> (ny, nx); guarded so that a slot released by one thread and
+        # taken again by another's admission keeps the new simulation's shape
+        self._shapes_lock = threading.Lock()
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -75,12 +79,16 @@ class Batch(object):
         slot = ctypes.c_int()
         _lib.check(_L().fv_batch_add(self._h, int(nx), int(ny), float(dx), float(dy), int(bc), ptrs, rows, cols,
                                      float(t_end), ctypes.byref(slot)))
-        self.shapes[slot.value] = (int(ny), int(nx))
+        with self._shapes_lock:
+            self.shapes[slot.value] = (int(ny), int(nx))
         return slot.value
 
     def remove(self, slot):
+        # forget the shape first: once the library releases the slot, another
+        # thread's admission may receive the same slot number
+        with self._shapes_lock:
+            self.shapes.pop(slot, None)
         _lib.check(_L().fv_batch_remove(self._h, int(slot)))
-        self.shapes.pop(slot, None)
 
     def run(self, n_steps):
         """Queue n_steps steps for every simulation (asynchronous)."""
@@ -98,7 +106,8 @@ class Batch(object):
         return {"t": t.value, "nt": nt.value, "dt": dt.value, "done": bool(done.value), "failed": done.value == 2}
 
     def download(self, slot):
-        ny, nx = self.shapes[slot]
+        with self._shapes_lock:
+            ny, nx = self.shapes[slot]
         out = []
         for v in range(self.nv):
             a = np.empty((ny, nx), dtype=np.float32)
@@ -132,7 +141,9 @@ class Batch(object):
         steps = 0
         while True:
             self.sync()
-            if all(self.status(s)["done"] for s in self.shapes):
+            with self._shapes_lock:
+                slots = list(self.shapes)
+            if all(self.status(s)["done"] for s in slots):
                 return steps
             self.run(chunk)
             steps += chunk

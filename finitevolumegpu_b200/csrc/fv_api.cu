@@ -111,6 +111,17 @@ const KEntry kTable[] = {
     {FV_EE2D_KP07_DIMSPLIT, 124, 28, 64, true, fv::dimsplit_stage_kernel<fv::EE2D, 124, 28, 64, 0, 2>},
     {FV_EE2D_KP07_DIMSPLIT, 124, 60, 128, true, fv::dimsplit_stage_kernel<fv::EE2D, 124, 60, 128, 0, 2>},
     {FV_EE2D_KP07_DIMSPLIT, 60, 28, 64, true, fv::dimsplit_stage_kernel<fv::EE2D, 60, 28, 64, 0, 2>},
+    {FV_WAF, 124, 28, 64, true, fv::dimsplit_stage_kernel<fv::WAF, 124, 28, 64, 0, 2>},
+    {FV_WAF, 124, 60, 128, true, fv::dimsplit_stage_kernel<fv::WAF, 124, 60, 128, 0, 2>},
+    {FV_WAF, 60, 28, 64, true, fv::dimsplit_stage_kernel<fv::WAF, 60, 28, 64, 0, 2>},
+    // 8-segment rows (120 wide, padded pitch 136): twice the warps of the 124-wide packed tiles
+    {FV_KP07_DIMSPLIT, 120, 28, 128, true, fv::dimsplit_stage_kernel<fv::KP07_DIMSPLIT, 120, 28, 128, 0, 2>},
+    {FV_KP07_DIMSPLIT, 120, 60, 256, true, fv::dimsplit_stage_kernel<fv::KP07_DIMSPLIT, 120, 60, 256, 0, 2>},
+    {FV_HLL2, 120, 28, 128, true, fv::dimsplit_stage_kernel<fv::HLL2, 120, 28, 128, 0, 2>},
+    {FV_HLL2, 120, 60, 256, true, fv::dimsplit_stage_kernel<fv::HLL2, 120, 60, 256, 0, 2>},
+    {FV_EE2D_KP07_DIMSPLIT, 120, 28, 128, true, fv::dimsplit_stage_kernel<fv::EE2D, 120, 28, 128, 0, 2>},
+    {FV_WAF, 120, 28, 128, true, fv::dimsplit_stage_kernel<fv::WAF, 120, 28, 128, 0, 2>},
+    {FV_WAF, 120, 60, 256, true, fv::dimsplit_stage_kernel<fv::WAF, 120, 60, 256, 0, 2>},
 };
 constexpr int kNumEntries = sizeof(kTable) / sizeof(kTable[0]);
 
@@ -176,7 +187,9 @@ const VBEntry kBatchVariantTable[] = {
 };
 constexpr int kNumBatchVariants = sizeof(kBatchVariantTable) / sizeof(kBatchVariantTable[0]);
 
-size_t batch_smem(const BEntry& e) { return scheme_nv(e.scheme) * (size_t)(e.W + 8) * (e.H + 4) * sizeof(float); }
+size_t batch_smem(const BEntry& e) {
+    return scheme_nv(e.scheme) * (size_t)fv::split_pitch(e.W) * (e.H + 4) * sizeof(float);
+}
 
 // The batched kernel of tile configuration `cfg`, or for variant > 0 the
 // variant's single kernel (cfg is then ignored).
@@ -197,8 +210,11 @@ const BEntry* find_batch_entry(int scheme, int cfg, int variant) {
 }
 
 
+int entry_box_w(const KEntry& e) { return e.split ? fv::split_pitch(e.W) : e.W + 8; }
+
 size_t entry_smem(const KEntry& e) {
-    const size_t tile = (size_t)(e.W + 8) * (e.H + 4) * sizeof(float);
+    // row pitch of the shared tile = width of the TMA box (entry_box_w)
+    const size_t tile = (size_t)entry_box_w(e) * (e.H + 4) * sizeof(float);
     return scheme_nv(e.scheme) * tile;
 }
 
@@ -892,7 +908,7 @@ int fv_sim_create(fv_context* ctx, int scheme, int nx, int ny, float dx, float d
             a.buf[b][v] = s->buf[b][v];
             cuuint64_t dims[2] = {(cuuint64_t)(nx + 8), (cuuint64_t)(ny + 4)};
             cuuint64_t strides[1] = {(cuuint64_t)s->pitch * sizeof(float)};
-            cuuint32_t box[2] = {(cuuint32_t)(ke->W + 8), (cuuint32_t)(ke->H + 4)};
+            cuuint32_t box[2] = {(cuuint32_t)entry_box_w(*ke), (cuuint32_t)(ke->H + 4)};
             cuuint32_t estr[2] = {1, 1};
             CUresult r = enc(&a.tmap[b][v], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, s->buf[b][v], dims, strides, box, estr,
                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -1570,7 +1586,7 @@ int fv_batch_add(fv_batch* b, int nx, int ny, float dx, float dy, int bc, const 
         for (int v = 0; v < b->nv; ++v) {
             cuuint64_t dims[2] = {(cuuint64_t)(nx + 8), (cuuint64_t)(ny + 4)};
             cuuint64_t strides[1] = {(cuuint64_t)pitch * sizeof(float)};
-            cuuint32_t box[2] = {(cuuint32_t)(W + 8), (cuuint32_t)(H + 4)};
+            cuuint32_t box[2] = {(cuuint32_t)fv::split_pitch(W), (cuuint32_t)(H + 4)};
             cuuint32_t estr[2] = {1, 1};
             CUresult r = enc(&I.tmap[k][v], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, I.buf[k][v], dims, strides, box, estr,
                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,

@@ -162,15 +162,37 @@ template <class N> __device__ __forceinline__ N splat(float a);
 template <> __device__ __forceinline__ float splat<float>(float a) { return a; }
 template <> __device__ __forceinline__ f2 splat<f2>(float a) { return f2{a, a}; }
 
+// Fast-math division, reciprocal and square root as explicit PTX: the
+// approximations the reference's --use_fast_math build uses for x / y,
+// 1.0f / x and sqrtf(x), written out so that the compiler cannot rewrite them
+// per call site (fast math lets it turn a / b into a * (1 / b) where it
+// shares a reciprocal), which would round a cell differently depending on
+// the kernel that inlines the formula.
+__device__ __forceinline__ float fdiv_fast(float a, float b) {
+    float d;
+    asm("div.full.ftz.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+    return d;
+}
+__device__ __forceinline__ float frcp_fast(float a) {
+    float d;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(d) : "f"(a));
+    return d;
+}
+__device__ __forceinline__ float fsqrt_fast(float a) {
+    float d;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(d) : "f"(a));
+    return d;
+}
+
 // Lane-wise operations, scalar or pair.
 __device__ __forceinline__ float vneg(float a) { return -a; }
 __device__ __forceinline__ f2 vneg(f2 a) { return f2{-a.x, -a.y}; }
-__device__ __forceinline__ float vdiv(float a, float b) { return a / b; }  // fast-math division
-__device__ __forceinline__ f2 vdiv(f2 a, f2 b) { return f2{a.x / b.x, a.y / b.y}; }
-__device__ __forceinline__ float vrcp(float a) { return 1.0f / a; }
-__device__ __forceinline__ f2 vrcp(f2 a) { return f2{1.0f / a.x, 1.0f / a.y}; }
-__device__ __forceinline__ float vsqrt(float a) { return sqrtf(a); }
-__device__ __forceinline__ f2 vsqrt(f2 a) { return f2{sqrtf(a.x), sqrtf(a.y)}; }
+__device__ __forceinline__ float vdiv(float a, float b) { return fdiv_fast(a, b); }
+__device__ __forceinline__ f2 vdiv(f2 a, f2 b) { return f2{fdiv_fast(a.x, b.x), fdiv_fast(a.y, b.y)}; }
+__device__ __forceinline__ float vrcp(float a) { return frcp_fast(a); }
+__device__ __forceinline__ f2 vrcp(f2 a) { return f2{frcp_fast(a.x), frcp_fast(a.y)}; }
+__device__ __forceinline__ float vsqrt(float a) { return fsqrt_fast(a); }
+__device__ __forceinline__ f2 vsqrt(f2 a) { return f2{fsqrt_fast(a.x), fsqrt_fast(a.y)}; }
 __device__ __forceinline__ float vmin(float a, float b) { return fminf(a, b); }
 __device__ __forceinline__ f2 vmin(f2 a, f2 b) { return f2{fminf(a.x, b.x), fminf(a.y, b.y)}; }
 __device__ __forceinline__ float vmax(float a, float b) { return fmaxf(a, b); }
@@ -285,7 +307,7 @@ __device__ __forceinline__ float flux_limiter(float r, int id, float beta) {
 
 // GPUSimulators/cuda/common.h:81-83
 __device__ __forceinline__ float desingularize(float x, float eps) {
-    return copysignf(fmaxf(fabsf(x), fminf(x * x / (2.0f * eps) + 0.5f * eps, eps)), x);
+    return copysignf(fmaxf(fabsf(x), fminf(fadd(fdiv_fast(fmul(x, x), 2.0f * eps), 0.5f * eps), eps)), x);
 }
 
 // ------------------------------------------------------------------ shallow water
@@ -488,69 +510,84 @@ __device__ __forceinline__ void euler_muscl_hancock(const N (&qm)[4], const N (&
 // ------------------------------------------------------------------ WAF
 
 // Per-cell quantities of the WAF flux (GPUSimulators/cuda/SWECommon.h:131-210):
-// state, velocities, wave speed and physical flux.
-struct WafCell {
-    float q[3];
-    float f[3];
-    float u, v, c;
+// state, velocities, wave speed and physical flux.  N is float, or f2 for two
+// lines walked side by side.
+template <class N>
+struct WafCellT {
+    N q[3];
+    N f[3];
+    N u, v, c;
 };
+using WafCell = WafCellT<float>;
 
-__device__ __forceinline__ WafCell waf_cell(const float q[3], float g, float half_g) {
-    WafCell s;
+template <class N>
+__device__ __forceinline__ WafCellT<N> waf_cell(const N q[3], N g, N half_g) {
+    WafCellT<N> s;
     s.q[0] = q[0];
     s.q[1] = q[1];
     s.q[2] = q[2];
-    const float rh = 1.0f / q[0];
-    s.u = q[1] * rh;
-    s.v = q[2] * rh;
-    s.c = sqrtf(g * q[0]);
+    const N rh = vrcp(q[0]);
+    s.u = fmul(q[1], rh);
+    s.v = fmul(q[2], rh);
+    s.c = vsqrt(fmul(g, q[0]));
     s.f[0] = q[1];
-    s.f[1] = fmaf(q[1], s.u, half_g * q[0] * q[0]);
-    s.f[2] = q[2] * s.u;
+    s.f[1] = ffma(q[1], s.u, fmul(fmul(half_g, q[0]), q[0]));
+    s.f[2] = fmul(q[2], s.u);
     return s;
 }
 
 // h in the star region between two cells (GPUSimulators/cuda/SWECommon.h:114-121).
-__device__ __forceinline__ float waf_h_star(const WafCell& l, const WafCell& r, float inv_g) {
-    const float t = 0.5f * (l.c + r.c) + 0.25f * (l.u - r.u);
-    return t * t * inv_g;
+template <class N>
+__device__ __forceinline__ N waf_h_star(const WafCellT<N>& l, const WafCellT<N>& r, N inv_g) {
+    const N t = fadd(fmul(splat<N>(0.5f), fadd(l.c, r.c)), fmul(splat<N>(0.25f), fsub(l.u, r.u)));
+    return fmul(fmul(t, t), inv_g);
+}
+
+// The WAF weight of one wave (SWECommon.h:109-111, :199-201): the ratio r of
+// upwind to local jumps (both desingularised) through the flux limiter,
+// A = sign(c) * (1 - (1 - |c|) * limiter(r)); up: upwind jump for c > 0,
+// dn: for c <= 0, loc: the local jump.
+__device__ __forceinline__ float waf_weight(float c, float up, float dn, float loc, int limiter, float beta) {
+    const float eps = 1.0e-6f;
+    const float r = fdiv_fast(desingularize((c > 0.0f) ? up : dn, eps), desingularize(loc, eps));
+    return fmul(copysignf(1.0f, c), fsub(1.0f, fmul(fsub(1.0f, fabsf(c)), flux_limiter(r, limiter, beta))));
+}
+__device__ __forceinline__ f2 waf_weight(f2 c, f2 up, f2 dn, f2 loc, int limiter, float beta) {
+    return f2{waf_weight(c.x, up.x, dn.x, loc.x, limiter, beta), waf_weight(c.y, up.y, dn.y, loc.y, limiter, beta)};
 }
 
 // WAF flux at the face between l1 and r1 (GPUSimulators/cuda/SWECommon.h:131-210);
 // hd_l, hd, hd_r are the star depths of the pairs (l2,l1), (l1,r1), (r1,r2).
-__device__ __forceinline__ void waf_flux(const WafCell& l2, const WafCell& l1, const WafCell& r1,
-                                         const WafCell& r2, float hd_l, float hd, float hd_r, float dtdx,
-                                         float out[3], int limiter = 0, float beta = 0.0f) {
-    const float h_l = l1.q[0], h_r = r1.q[0];
-    const float q_l = (hd > h_l) ? sqrtf(0.5f * ((hd + h_l) * hd)) / h_l : 1.0f;
-    const float q_r = (hd > h_r) ? sqrtf(0.5f * ((hd + h_r) * hd)) / h_r : 1.0f;
-    const float S_l = fmaf(-l1.c, q_l, l1.u);
-    const float S_r = fmaf(r1.c, q_r, r1.u);
-    const float a_r = h_r * (r1.u - S_r);
-    const float a_l = h_l * (l1.u - S_l);
-    const float S_star = (S_l * a_r - S_r * a_l) / (a_r - a_l);
-    const float sl = h_l * (S_l - l1.u) / (S_l - S_star);
-    const float sr = h_r * (S_r - r1.u) / (S_r - S_star);
-    const float Qsl[3] = {sl, sl * S_star, sl * l1.v};
-    const float Qsr[3] = {sr, sr * S_star, sr * r1.v};
-    const float c_1 = S_l * dtdx;
-    const float c_2 = S_star * dtdx;
-    const float c_3 = S_r * dtdx;
-    const float eps = 1.0e-6f;
-    const float r_1 = desingularize((c_1 > 0.0f) ? (hd_l - l2.q[0]) : (hd_r - h_r), eps) / desingularize(hd - h_l, eps);
-    const float r_2 = desingularize((c_2 > 0.0f) ? (l1.v - l2.v) : (r2.v - r1.v), eps) / desingularize(r1.v - l1.v, eps);
-    const float r_3 = desingularize((c_3 > 0.0f) ? (h_l - hd_l) : (r2.q[0] - hd_r), eps) / desingularize(h_r - hd, eps);
-    // A_k = sign(c_k) * (1 - (1 - |c_k|) * limiter(r_k)) (SWECommon.h:109-111, :199-201)
-    const float A_1 = copysignf(1.0f, c_1) * (1.0f - (1.0f - fabsf(c_1)) * flux_limiter(r_1, limiter, beta));
-    const float A_2 = copysignf(1.0f, c_2) * (1.0f - (1.0f - fabsf(c_2)) * flux_limiter(r_2, limiter, beta));
-    const float A_3 = copysignf(1.0f, c_3) * (1.0f - (1.0f - fabsf(c_3)) * flux_limiter(r_3, limiter, beta));
+template <class N>
+__device__ __forceinline__ void waf_flux(const WafCellT<N>& l2, const WafCellT<N>& l1, const WafCellT<N>& r1,
+                                         const WafCellT<N>& r2, N hd_l, N hd, N hd_r, N dtdx, N out[3],
+                                         int limiter = 0, float beta = 0.0f) {
+    const N h_l = l1.q[0], h_r = r1.q[0];
+    const N one = splat<N>(1.0f), half = splat<N>(0.5f);
+    const N q_l = vsel_gt(hd, h_l, vdiv(vsqrt(fmul(half, fmul(fadd(hd, h_l), hd))), h_l), one);
+    const N q_r = vsel_gt(hd, h_r, vdiv(vsqrt(fmul(half, fmul(fadd(hd, h_r), hd))), h_r), one);
+    const N S_l = ffma(vneg(l1.c), q_l, l1.u);
+    const N S_r = ffma(r1.c, q_r, r1.u);
+    const N a_r = fmul(h_r, fsub(r1.u, S_r));
+    const N a_l = fmul(h_l, fsub(l1.u, S_l));
+    const N S_star = vdiv(fsub(fmul(S_l, a_r), fmul(S_r, a_l)), fsub(a_r, a_l));
+    const N sl = vdiv(fmul(h_l, fsub(S_l, l1.u)), fsub(S_l, S_star));
+    const N sr = vdiv(fmul(h_r, fsub(S_r, r1.u)), fsub(S_r, S_star));
+    const N Qsl[3] = {sl, fmul(sl, S_star), fmul(sl, l1.v)};
+    const N Qsr[3] = {sr, fmul(sr, S_star), fmul(sr, r1.v)};
+    const N c_1 = fmul(S_l, dtdx);
+    const N c_2 = fmul(S_star, dtdx);
+    const N c_3 = fmul(S_r, dtdx);
+    const N A_1 = waf_weight(c_1, fsub(hd_l, l2.q[0]), fsub(hd_r, h_r), fsub(hd, h_l), limiter, beta);
+    const N A_2 = waf_weight(c_2, fsub(l1.v, l2.v), fsub(r2.v, r1.v), fsub(r1.v, l1.v), limiter, beta);
+    const N A_3 = waf_weight(c_3, fsub(h_l, hd_l), fsub(r2.q[0], hd_r), fsub(h_r, hd), limiter, beta);
 #pragma unroll
     for (int v = 0; v < 3; ++v) {
-        const float F1 = l1.f[v], F4 = r1.f[v];
-        const float F2 = fmaf(S_l, Qsl[v] - l1.q[v], F1);
-        const float F3 = fmaf(S_r, Qsr[v] - r1.q[v], F4);
-        const float wsum = fmaf(A_3, F4 - F3, fmaf(A_2, F3 - F2, A_1 * (F2 - F1)));
-        out[v] = fmaf(-0.5f, wsum, 0.5f * (F1 + F4));
+        const N F1 = l1.f[v], F4 = r1.f[v];
+        const N F2 = ffma(S_l, fsub(Qsl[v], l1.q[v]), F1);
+        const N F3 = ffma(S_r, fsub(Qsr[v], r1.q[v]), F4);
+        const N wsum = ffma(A_3, fsub(F4, F3), ffma(A_2, fsub(F3, F2), fmul(A_1, fsub(F2, F1))));
+        out[v] = ffma(splat<N>(-0.5f), wsum, fmul(half, fadd(F1, F4)));
     }
 }
 
@@ -624,10 +661,10 @@ __device__ __forceinline__ void swe_lxf_2d(const SweFace& l, const SweFace& r, f
 // Per-cell CFL time step (GPUSimulators/cuda/SWECommon.h:497-504; EulerCommon.h:42-49
 // with sqrt(gamma*rho)).
 __device__ __forceinline__ float cell_cfl(float h, float hu, float hv, float dx, float dy, float gg) {
-    const float rh = 1.0f / h;
-    const float c = sqrtf(gg * h);
-    const float max_u = dx / fmaf(fabsf(hu), fabsf(rh), c);
-    const float max_v = dy / fmaf(fabsf(hv), fabsf(rh), c);
+    const float rh = frcp_fast(h);
+    const float c = fsqrt_fast(fmul(gg, h));
+    const float max_u = fdiv_fast(dx, ffma(fabsf(hu), fabsf(rh), c));
+    const float max_v = fdiv_fast(dy, ffma(fabsf(hv), fabsf(rh), c));
     return fminf(max_u, max_v);
 }
 

@@ -95,6 +95,18 @@ __host__ __device__ inline long long cell_index(int y, int x, int pitch) {
     return (long long)(y + 2) * pitch + (x + 4);
 }
 
+// Split-scheme tiles: x-sweep segments per tile row and the shared-memory row
+// pitch (the TMA box width) of a W-wide tile.  A warp's x-sweep lanes cover
+// 32/NSEG rows x NSEG segments of W/NSEG cells; they hit 32 distinct banks
+// when the segment length is odd and the pitch is 4 (mod 32) for 4 segments,
+// 8 (mod 32) for 8.  W + 8 (4 halo columns each side) is 4 (mod 32) for the
+// 4-segment widths (124, 60, 28); 8-segment widths (120) load a box padded on
+// the right to the next pitch of 8 (mod 32).
+__host__ __device__ constexpr int split_nseg_x(int W) { return ((W / 4) % 2 == 1) ? 4 : 8; }
+__host__ __device__ constexpr int split_pitch(int W) {
+    return split_nseg_x(W) == 4 ? W + 8 : W + 8 + (((8 - (W + 8)) % 32) + 32) % 32;
+}
+
 struct StepCtl {
     float dt;      // step dt (before dt_scale)
     double t_new;  // t after this step
@@ -315,9 +327,9 @@ __device__ __forceinline__ float sign_y(int v) { return v == 2 ? -1.0f : 1.0f; }
 // wrapped cell from global memory, then reflective sides mirror interior cells
 // with the normal momentum negated, north, south, east, west in turn.
 // Dirichlet ghosts keep the stored values the TMA load brought in.
-template <int NV, int W, int H, int NT>
+template <int NV, int W, int H, int NT, int SP = W + 8>
 __device__ void apply_boundary(float* Qs, const TileJob& J) {
-    constexpr int SP = W + 8, TR = H + 4, PS = SP * TR;
+    constexpr int TR = H + 4, PS = SP * TR;
     const int nx = J.nx, ny = J.ny, bc = J.bc, x0 = J.x0, y0 = J.y0;
     const bool pw = bc_west(bc) == BC_PERIODIC, pe = bc_east(bc) == BC_PERIODIC;
     const bool ps = bc_south(bc) == BC_PERIODIC, pn = bc_north(bc) == BC_PERIODIC;
@@ -587,25 +599,25 @@ __device__ __forceinline__ void walk_2pt(float* line, int step, int a, int b, co
 
 // WAF walker (GPUSimulators/cuda/SWE2D_WAF.cu:35-87): the flux at c-1/2 uses
 // cells c-2 .. c+1; per-cell quantities and the star depths of neighbouring
-// pairs are carried along the window.
-template <bool SWAP, int PS, int LIM>
-__device__ __forceinline__ void walk_waf(float* line, int step, int a, int b, const float (&pre)[4][3], float g,
-                                         float half_g, float inv_g, float dtdx, float kdx, float beta) {
+// pairs are carried along the window.  N = f2 walks two lines d2 floats apart.
+template <bool SWAP, int PS, int LIM, class N>
+__device__ __forceinline__ void walk_waf(float* line, int step, int d2, int a, int b, const N (&pre)[4][3], N g,
+                                         N half_g, N inv_g, N dtdx, N kdx, float beta) {
     constexpr int limiter = LIM;
-    WafCell C0 = waf_cell(pre[0], g, half_g);
-    WafCell C1 = waf_cell(pre[1], g, half_g);
-    float q[3];
-    ld_cell<3, SWAP, PS>(line, a, step, q);
-    WafCell C2 = waf_cell(q, g, half_g);
-    ld_cell<3, SWAP, PS>(line, a + 1, step, q);
-    WafCell C3 = waf_cell(q, g, half_g);
-    float hs01 = waf_h_star(C0, C1, inv_g), hs12 = waf_h_star(C1, C2, inv_g), hs23 = waf_h_star(C2, C3, inv_g);
-    float Fprev[3];
+    WafCellT<N> C0 = waf_cell(pre[0], g, half_g);
+    WafCellT<N> C1 = waf_cell(pre[1], g, half_g);
+    N q[3];
+    ld_cell<3, SWAP, PS>(line, a, step, d2, q);
+    WafCellT<N> C2 = waf_cell(q, g, half_g);
+    ld_cell<3, SWAP, PS>(line, a + 1, step, d2, q);
+    WafCellT<N> C3 = waf_cell(q, g, half_g);
+    N hs01 = waf_h_star(C0, C1, inv_g), hs12 = waf_h_star(C1, C2, inv_g), hs23 = waf_h_star(C2, C3, inv_g);
+    N Fprev[3];
     waf_flux(C0, C1, C2, C3, hs01, hs12, hs23, dtdx, Fprev, limiter, beta);  // face a-1/2
 #pragma unroll 4
     for (int c = a + 1; c <= b; ++c) {
         if (c + 1 < b) {
-            ld_cell<3, SWAP, PS>(line, c + 1, step, q);
+            ld_cell<3, SWAP, PS>(line, c + 1, step, d2, q);
         } else {
             // a select, not pre[k]: a run-time index would put pre in local memory
             const bool first = (c + 1 == b);
@@ -619,23 +631,33 @@ __device__ __forceinline__ void walk_waf(float* line, int step, int a, int b, co
         hs01 = hs12;
         hs12 = hs23;
         hs23 = waf_h_star(C2, C3, inv_g);
-        float F[3];
+        N F[3];
         waf_flux(C0, C1, C2, C3, hs01, hs12, hs23, dtdx, F, limiter, beta);  // face c-1/2
-        float out[3];
+        N out[3];
 #pragma unroll
-        for (int v = 0; v < 3; ++v) out[v] = fmaf(Fprev[v] - F[v], kdx, C1.q[v]);
-        st_cell<3, SWAP, PS>(line, c - 1, step, out);
+        for (int v = 0; v < 3; ++v) out[v] = ffma(fsub(Fprev[v], F[v]), kdx, C1.q[v]);
+        st_cell<3, SWAP, PS>(line, c - 1, step, d2, out);
 #pragma unroll
         for (int v = 0; v < 3; ++v) Fprev[v] = F[v];
     }
 }
 
-// Per-scheme parameters of one sweep direction.
+// Per-scheme parameters of one sweep direction.  The ratios of the time step
+// to the cell size are formed once per sweep, here, for every walker (one
+// line or two lines per thread), so each tile configuration uses the same
+// bits.
 struct SweepPar {
     float theta, g, half_g, inv_g, gamma;
     float kdt;   // kernel dt
     float dxx;   // cell size along the sweep
+    float kdx;   // kdt / dxx
+    float k2;    // kdt / (2 dxx)
     float beta;   // parameter of the Osher and Sweby limiters
+    __device__ __forceinline__ void set_direction(float cell) {
+        dxx = cell;
+        kdx = fdiv_fast(kdt, cell);
+        k2 = fmul(kdx, 0.5f);
+    }
 };
 
 // VAR: HLL's flux variant or WAF's limiter (walk_2pt, flux_limiter); 0 is the
@@ -643,36 +665,39 @@ struct SweepPar {
 template <int SCHEME, bool SWAP, int PS, int VAR>
 __device__ __forceinline__ void walk_line(float* line, int step, int a, int b, const float (&pre)[4][(SCHEME == EE2D) ? 4 : 3],
                                           const SweepPar& p) {
-    const float kdx = p.kdt / p.dxx;
+    const float kdx = p.kdx;
     if constexpr (SCHEME == KP07_DIMSPLIT || SCHEME == HLL2) {
-        const SwePhys<float> P{2.0f * p.theta, p.g, p.half_g, p.kdt / (2.0f * p.dxx)};
+        const SwePhys<float> P{2.0f * p.theta, p.g, p.half_g, p.k2};
         walk_mh<SwePhys<float>, SCHEME == HLL2, SWAP, PS>(line, step, 0, a, b, pre, P, kdx);
     } else if constexpr (SCHEME == EE2D) {
-        const EulerPhys<float> P{2.0f * p.theta, p.gamma, p.gamma - 1.0f, p.kdt / (2.0f * p.dxx)};
+        const EulerPhys<float> P{2.0f * p.theta, p.gamma, fsub(p.gamma, 1.0f), p.k2};
         // x sweeps use HLL, y sweeps central-upwind (GPUSimulators/cuda/EE2D_KP07_dimsplit.cu:62, :106)
         walk_mh<EulerPhys<float>, !SWAP, SWAP, PS>(line, step, 0, a, b, pre, P, kdx);
     } else if constexpr (SCHEME == WAF) {
-        walk_waf<SWAP, PS, VAR>(line, step, a, b, pre, p.g, p.half_g, p.inv_g, kdx, kdx, p.beta);
+        walk_waf<SWAP, PS, VAR>(line, step, 0, a, b, pre, p.g, p.half_g, p.inv_g, kdx, kdx, p.beta);
     } else {
-        walk_2pt<SCHEME, SWAP, PS, VAR>(line, step, a, b, pre, p.g, p.half_g, p.dxx / (2.0f * p.kdt),
-                                        p.kdt / (2.0f * p.dxx), kdx);
+        walk_2pt<SCHEME, SWAP, PS, VAR>(line, step, a, b, pre, p.g, p.half_g, fdiv_fast(p.dxx, fmul(2.0f, p.kdt)),
+                                        p.k2, kdx);
     }
 }
 
 // Two lines, d2 floats apart, walked side by side in packed arithmetic
 // (the MUSCL-Hancock schemes).  Each cell gets the same bits as walk_line.
-template <int SCHEME, bool SWAP, int PS>
+template <int SCHEME, bool SWAP, int PS, int VAR>
 __device__ __forceinline__ void walk_line2(float* line, int step, int d2, int a, int b,
                                            const f2 (&pre)[4][(SCHEME == EE2D) ? 4 : 3], const SweepPar& p) {
-    static_assert(SCHEME == KP07_DIMSPLIT || SCHEME == HLL2 || SCHEME == EE2D, "packed walkers: MUSCL-Hancock only");
-    const f2 kdx = splat<f2>(p.kdt / p.dxx);
-    if constexpr (SCHEME == EE2D) {
-        const EulerPhys<f2> P{splat<f2>(2.0f * p.theta), splat<f2>(p.gamma), splat<f2>(p.gamma - 1.0f),
-                              splat<f2>(p.kdt / (2.0f * p.dxx))};
+    static_assert(SCHEME == KP07_DIMSPLIT || SCHEME == HLL2 || SCHEME == EE2D || SCHEME == WAF,
+                  "packed walkers: MUSCL-Hancock schemes and WAF");
+    const f2 kdx = splat<f2>(p.kdx);
+    if constexpr (SCHEME == WAF) {
+        walk_waf<SWAP, PS, VAR>(line, step, d2, a, b, pre, splat<f2>(p.g), splat<f2>(p.half_g), splat<f2>(p.inv_g),
+                                kdx, kdx, p.beta);
+    } else if constexpr (SCHEME == EE2D) {
+        const EulerPhys<f2> P{splat<f2>(2.0f * p.theta), splat<f2>(p.gamma), splat<f2>(fsub(p.gamma, 1.0f)),
+                              splat<f2>(p.k2)};
         walk_mh<EulerPhys<f2>, !SWAP, SWAP, PS>(line, step, d2, a, b, pre, P, kdx);
     } else {
-        const SwePhys<f2> P{splat<f2>(2.0f * p.theta), splat<f2>(p.g), splat<f2>(p.half_g),
-                            splat<f2>(p.kdt / (2.0f * p.dxx))};
+        const SwePhys<f2> P{splat<f2>(2.0f * p.theta), splat<f2>(p.g), splat<f2>(p.half_g), splat<f2>(p.k2)};
         walk_mh<SwePhys<f2>, SCHEME == HLL2, SWAP, PS>(line, step, d2, a, b, pre, P, kdx);
     }
 }
@@ -681,7 +706,7 @@ __device__ __forceinline__ void walk_line2(float* line, int step, int d2, int a,
 // LPT = 2: a thread walks rows t and t + (t1 - t0)/2 side by side.
 template <int SCHEME, int NV, int W, int H, int NT, int VAR, int LPT>
 __device__ __forceinline__ void sweep_x(float* Qs, int t0, int t1, const SweepPar& p) {
-    constexpr int SP = W + 8, PS = SP * (H + 4), NSEG = 4, R = W / NSEG;
+    constexpr int SP = split_pitch(W), PS = SP * (H + 4), NSEG = split_nseg_x(W), R = W / NSEG;
     const int item = threadIdx.x;
     const int nlines = (t1 - t0) / LPT;
     const bool has = item < nlines * NSEG;
@@ -708,7 +733,7 @@ __device__ __forceinline__ void sweep_x(float* Qs, int t0, int t1, const SweepPa
             ld_cell<NV, false, PS>(line, b + 1, 1, d2, pre[3]);
         }
         __syncthreads();
-        if (has) walk_line2<SCHEME, false, PS>(line, 1, d2, a, b, pre, p);
+        if (has) walk_line2<SCHEME, false, PS, VAR>(line, 1, d2, a, b, pre, p);
     }
     __syncthreads();
 }
@@ -717,7 +742,7 @@ __device__ __forceinline__ void sweep_x(float* Qs, int t0, int t1, const SweepPa
 // LPT = 2: a thread walks columns s and s + (s1 - s0)/2 side by side.
 template <int SCHEME, int NV, int W, int H, int NT, int VAR, int LPT>
 __device__ __forceinline__ void sweep_y(float* Qs, int s0, int s1, const SweepPar& p) {
-    constexpr int SP = W + 8, PS = SP * (H + 4);
+    constexpr int SP = split_pitch(W), PS = SP * (H + 4);
     constexpr int NSEG = NT * LPT / (W + 4), R = H / NSEG;
     const int ncols = (s1 - s0) / LPT;
     const int item = threadIdx.x;
@@ -745,7 +770,7 @@ __device__ __forceinline__ void sweep_y(float* Qs, int s0, int s1, const SweepPa
             ld_cell<NV, true, PS>(line, b + 1, SP, d2, pre[3]);
         }
         __syncthreads();
-        if (has) walk_line2<SCHEME, true, PS>(line, SP, d2, a, b, pre, p);
+        if (has) walk_line2<SCHEME, true, PS, VAR>(line, SP, d2, a, b, pre, p);
     }
     __syncthreads();
 }
@@ -773,34 +798,36 @@ __device__ bool process_tile_dimsplit(float* Qs, uint64_t* bar, uint32_t phase, 
                                       bool health = false, bool* unhealthy = nullptr) {
     constexpr int NV = (SCHEME == EE2D) ? 4 : 3;
     constexpr int G = (SCHEME == FORCE || SCHEME == HLL) ? 1 : 2;
-    constexpr int SP = W + 8, TR = H + 4, PS = SP * TR;
-    static_assert(W % 4 == 0 && (W / 4) % 2 == 1, "row segments must be odd for conflict-free x sweeps");
-    static_assert(TR * 4 <= NT * LPT, "one x-sweep segment (LPT lines) per thread");
-    static_assert((NT * LPT) % (W + 4) == 0 && H % ((NT * LPT) / (W + 4)) == 0, "y-sweep segments must tile the block");
-    static_assert(LPT == 1 || (LPT == 2 && H % 2 == 0 && (SCHEME == KP07_DIMSPLIT || SCHEME == HLL2 || SCHEME == EE2D)),
-                  "two lines per thread: MUSCL-Hancock schemes with an even number of tile rows");
+    constexpr int SP = split_pitch(W), TR = H + 4, PS = SP * TR, NSEG_X = split_nseg_x(W);
+    static_assert(W % NSEG_X == 0 && (W / NSEG_X) % 2 == 1 && SP % 32 == (NSEG_X == 4 ? 4 : 8),
+                  "row segments must be odd and the pitch 4 (8) mod 32 for conflict-free x sweeps");
+    static_assert(TR * NSEG_X <= NT * LPT, "one x-sweep segment (LPT lines) per thread");
+    static_assert((NT * LPT) / (W + 4) >= 1 && H % ((NT * LPT) / (W + 4)) == 0, "y-sweep segments must tile the block");
+    static_assert(LPT == 1 || (LPT == 2 && H % 2 == 0 &&
+                               (SCHEME == KP07_DIMSPLIT || SCHEME == HLL2 || SCHEME == EE2D || SCHEME == WAF)),
+                  "two lines per thread: MUSCL-Hancock schemes and WAF, with an even number of tile rows");
     if (!load_tile<NV, SP, TR, GLOBAL_TMAP>(Qs, J.tmap, J.x0, J.y0, bar, phase, init_bar, err, polls)) return false;
     const int x0 = J.x0, y0 = J.y0;
-    if (x0 == 0 || x0 + W + 2 > J.nx || y0 == 0 || y0 + H + 2 > J.ny) apply_boundary<NV, W, H, NT>(Qs, J);
+    if (x0 == 0 || x0 + W + 2 > J.nx || y0 == 0 || y0 + H + 2 > J.ny) apply_boundary<NV, W, H, NT, SP>(Qs, J);
 
     SweepPar p;
     p.theta = P.theta;
     p.g = P.g;
-    p.half_g = 0.5f * P.g;
-    p.inv_g = 1.0f / P.g;
+    p.half_g = fmul(0.5f, P.g);
+    p.inv_g = frcp_fast(P.g);
     p.gamma = P.gamma;
     p.kdt = P.kdt;
     p.beta = P.beta;
     const bool x_first = (SCHEME == FORCE || SCHEME == HLL) ? true : (P.substep == 0);
     if (x_first) {
-        p.dxx = P.dx;
+        p.set_direction(P.dx);
         sweep_x<SCHEME, NV, W, H, NT, VAR, LPT>(Qs, 2 - G, H + 2 + G, p);
-        p.dxx = P.dy;
+        p.set_direction(P.dy);
         sweep_y<SCHEME, NV, W, H, NT, VAR, LPT>(Qs, 4, W + 4, p);
     } else {
-        p.dxx = P.dy;
+        p.set_direction(P.dy);
         sweep_y<SCHEME, NV, W, H, NT, VAR, LPT>(Qs, 4 - G, W + 4 + G, p);
-        p.dxx = P.dx;
+        p.set_direction(P.dx);
         sweep_x<SCHEME, NV, W, H, NT, VAR, LPT>(Qs, 2, H + 2, p);
     }
 
