@@ -59,6 +59,10 @@ ALG_OPS_PER_CELL_LAUNCH = {
 # reference formulation's operations.  Packing two lines per instruction
 # (f32x2) does the same operations in fewer instructions.
 EXECUTED_FLOP_PER_CELL_LAUNCH = {"KP07_dimsplit": 215.0, "HLL2": 233.0, "WAF": 354.0, "KP07": 172.0}
+# The same counts as FP32 pipe operations (fadd + fmul + ffma per cell and
+# launch, one FMA-pipe lane slot each): an add or a multiply occupies a lane
+# as long as an FMA does, so these, not the FLOPs, set the FP32 pipe's floor.
+FP32_PIPE_OPS_PER_CELL_LAUNCH = {"KP07_dimsplit": 159.0, "HLL2": 171.0, "WAF": 308.0, "KP07": 138.0}
 FP32_LANES_PER_SM = 128  # FP32 FMA lanes per Blackwell SM
 PROFILE_JSON = os.path.join(ROOT, "profiles", "kp07_dimsplit_stage_4096.json")
 
@@ -624,7 +628,16 @@ def run_mine(args, rank, world, local_rank):
         roof_fp32["executed_inst_per_cell_launch"] = prof["executed_inst_per_cell_substep"]
     t_hbm = alg_bytes / (pk["hbm_gbs"] * 1e9)
     t_fp32 = (own_flop or ref_flop) / (fp32_peak * 1e12)
-    roof["binding"] = "fp32" if t_fp32 > t_hbm else "hbm"
+    pipe_ops = FP32_PIPE_OPS_PER_CELL_LAUNCH.get(scheme)
+    if pipe_ops:
+        # FP32 lanes x clock: the pipe's operation rate (half the FLOP peak)
+        t_pipe = pipe_ops * cells / (fp32_peak * 1e12 / 2.0)
+        roof_fp32["pipe"] = {"fp32_ops_per_cell_launch": pipe_ops, "floor_us_per_launch": t_pipe * 1e6,
+                             "frac": t_pipe / launch_s,
+                             "what": "fadd + fmul + ffma lane operations (ncu sass counters) on 128 FP32 lanes "
+                                     "per SM at the maximum SM clock"}
+        t_fp32 = max(t_fp32, t_pipe)
+    roof["binding"] = "fp32_pipe" if t_fp32 > t_hbm else "hbm"
     roof["frac_of_binding"] = max(t_hbm, t_fp32) / launch_s
 
     result = None

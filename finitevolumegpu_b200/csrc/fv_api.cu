@@ -13,6 +13,7 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
+#include <atomic>
 #include <condition_variable>
 #include <cmath>
 #include <cstdarg>
@@ -402,11 +403,11 @@ void fv_internal_set_error(const char* msg) { g_err = msg; }
 // copies of different threads proceed in parallel), waits for the slot's
 // previous copy (its event) and releases the slot when done.
 struct HostStaging {
-    static constexpr int kSlots = 4;
-    void* ptr[kSlots] = {nullptr, nullptr, nullptr, nullptr};
-    size_t cap[kSlots] = {0, 0, 0, 0};
-    cudaEvent_t ev[kSlots] = {nullptr, nullptr, nullptr, nullptr};
-    bool busy[kSlots] = {false, false, false, false};
+    static constexpr int kSlots = 8;
+    void* ptr[kSlots] = {};
+    size_t cap[kSlots] = {};
+    cudaEvent_t ev[kSlots] = {};
+    bool busy[kSlots] = {};
     int next = 0;
     std::mutex mu;
     std::condition_variable freed;
@@ -494,8 +495,14 @@ bool is_pinned(const void* p) {
     return a.type == cudaMemoryTypeHost;
 }
 
+// Host copies in progress (all contexts): copy_rows shares 8 helper threads
+// among them, so that several host threads copying at once (admissions and
+// returns of a served stream) do not oversubscribe the cores.
+std::atomic<int> g_active_copies{0};
+
 // rows x width bytes from src (row stride spitch) to dst (row stride dpitch),
-// split across up to 8 threads (one per 512 KB) for copies of 1 MB and more.
+// split across up to 8 threads (one per 512 KB) for copies of 1 MB and more,
+// fewer while other copies run.
 void copy_rows(char* dst, size_t dpitch, const char* src, size_t spitch, size_t width, size_t rows) {
     auto work = [=](size_t r0, size_t r1) {
         if (dpitch == width && spitch == width) {
@@ -506,7 +513,12 @@ void copy_rows(char* dst, size_t dpitch, const char* src, size_t spitch, size_t 
     };
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
     const size_t bytes = width * rows;
-    const size_t nt = (bytes >= (1u << 20)) ? std::min<size_t>({8, hw, rows, bytes >> 19}) : 1;
+    const int active = g_active_copies.fetch_add(1) + 1;
+    struct Leave {
+        ~Leave() { g_active_copies.fetch_sub(1); }
+    } leave;
+    const size_t share = std::max<size_t>(1, 8 / (size_t)active);
+    const size_t nt = (bytes >= (1u << 20)) ? std::min<size_t>({share, hw, rows, bytes >> 19}) : 1;
     if (nt <= 1) {
         work(0, rows);
         return;
@@ -1314,6 +1326,7 @@ int batch_launch_step(fv_batch* b) {
     for (int i = 0; i < b->num_substeps; ++i) {
         fv::BatchArgs a;
         a.inst = b->d_inst;
+        a.ctl = b->d_ctl;
         a.work = b->d_work;
         a.nwork = b->d_nwork;
         a.substep = i;

@@ -136,6 +136,16 @@ struct __align__(8) f2 {
 __device__ __forceinline__ uint64_t& u64(f2& a) { return reinterpret_cast<uint64_t&>(a); }
 __device__ __forceinline__ const uint64_t& u64(const f2& a) { return reinterpret_cast<const uint64_t&>(a); }
 
+// The packed multiply is an FMA with a -0.0 addend read from constant memory
+// (a*b + -0 is a*b exactly, signed zeros included).  A plain packed multiply
+// whose product feeds a packed add or subtract may be fused with it into one
+// FMA by the assembler (round-to-nearest modifiers notwithstanding), which
+// rounds once instead of twice; measured on a B200, that made two-line walkers
+// differ from one-line ones in the last bits.  An FMA result cannot be fused
+// further, and the addend's value is not known at compile time, so the
+// multiply stays a separate, correctly rounded operation as in the scalar code.
+static __constant__ float kOpaqueNegZero = -0.0f;
+
 __device__ __forceinline__ f2 fadd(f2 a, f2 b) {
     f2 d;
     asm("add.rn.ftz.f32x2 %0, %1, %2;" : "=l"(u64(d)) : "l"(u64(a)), "l"(u64(b)));
@@ -146,16 +156,12 @@ __device__ __forceinline__ f2 fsub(f2 a, f2 b) {
     asm("sub.rn.ftz.f32x2 %0, %1, %2;" : "=l"(u64(d)) : "l"(u64(a)), "l"(u64(b)));
     return d;
 }
-__device__ __forceinline__ f2 fmul(f2 a, f2 b) {
-    f2 d;
-    asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(u64(d)) : "l"(u64(a)), "l"(u64(b)));
-    return d;
-}
 __device__ __forceinline__ f2 ffma(f2 a, f2 b, f2 c) {
     f2 d;
     asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(u64(d)) : "l"(u64(a)), "l"(u64(b)), "l"(u64(c)));
     return d;
 }
+__device__ __forceinline__ f2 fmul(f2 a, f2 b) { return ffma(a, b, f2{kOpaqueNegZero, kOpaqueNegZero}); }
 
 // A scalar constant in the number type of a computation (both lanes for f2).
 template <class N> __device__ __forceinline__ N splat(float a);
@@ -168,16 +174,15 @@ template <> __device__ __forceinline__ f2 splat<f2>(float a) { return f2{a, a}; 
 // per call site (fast math lets it turn a / b into a * (1 / b) where it
 // shares a reciprocal), which would round a cell differently depending on
 // the kernel that inlines the formula.
-__device__ __forceinline__ float fdiv_fast(float a, float b) {
-    float d;
-    asm("div.full.ftz.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
-    return d;
-}
 __device__ __forceinline__ float frcp_fast(float a) {
     float d;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(d) : "f"(a));
     return d;
 }
+// a * (1 / b) with the approximate reciprocal: bit for bit the fast-math
+// quotient for divisors below 2^126 (checked on a B200), and two
+// instructions, of which the multiply can be packed.
+__device__ __forceinline__ float fdiv_fast(float a, float b) { return fmul(a, frcp_fast(b)); }
 __device__ __forceinline__ float fsqrt_fast(float a) {
     float d;
     asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(d) : "f"(a));
@@ -188,7 +193,7 @@ __device__ __forceinline__ float fsqrt_fast(float a) {
 __device__ __forceinline__ float vneg(float a) { return -a; }
 __device__ __forceinline__ f2 vneg(f2 a) { return f2{-a.x, -a.y}; }
 __device__ __forceinline__ float vdiv(float a, float b) { return fdiv_fast(a, b); }
-__device__ __forceinline__ f2 vdiv(f2 a, f2 b) { return f2{fdiv_fast(a.x, b.x), fdiv_fast(a.y, b.y)}; }
+__device__ __forceinline__ f2 vdiv(f2 a, f2 b) { return fmul(a, f2{frcp_fast(b.x), frcp_fast(b.y)}); }
 __device__ __forceinline__ float vrcp(float a) { return frcp_fast(a); }
 __device__ __forceinline__ f2 vrcp(f2 a) { return f2{frcp_fast(a.x), frcp_fast(a.y)}; }
 __device__ __forceinline__ float vsqrt(float a) { return fsqrt_fast(a); }

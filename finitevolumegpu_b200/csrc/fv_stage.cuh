@@ -952,6 +952,7 @@ struct alignas(64) BatchInstance {
 
 struct BatchArgs {
     const BatchInstance* inst;
+    SimCtl* ctl;          // control blocks, one per instance: inst[i].ctl == ctl + i
     const int2* work;     // (instance, tile within instance) per work item
     const int* nwork;     // number of work items (device scalar, updated between graph replays)
     int substep;
@@ -976,11 +977,22 @@ __global__ void __launch_bounds__(NT) batched_stage_kernel(const __grid_constant
     const int n = *B.nwork;
     uint32_t phase = 0;
     bool init = true;
-    for (int w = blockIdx.x; w < n; w += gridDim.x) {
-        const int2 job = B.work[w];
+    // Tile prologue latency: the next work item is fetched a tile ahead, and
+    // a simulation's control block is addressed from its index (not through
+    // its instance record), so the control-block and instance loads of a
+    // tile issue together instead of one after the other.
+    int w = blockIdx.x;
+    int2 job = (w < n) ? B.work[w] : make_int2(0, 0);
+    for (; w < n; w += gridDim.x) {
+        const int wn = w + gridDim.x;
+        const int2 next = (wn < n) ? B.work[wn] : job;
         const BatchInstance& I = B.inst[job.x];
-        StepCtl sc = read_step(I.ctl, false, 0.0f, false, B.is_last != 0);
-        if (!sc.active) continue;  // uniform across the CTA
+        SimCtl* const ctl = B.ctl + job.x;
+        StepCtl sc = read_step(ctl, false, 0.0f, false, B.is_last != 0);
+        if (!sc.active) {  // uniform across the CTA
+            job = next;
+            continue;
+        }
         if (SCHEME == WAF) sc.do_cfl = false;
         float my_cfl = __int_as_float(0x7f800000);
         double my_sums[NV];
@@ -1004,11 +1016,12 @@ __global__ void __launch_bounds__(NT) batched_stage_kernel(const __grid_constant
                                                                       B.err, my_cfl, my_sums, kWaitPolls,
                                                                       B.is_last != 0, &unhealthy);
         // ordered before this tile's arrival (tile_epilogue fences before it counts)
-        if (__syncthreads_or(unhealthy) && threadIdx.x == 0) atomicOr(&I.ctl->bad, 1);
+        if (__syncthreads_or(unhealthy) && threadIdx.x == 0) atomicOr(&ctl->bad, 1);
         init = false;
         phase ^= 1u;
-        tile_epilogue<NT, NV>(I.ctl, I.block_cfl, I.block_sums, job.y, I.ntiles, B.is_last != 0, false, sc, my_cfl,
+        tile_epilogue<NT, NV>(ctl, I.block_cfl, I.block_sums, job.y, I.ntiles, B.is_last != 0, false, sc, my_cfl,
                               my_sums, sums);
+        job = next;
     }
 }
 
