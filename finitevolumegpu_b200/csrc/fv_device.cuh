@@ -72,7 +72,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase,
     return false;
 }
 
-// 2-D tiled TMA load (no multicast) of one box into shared memory, completing
+// 2-D tiled TMA load of one box into this CTA's shared memory, completing
 // on `bar`.  x must be a multiple of 4 (16-byte rule for FP32).
 __device__ __forceinline__ void tma_load_2d(void* dst, const void* tmap, int x, int y, uint64_t* bar) {
     asm volatile(

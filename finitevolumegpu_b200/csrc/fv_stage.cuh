@@ -3,8 +3,9 @@
 // GPUSimulators/cuda/SWE2D_KP07_dimsplit.cu:123-205).
 //
 // Tile: a CTA owns W x H interior cells.  One TMA box per variable brings the
-// tile plus a 4-column / 2-row halo into shared memory ((H+4) x (W+8) floats,
-// box x aligned to 4 floats).  Ghost cells are then completed in shared memory
+// tile plus a 4-column / 2-row halo into shared memory ((H+4) x P floats with
+// row pitch P = W+8, or wider for 8-segment tiles, split_pitch; box x aligned
+// to 4 floats).  Ghost cells are then completed in shared memory
 // (periodic wrap from global memory, reflective mirror in the reference's
 // N, S, E, W order), the sweeps run in place, and the interior is written back
 // with 128-bit stores.  The CFL minimum and the FP64 conservation sums are
@@ -14,9 +15,12 @@
 //
 // Sweep mapping:
 //   x sweeps: a thread walks one row segment of W/4 cells (lanes = 8 rows x
-//     4 segments).  With a shared row pitch of W+8 = 4 (mod 32) floats and
-//     W/4 = -1 (mod 32) the 32 lanes hit 32 distinct banks.
+//     4 segments; or W/8 cells, lanes = 4 rows x 8 segments).  With a shared
+//     row pitch of 4 (8) mod 32 floats and an odd segment length the 32
+//     lanes hit 32 distinct banks.
 //   y sweeps: a thread walks one column segment (lanes = consecutive columns).
+//   LPT = 2: a thread walks two lines side by side in packed f32x2
+//     arithmetic (rows t and t + n/2, columns s and s + n/2).
 // Each thread keeps a 3-cell window in registers and reconstructs every cell
 // once; the halo cells of its segment are read before a barrier so that
 // in-place updates by neighbouring segments cannot race with them.
