@@ -637,7 +637,10 @@ def run_mine(args, rank, world, local_rank):
                              "what": "fadd + fmul + ffma lane operations (ncu sass counters) on 128 FP32 lanes "
                                      "per SM at the maximum SM clock"}
         t_fp32 = max(t_fp32, t_pipe)
-    roof["binding"] = "fp32_pipe" if t_fp32 > t_hbm else "hbm"
+    if t_fp32 > t_hbm:
+        roof["binding"] = "fp32_pipe" if pipe_ops else ("fp32_flop" if own_flop else "fp32_flop_reference_formulation")
+    else:
+        roof["binding"] = "hbm"
     roof["frac_of_binding"] = max(t_hbm, t_fp32) / launch_s
 
     result = None
