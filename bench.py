@@ -58,11 +58,13 @@ ALG_OPS_PER_CELL_LAUNCH = {
 # sweep and each face flux computed once, so the kernels need half the
 # reference formulation's operations.  Packing two lines per instruction
 # (f32x2) does the same operations in fewer instructions.
-EXECUTED_FLOP_PER_CELL_LAUNCH = {"KP07_dimsplit": 215.0, "HLL2": 233.0, "WAF": 354.0, "KP07": 172.0}
+EXECUTED_FLOP_PER_CELL_LAUNCH = {"LxF": 66.0, "FORCE": 118.0, "HLL": 130.0, "HLL2": 233.0, "WAF": 354.0,
+                                 "KP07": 172.0, "KP07_dimsplit": 215.0, "EE2D_KP07_dimsplit": 321.0}
 # The same counts as FP32 pipe operations (fadd + fmul + ffma per cell and
 # launch, one FMA-pipe lane slot each): an add or a multiply occupies a lane
 # as long as an FMA does, so these, not the FLOPs, set the FP32 pipe's floor.
-FP32_PIPE_OPS_PER_CELL_LAUNCH = {"KP07_dimsplit": 159.0, "HLL2": 171.0, "WAF": 308.0, "KP07": 138.0}
+FP32_PIPE_OPS_PER_CELL_LAUNCH = {"LxF": 54.0, "FORCE": 95.0, "HLL": 105.0, "HLL2": 171.0, "WAF": 308.0,
+                                 "KP07": 138.0, "KP07_dimsplit": 159.0, "EE2D_KP07_dimsplit": 235.0}
 FP32_LANES_PER_SM = 128  # FP32 FMA lanes per Blackwell SM
 PROFILE_JSON = os.path.join(ROOT, "profiles", "kp07_dimsplit_stage_4096.json")
 
