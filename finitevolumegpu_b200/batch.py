@@ -105,12 +105,19 @@ class Batch(object):
         # a non-positive depth (density), or t/dt is not a number
         return {"t": t.value, "nt": nt.value, "dt": dt.value, "done": bool(done.value), "failed": done.value == 2}
 
-    def download(self, slot):
+    def download(self, slot, scratch=None):
+        """The simulation's state as (ny, nx) float32 arrays.  With `scratch` (a
+        float32 array of at least nv * ny * nx elements, e.g. reused by a
+        thread) the arrays are views into it: no fresh host memory to fault in,
+        valid until the scratch is reused."""
         with self._shapes_lock:
             ny, nx = self.shapes[slot]
         out = []
         for v in range(self.nv):
-            a = np.empty((ny, nx), dtype=np.float32)
+            if scratch is None:
+                a = np.empty((ny, nx), dtype=np.float32)
+            else:
+                a = scratch[v * ny * nx:(v + 1) * ny * nx].reshape(ny, nx)
             _lib.check(_L().fv_batch_download(self._h, int(slot), v, a.ctypes.data_as(_lib._FP), nx))
             out.append(a)
         return out

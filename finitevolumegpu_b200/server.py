@@ -138,9 +138,10 @@ class Server(object):
 
         Every request comes back as one Result: "done" with its state
         (``result_fn(request, arrays)`` if given, on a return thread, e.g. to
-        keep a checksum instead of the arrays), or "rejected" / "failed" with
-        the reason (see the module docstring).  Returns (results, stats);
-        the stats count and time the done requests.
+        keep a checksum instead of the arrays; the arrays it receives live in
+        a buffer the thread reuses, so it copies what it keeps), or
+        "rejected" / "failed" with the reason (see the module docstring).
+        Returns (results, stats); the stats count and time the done requests.
         """
         pending = collections.deque()
         running = {}  # (batch key, slot) -> (request, admitted, bytes): on the GPU, not yet at t_end
@@ -166,6 +167,7 @@ class Server(object):
                 pending.append(r)
 
         def return_finished():
+            scratch = np.empty(0, dtype=np.float32)  # this thread's download buffer when result_fn reduces
             while True:
                 item = returns.get()
                 if item is None:
@@ -176,7 +178,13 @@ class Server(object):
                 try:
                     b = self.batches[bk]
                     st = b.status(slot)
-                    state = b.download(slot)
+                    if result_fn is not None:
+                        n = b.nv * r.nx * r.ny
+                        if scratch.size < n:
+                            scratch = np.empty(n, dtype=np.float32)
+                        state = b.download(slot, scratch)
+                    else:
+                        state = b.download(slot)
                     b.remove(slot)
                     if result_fn is not None:
                         state = result_fn(r, state)

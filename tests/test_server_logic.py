@@ -63,7 +63,9 @@ class FakeBatch(object):
             bad = bool(st.get("bad"))
             return {"t": st["t"], "nt": st["nt"], "dt": 1.0, "done": bad or st["t"] >= st["t_end"], "failed": bad}
 
-    def download(self, slot):
+    nv = 3
+
+    def download(self, slot, scratch=None):
         with self.lock:
             st = self.slots[slot]
             return [np.full((2, 2), st["rid"], dtype=np.float32)]
