@@ -32,12 +32,12 @@ import numpy as np
 
 # Number of tile configurations per scheme in libfvgpu's kernel table.
 TILE_CONFIGS = {
-    "KP07_dimsplit": 9,
-    "HLL2": 9,
-    "WAF": 9,
+    "KP07_dimsplit": 11,
+    "HLL2": 11,
+    "WAF": 11,
     "FORCE": 4,
     "HLL": 4,
-    "EE2D_KP07_dimsplit": 8,
+    "EE2D_KP07_dimsplit": 10,
     "LxF": 4,
     "KP07": 4,
 }

@@ -123,6 +123,15 @@ const KEntry kTable[] = {
     {FV_EE2D_KP07_DIMSPLIT, 120, 28, 128, true, fv::dimsplit_stage_kernel<fv::EE2D, 120, 28, 128, 0, 2>},
     {FV_WAF, 120, 28, 128, true, fv::dimsplit_stage_kernel<fv::WAF, 120, 28, 128, 0, 2>},
     {FV_WAF, 120, 60, 256, true, fv::dimsplit_stage_kernel<fv::WAF, 120, 60, 256, 0, 2>},
+    // 60 x 60: fewer halo rows per tile than 60 x 28 at the same warps per SM
+    {FV_KP07_DIMSPLIT, 60, 60, 128, true, fv::dimsplit_stage_kernel<fv::KP07_DIMSPLIT, 60, 60, 128, 0, 2>},
+    {FV_KP07_DIMSPLIT, 60, 60, 256, true, fv::dimsplit_stage_kernel<fv::KP07_DIMSPLIT, 60, 60, 256, 0, 1>},
+    {FV_HLL2, 60, 60, 128, true, fv::dimsplit_stage_kernel<fv::HLL2, 60, 60, 128, 0, 2>},
+    {FV_HLL2, 60, 60, 256, true, fv::dimsplit_stage_kernel<fv::HLL2, 60, 60, 256, 0, 1>},
+    {FV_EE2D_KP07_DIMSPLIT, 60, 60, 128, true, fv::dimsplit_stage_kernel<fv::EE2D, 60, 60, 128, 0, 2>},
+    {FV_EE2D_KP07_DIMSPLIT, 60, 60, 256, true, fv::dimsplit_stage_kernel<fv::EE2D, 60, 60, 256, 0, 1>},
+    {FV_WAF, 60, 60, 128, true, fv::dimsplit_stage_kernel<fv::WAF, 60, 60, 128, 0, 2>},
+    {FV_WAF, 60, 60, 256, true, fv::dimsplit_stage_kernel<fv::WAF, 60, 60, 256, 0, 1>},
 };
 constexpr int kNumEntries = sizeof(kTable) / sizeof(kTable[0]);
 
