@@ -101,8 +101,14 @@ def state_bytes(scheme, nx, ny, tile_w=60, tile_h=28):
 
 class Server(object):
     def __init__(self, context, budget_bytes=120e9, chunk_steps=8, max_instances=4096, schemes=None,
-                 cfl_scale=0.9, return_threads=3, admit_threads=3):
+                 cfl_scale=0.9, return_threads=3, admit_threads=3, max_running=256):
+        """max_running: scenarios held at once (on the GPU, being uploaded or
+        waiting to be returned).  Past
+        the server's capacity the extra arrivals wait to be admitted instead of
+        all sharing the GPU: each chunk then stays short, the admitted scenarios
+        finish at the device's rate and the host copies do not crowd the cores."""
         self.context = context
+        self.max_running = max(1, int(max_running))
         self.return_threads = max(1, int(return_threads))
         self.admit_threads = max(1, int(admit_threads))
         self.budget = float(budget_bytes)
@@ -276,6 +282,11 @@ class Server(object):
                     ready += 1
                 burst = ready > self.admit_threads
                 while pending and pending[0].arrival <= now:
+                    # on the GPU, being uploaded or waiting to be returned
+                    with lock:
+                        held = len(running) + len(admitting) + shared["outstanding"]
+                    if held >= self.max_running:
+                        break
                     r = pending[0]
                     need = state_bytes(r.scheme, r.nx, r.ny)
                     with lock:

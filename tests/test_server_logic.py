@@ -223,3 +223,20 @@ def test_gpu_full_with_nothing_resident_is_rejected(fake, monkeypatch, n, spacin
     results, stats = srv.serve(requests(n, spacing))
     assert len(results) == n and all(r.status == "rejected" and "does not fit" in r.error for r in results)
     assert srv.used == 0.0
+
+
+def test_running_scenarios_capped(fake, monkeypatch):
+    """Past max_running the arrivals wait to be admitted; all are served."""
+    reqs = requests(40, 0.0)
+    srv = Server(None, budget_bytes=1e12, chunk_steps=1, schemes=("KP07_dimsplit",), max_running=5)
+    peak = {"n": 0}
+    orig_run = FakeBatch.run
+
+    def run(self, n):
+        peak["n"] = max(peak["n"], len(self.slots))
+        orig_run(self, n)
+
+    monkeypatch.setattr(FakeBatch, "run", run)
+    results, stats = srv.serve(reqs)
+    assert done_ids(results) == list(range(40)) and stats["requests"] == 40
+    assert peak["n"] <= 5
