@@ -557,6 +557,117 @@ def make_scheme_sim(ctx, scheme, seed):
     return sim, NX, NY, [h, hu, hv], "circular dam break %dx%d (R=%.0f cells), reflective walls" % (NX, NY, R)
 
 
+def rooflines(scheme, cells, launch_s, pk, pk_kind, props, prof=None):
+    """HBM and FP32 rooflines of one stage launch of `scheme` over `cells`
+    cells taking `launch_s` seconds on average.
+
+    HBM: the algorithmic bytes (BYTES_PER_CELL_LAUNCH) against the measured
+    copy bandwidth.  FP32, against the nominal FP32 peak (an FMA is 2
+    operations): the FLOP this kernel executes (its own formulation) and, for
+    comparison, the reference formulation's algorithmic count; and the floor
+    set by its FP32 pipe operations.  The binding roofline is the longer of
+    the HBM and FP32 lower-bound times."""
+    prof = prof or {}
+    alg_bytes = BYTES_PER_CELL_LAUNCH[scheme] * cells
+    achieved = alg_bytes / launch_s / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / pk["hbm_gbs"], "traffic": prof.get("dram_bytes_per_launch"), "peak_kind": pk_kind,
+            "algorithmic_bytes_per_launch": alg_bytes}
+    sm_max_mhz = float(pk.get("sm_max_mhz") or 1965.0)
+    fp32_peak = props.multi_processor_count * FP32_LANES_PER_SM * 2 * sm_max_mhz * 1e6 / 1e12
+    ops = ALG_OPS_PER_CELL_LAUNCH[scheme]
+    ref_flop = ops["flops"] * cells
+    own = EXECUTED_FLOP_PER_CELL_LAUNCH.get(scheme)
+    own_flop = own * cells if own else None
+    roof_fp32 = {"bound": "fp32", "peak": fp32_peak, "unit": "TFLOP/s",
+                 "peak_kind": "nominal: %d SMs x %d FP32 lanes x 2 x %.0f MHz" % (
+                     props.multi_processor_count, FP32_LANES_PER_SM, sm_max_mhz),
+                 "reference_formulation_flop_per_cell_launch": ops["flops"],
+                 "reference_formulation_achieved": ref_flop / launch_s / 1e12,
+                 "reference_formulation_frac": ref_flop / launch_s / 1e12 / fp32_peak,
+                 "mufu_per_cell_launch_reference_formulation": ops["mufu"]}
+    if own_flop:
+        roof_fp32.update({"achieved": own_flop / launch_s / 1e12, "frac": own_flop / launch_s / 1e12 / fp32_peak,
+                          "flop_per_cell_launch": own,
+                          "flop_source": "FP32 FLOP this kernel executes per cell-substep (ncu sass op counters)"})
+    if prof.get("executed_inst_per_cell_substep"):
+        roof_fp32["executed_inst_per_cell_launch"] = prof["executed_inst_per_cell_substep"]
+    t_hbm = alg_bytes / (pk["hbm_gbs"] * 1e9)
+    t_fp32 = (own_flop or ref_flop) / (fp32_peak * 1e12)
+    pipe_ops = FP32_PIPE_OPS_PER_CELL_LAUNCH.get(scheme)
+    if pipe_ops:
+        # FP32 lanes x clock: the pipe's operation rate (half the FLOP peak)
+        t_pipe = pipe_ops * cells / (fp32_peak * 1e12 / 2.0)
+        roof_fp32["pipe"] = {"fp32_ops_per_cell_launch": pipe_ops, "floor_us_per_launch": t_pipe * 1e6,
+                             "frac": t_pipe / launch_s,
+                             "what": "fadd + fmul + ffma lane operations (ncu sass counters) on 128 FP32 lanes "
+                                     "per SM at the maximum SM clock"}
+        t_fp32 = max(t_fp32, t_pipe)
+    if t_fp32 > t_hbm:
+        roof["binding"] = "fp32_pipe" if pipe_ops else ("fp32_flop" if own_flop else "fp32_flop_reference_formulation")
+    else:
+        roof["binding"] = "hbm"
+    roof["frac_of_binding"] = max(t_hbm, t_fp32) / launch_s
+    return roof, roof_fp32
+
+
+ALL_SCHEMES = ("LxF", "FORCE", "HLL", "HLL2", "WAF", "KP07", "KP07_dimsplit", "EE2D_KP07_dimsplit")
+
+
+def schemes_leg(ctx, steps=200, warmup=5, ref_steps=40):
+    """Every scheme on its benchmark workload (the seven shallow-water schemes
+    on the 4096 x 4096 dam break, Euler on the 4096 x 2048 Kelvin-Helmholtz
+    problem): device ms per step over `steps` steps of simulate()'s dt
+    schedule (CUDA events), HBM and FP32 rooflines of the stage kernel, and
+    the reference's own kernel of the scheme (CUDA source compiled unmodified
+    for sm_100a) on the same input and GPU at the fastest of its built block
+    shapes, `ref_steps` steps of fixed dt."""
+    import torch
+
+    from oracle import ref_kernels
+
+    pk, pk_kind = peaks()
+    props = torch.cuda.get_device_properties(ctx.device_id)
+    out = {}
+    for scheme in ALL_SCHEMES:
+        sim, nx, ny, q, desc = make_scheme_sim(ctx, scheme, 0)
+        sim.advance(warmup)
+        sim.advance(steps)
+        ms = sim.last_advance_ms()
+        info = sim.tile_info()
+        del sim
+        torch.cuda.synchronize(ctx.device_id)
+        cells = nx * ny
+        roof, roof_fp32 = rooflines(scheme, cells, ms * 1e-3 / info["launches_per_step"], pk, pk_kind, props)
+        row = {"workload": desc, "ms_per_step": ms, "cell_updates_per_s": cells / (ms * 1e-3),
+               "launches_per_step": info["launches_per_step"],
+               "tile": "%dx%d, %d threads" % (info["tile_w"], info["tile_h"], info["threads"]),
+               "hbm_gbs": roof["achieved"], "hbm_frac": roof["frac"], "binding": roof["binding"],
+               "frac_of_binding": roof["frac_of_binding"]}
+        if "pipe" in roof_fp32:
+            row["fp32_pipe_floor_us_per_launch"] = roof_fp32["pipe"]["floor_us_per_launch"]
+        per_block = {}
+        kw = {"gamma": 1.4, "bc": 0x02020202} if scheme == "EE2D_KP07_dimsplit" else {}
+        dx, dy, g = (1.0 / nx, 1.0 / ny, 0.0) if scheme == "EE2D_KP07_dimsplit" else (1.0, 1.0, 9.81)
+        for block in [None] + list(ref_kernels.BLOCKS):
+            if not ref_kernels.available(scheme, block):
+                continue
+            ref = ref_kernels.RefKernelSim(scheme, q, nx, ny, dx, dy, g, block=block, **kw)
+            dt = np.float32(ref.computeDt() * np.float32(0.9))
+            ref.time_steps(warmup, dt)
+            per_block["%dx%d" % (ref.bw, ref.bh)] = ref.time_steps(ref_steps, dt)
+            ref.close()
+        if per_block:
+            best = min(per_block, key=per_block.get)
+            row["reference_kernels_gpu"] = {"ms_per_step": per_block[best], "block": best,
+                                            "speedup_of_this_library": per_block[best] / ms}
+        out[scheme] = row
+    return {"what": "each scheme on its benchmark workload, %d steps (simulate()'s dt schedule), device time; "
+                    "reference kernels: their CUDA source compiled unmodified for sm_100a, same input and GPU, "
+                    "fastest built block, %d steps of fixed dt" % (steps, ref_steps),
+            "schemes": out}
+
+
 def run_mine(args, rank, world, local_rank):
     import torch
 
@@ -598,56 +709,11 @@ def run_mine(args, rank, world, local_rank):
     # roofline of the dominant kernel (the stage kernel)
     pk, pk_kind = peaks()
     launch_s = T / launches
-    alg_bytes = BYTES_PER_CELL_LAUNCH[scheme] * cells
-    achieved = alg_bytes / launch_s / 1e9
     prof = load_profile() if scheme == SCHEME and NX == 4096 else {}
-    traffic = prof.get("dram_bytes_per_launch")
-    roof = {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
-            "frac": achieved / pk["hbm_gbs"], "traffic": traffic, "peak_kind": pk_kind,
-            "kernel": "%s stage kernel, tile %dx%d, %d threads" % (scheme, info["tile_w"], info["tile_h"],
-                                                                    info["threads"]),
-            "algorithmic_bytes_per_launch": alg_bytes}
-    # FP32 rooflines against the nominal FP32 peak (an FMA is 2 operations):
-    # the FLOP this kernel executes (its own formulation; what bounds it) and,
-    # for comparison, the reference formulation's algorithmic count.  The
-    # binding roofline is the longer lower-bound time of HBM and the
-    # kernel's own FP32 work.
-    props = torch.cuda.get_device_properties(local_rank)
-    sm_max_mhz = float(pk.get("sm_max_mhz") or 1965.0)
-    fp32_peak = props.multi_processor_count * FP32_LANES_PER_SM * 2 * sm_max_mhz * 1e6 / 1e12
-    ops = ALG_OPS_PER_CELL_LAUNCH[scheme]
-    ref_flop = ops["flops"] * cells
-    own = EXECUTED_FLOP_PER_CELL_LAUNCH.get(scheme)
-    own_flop = own * cells if own else None
-    roof_fp32 = {"bound": "fp32", "peak": fp32_peak, "unit": "TFLOP/s",
-                 "peak_kind": "nominal: %d SMs x %d FP32 lanes x 2 x %.0f MHz" % (
-                     props.multi_processor_count, FP32_LANES_PER_SM, sm_max_mhz),
-                 "reference_formulation_flop_per_cell_launch": ops["flops"],
-                 "reference_formulation_achieved": ref_flop / launch_s / 1e12,
-                 "reference_formulation_frac": ref_flop / launch_s / 1e12 / fp32_peak,
-                 "mufu_per_cell_launch_reference_formulation": ops["mufu"]}
-    if own_flop:
-        roof_fp32.update({"achieved": own_flop / launch_s / 1e12, "frac": own_flop / launch_s / 1e12 / fp32_peak,
-                          "flop_per_cell_launch": own,
-                          "flop_source": "FP32 FLOP this kernel executes per cell-substep (ncu sass op counters)"})
-    if prof.get("executed_inst_per_cell_substep"):
-        roof_fp32["executed_inst_per_cell_launch"] = prof["executed_inst_per_cell_substep"]
-    t_hbm = alg_bytes / (pk["hbm_gbs"] * 1e9)
-    t_fp32 = (own_flop or ref_flop) / (fp32_peak * 1e12)
-    pipe_ops = FP32_PIPE_OPS_PER_CELL_LAUNCH.get(scheme)
-    if pipe_ops:
-        # FP32 lanes x clock: the pipe's operation rate (half the FLOP peak)
-        t_pipe = pipe_ops * cells / (fp32_peak * 1e12 / 2.0)
-        roof_fp32["pipe"] = {"fp32_ops_per_cell_launch": pipe_ops, "floor_us_per_launch": t_pipe * 1e6,
-                             "frac": t_pipe / launch_s,
-                             "what": "fadd + fmul + ffma lane operations (ncu sass counters) on 128 FP32 lanes "
-                                     "per SM at the maximum SM clock"}
-        t_fp32 = max(t_fp32, t_pipe)
-    if t_fp32 > t_hbm:
-        roof["binding"] = "fp32_pipe" if pipe_ops else ("fp32_flop" if own_flop else "fp32_flop_reference_formulation")
-    else:
-        roof["binding"] = "hbm"
-    roof["frac_of_binding"] = max(t_hbm, t_fp32) / launch_s
+    roof, roof_fp32 = rooflines(scheme, cells, launch_s, pk, pk_kind, torch.cuda.get_device_properties(local_rank),
+                                prof)
+    roof["kernel"] = "%s stage kernel, tile %dx%d, %d threads" % (scheme, info["tile_w"], info["tile_h"],
+                                                                   info["threads"])
 
     result = None
     if rank == 0:
@@ -726,6 +792,8 @@ def run_mine(args, rank, world, local_rank):
         result["cpu_baseline"] = aux_leg(cpu_baseline_leg)
     if rank == 0 and world == 1 and not args.no_reference_kernels and scheme == SCHEME and NX == 4096:
         result["reference_kernels_gpu"] = aux_leg(reference_kernels_leg, dev_ms_per_step)
+    if rank == 0 and world == 1 and not args.no_schemes and scheme == SCHEME and NX == 4096:
+        result["schemes"] = aux_leg(schemes_leg, ctx)
     return result
 
 
@@ -741,6 +809,8 @@ def main():
     ap.add_argument("--no-served", action="store_true", help="skip the served request stream")
     ap.add_argument("--no-reference-kernels", action="store_true",
                     help="skip timing the reference's own kernel on the same GPU")
+    ap.add_argument("--no-schemes", action="store_true",
+                    help="skip the per-scheme leg (every scheme on its benchmark workload, with the reference kernels)")
     ap.add_argument("--served-requests", type=int, default=10000)
     ap.add_argument("--served-rates", default="300,600,1200",
                     help="Poisson arrival rates (requests/s) of the served sweep, comma separated; the top-level "

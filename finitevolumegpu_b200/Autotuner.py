@@ -43,6 +43,8 @@ TILE_CONFIGS = {
 }
 # Tile configurations of the batched (persistent) kernels per scheme.
 BATCH_TILE_CONFIGS = {
+    "LxF": 2,
+    "KP07": 2,
     "KP07_dimsplit": 4,
     "HLL": 4,
     "EE2D_KP07_dimsplit": 3,

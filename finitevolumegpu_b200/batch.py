@@ -1,10 +1,10 @@
 """Batched simulation: many grids of uneven sizes advanced together on one GPU.
 
 The reference runs one simulator per class instance, one kernel launch per
-substep.  A ``Batch`` holds many simulations of one dimensionally split scheme
-(FORCE, HLL, HLL2, WAF, KP07_dimsplit, EE2D_KP07_dimsplit) resident in HBM and
-advances all of them with one persistent kernel per substep that walks a tile
-work list; the step sequence is replayed from CUDA graphs.  Each simulation
+substep.  A ``Batch`` holds many simulations of one scheme (any of the eight)
+resident in HBM and advances all of them with one persistent kernel per
+substep (one per Runge-Kutta stage for KP07) that walks a tile work list; the
+step sequence is replayed from CUDA graphs.  Each simulation
 follows the reference's ``simulate(t_end)`` semantics on its own: its own CFL
 time step recomputed every 100 of its steps, its last step shortened to hit
 its t_end (GPUSimulators/Simulator.py:176-217).  Its result is therefore the
@@ -21,8 +21,8 @@ import numpy as np
 from . import _lib
 from .Simulator import BoundaryCondition
 
-BATCH_SCHEMES = ("FORCE", "HLL", "HLL2", "WAF", "KP07_dimsplit", "EE2D_KP07_dimsplit")
-GHOST = {"FORCE": 1, "HLL": 1}
+BATCH_SCHEMES = ("LxF", "FORCE", "HLL", "HLL2", "WAF", "KP07", "KP07_dimsplit", "EE2D_KP07_dimsplit")
+GHOST = {"LxF": 1, "FORCE": 1, "HLL": 1}
 DEFAULT_THETA = {"HLL2": 1.8}
 
 def _L():
@@ -30,10 +30,12 @@ def _L():
 
 
 class Batch(object):
-    """Simulations of one split scheme advanced together by a persistent kernel."""
+    """Simulations of one scheme advanced together by a persistent kernel.
+    ``order`` is KP07's Runge-Kutta order (1 or 2, GPUSimulators/KP07.py:62),
+    the same for every simulation of the batch."""
 
     def __init__(self, context, scheme, g=9.81, gamma=1.4, theta=None, cfl_scale=0.9, max_instances=1024,
-                 tile=None, variant=0, variant_beta=0.0):
+                 tile=None, variant=0, variant_beta=0.0, order=2):
         if scheme not in BATCH_SCHEMES:
             raise ValueError("batched kernels exist for %s" % (BATCH_SCHEMES,))
         self.context = context
@@ -47,7 +49,8 @@ class Batch(object):
                 tile = tuner.get_batch_tile(scheme, context.device_name)
         theta = DEFAULT_THETA.get(scheme, 1.3) if theta is None else theta
         # variant: HLL's flux or WAF's limiter id (HLL.FLUXES, WAF.LIMITERS)
-        p = _lib.fv_params(float(g), float(gamma), float(theta), float(cfl_scale), 2, int(tile), int(variant),
+        _lib.require(order in (1, 2), "order must be 1 or 2, got %r" % (order,))
+        p = _lib.fv_params(float(g), float(gamma), float(theta), float(cfl_scale), int(order), int(tile), int(variant),
                            float(variant_beta))
         h = ctypes.c_void_p()
         _lib.check(_L().fv_batch_create(context.handle, _lib.SCHEME_IDS[scheme], ctypes.byref(p), int(max_instances),

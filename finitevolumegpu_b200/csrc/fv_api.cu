@@ -160,6 +160,10 @@ struct BEntry {
 };
 // Batched (persistent) kernels; the first entry of a scheme is its default.
 const BEntry kBatchTable[] = {
+    {FV_LXF, 60, 28, 128, fv::batched_stage_kernel<fv::LXF, 60, 28, 128>},
+    {FV_LXF, 120, 28, 128, fv::batched_stage_kernel<fv::LXF, 120, 28, 128>},
+    {FV_KP07, 60, 28, 128, fv::batched_stage_kernel<fv::KP07, 60, 28, 128>},
+    {FV_KP07, 120, 28, 128, fv::batched_stage_kernel<fv::KP07, 120, 28, 128>},
     {FV_KP07_DIMSPLIT, 60, 28, 128, fv::batched_stage_kernel<fv::KP07_DIMSPLIT, 60, 28, 128>},
     {FV_KP07_DIMSPLIT, 124, 28, 128, fv::batched_stage_kernel<fv::KP07_DIMSPLIT, 124, 28, 128>},
     {FV_KP07_DIMSPLIT, 124, 60, 256, fv::batched_stage_kernel<fv::KP07_DIMSPLIT, 124, 60, 256>},
@@ -197,8 +201,13 @@ const VBEntry kBatchVariantTable[] = {
 };
 constexpr int kNumBatchVariants = sizeof(kBatchVariantTable) / sizeof(kBatchVariantTable[0]);
 
+bool scheme_split(int scheme) { return scheme != FV_LXF && scheme != FV_KP07; }
+
+// Width of a batched kernel's TMA box, the row pitch of its shared tile.
+int batch_box_w(const BEntry& e) { return scheme_split(e.scheme) ? fv::split_pitch(e.W) : e.W + 8; }
+
 size_t batch_smem(const BEntry& e) {
-    return scheme_nv(e.scheme) * (size_t)fv::split_pitch(e.W) * (e.H + 4) * sizeof(float);
+    return scheme_nv(e.scheme) * (size_t)batch_box_w(e) * (e.H + 4) * sizeof(float);
 }
 
 // The batched kernel of tile configuration `cfg`, or for variant > 0 the
@@ -1264,7 +1273,7 @@ int fv_host_free(void* ptr) {
 
 // ====================================================================== batches
 //
-// A batch advances many simulations of one split scheme together: the
+// A batch advances many simulations of one scheme together: the
 // persistent kernel walks a device-resident work list of (simulation, tile)
 // pairs, every simulation keeps its own control block (t, dt, t_end, buffer
 // parity), and graphs of 1 and 16 steps are captured once.  Adding or
@@ -1341,6 +1350,7 @@ int batch_launch_step(fv_batch* b) {
         a.substep = i;
         a.is_last = (i == b->num_substeps - 1) ? 1 : 0;
         a.want_sums = 0;
+        a.order = b->p.order;
         a.err = b->d_err;
         void* kargs[] = {&a};
         FV_CK(launch_dependent(reinterpret_cast<const void*>(b->be->fn), dim3(b->grid), dim3(b->be->NT), kargs,
@@ -1449,9 +1459,12 @@ int fv_batch_create(fv_context* ctx, int scheme, const fv_params* params, int ma
     b->scheme = scheme;
     b->nv = scheme_nv(scheme);
     b->gc = scheme_ghost(scheme);
-    b->num_substeps = (scheme == FV_FORCE || scheme == FV_HLL) ? 1 : 2;
-    b->dt_scale = (b->num_substeps == 2) ? 0.5f : 1.0f;
-    b->factor = (scheme == FV_FORCE) ? 1.0f : 0.5f;
+    // substeps, kernel dt and computeDt factor as for one simulation (fv_sim_create)
+    b->num_substeps = (scheme == FV_LXF || scheme == FV_FORCE || scheme == FV_HLL) ? 1
+                      : (scheme == FV_KP07)                                   ? (params->order == 1 ? 1 : 2)
+                                                                              : 2;
+    b->dt_scale = (scheme_split(scheme) && b->num_substeps == 2) ? 0.5f : 1.0f;
+    b->factor = (scheme == FV_FORCE) ? 1.0f : (scheme == FV_KP07 && params->order == 1) ? 1.0f : 0.5f;
     b->p = *params;
     b->be = be;
     b->max_inst = max_instances;
@@ -1608,7 +1621,7 @@ int fv_batch_add(fv_batch* b, int nx, int ny, float dx, float dy, int bc, const 
         for (int v = 0; v < b->nv; ++v) {
             cuuint64_t dims[2] = {(cuuint64_t)(nx + 8), (cuuint64_t)(ny + 4)};
             cuuint64_t strides[1] = {(cuuint64_t)pitch * sizeof(float)};
-            cuuint32_t box[2] = {(cuuint32_t)fv::split_pitch(W), (cuuint32_t)(H + 4)};
+            cuuint32_t box[2] = {(cuuint32_t)batch_box_w(*b->be), (cuuint32_t)(H + 4)};
             cuuint32_t estr[2] = {1, 1};
             CUresult r = enc(&I.tmap[k][v], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, I.buf[k][v], dims, strides, box, estr,
                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,

@@ -938,97 +938,6 @@ __global__ void __launch_bounds__(NT) dimsplit_stage_kernel(const __grid_constan
     stage_epilogue<NT, NV>(A, sc, my_cfl, my_sums, sums);
 }
 
-// ------------------------------------------------------------------ batched persistent stage kernel
-
-// One simulation of a batch, resident in device memory (64-byte aligned for
-// its tensor maps).
-struct alignas(64) BatchInstance {
-    CUtensorMap tmap[2][4];
-    float* buf[2][4];
-    SimCtl* ctl;
-    float* block_cfl;    // one float per tile of this simulation
-    double* block_sums;  // 4 doubles per tile
-    int nx, ny, pitch, bc;
-    int tiles_x, ntiles;
-    float dx, dy, g, gamma, theta, dt_scale;
-    float variant_beta;  // parameter of the Osher and Sweby limiters
-};
-
-struct BatchArgs {
-    const BatchInstance* inst;
-    SimCtl* ctl;          // control blocks, one per instance: inst[i].ctl == ctl + i
-    const int2* work;     // (instance, tile within instance) per work item
-    const int* nwork;     // number of work items (device scalar, updated between graph replays)
-    int substep;
-    int is_last;
-    int want_sums;
-    int* err;
-};
-
-// Persistent split-scheme stage: the CTAs walk the work list of all tiles of
-// all simulations of the batch; each simulation keeps its own t, dt (its own
-// CFL every 100 of its steps) and t_end, and its last tile finalises its
-// control block exactly as the single-simulation kernel does.  Simulations
-// that reached t_end are skipped.  The work list lives in device memory, so
-// one captured CUDA graph serves any batch composition.
-template <int SCHEME, int W, int H, int NT, int VAR = 0, int LPT = 1>
-__global__ void __launch_bounds__(NT) batched_stage_kernel(const __grid_constant__ BatchArgs B) {
-    constexpr int NV = (SCHEME == EE2D) ? 4 : 3;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    float* Qs = reinterpret_cast<float*>(smem_raw);
-    __shared__ __align__(8) uint64_t bar;
-    grid_dependency_wait();  // the previous substep's states and control blocks
-    const int n = *B.nwork;
-    uint32_t phase = 0;
-    bool init = true;
-    // Tile prologue latency: the next work item is fetched a tile ahead, and
-    // a simulation's control block is addressed from its index (not through
-    // its instance record), so the control-block and instance loads of a
-    // tile issue together instead of one after the other.
-    int w = blockIdx.x;
-    int2 job = (w < n) ? B.work[w] : make_int2(0, 0);
-    for (; w < n; w += gridDim.x) {
-        const int wn = w + gridDim.x;
-        const int2 next = (wn < n) ? B.work[wn] : job;
-        const BatchInstance& I = B.inst[job.x];
-        SimCtl* const ctl = B.ctl + job.x;
-        StepCtl sc = read_step(ctl, false, 0.0f, false, B.is_last != 0);
-        if (!sc.active) {  // uniform across the CTA
-            job = next;
-            continue;
-        }
-        if (SCHEME == WAF) sc.do_cfl = false;
-        float my_cfl = __int_as_float(0x7f800000);
-        double my_sums[NV];
-#pragma unroll
-        for (int v = 0; v < NV; ++v) my_sums[v] = 0.0;
-        const bool sums = B.want_sums && B.is_last;
-        TileJob J;
-        J.tmap = &I.tmap[sc.cur][0];
-        J.in = I.buf[sc.cur];
-        J.out = I.buf[sc.cur ^ 1];
-        J.nx = I.nx;
-        J.ny = I.ny;
-        J.pitch = I.pitch;
-        J.bc = I.bc;
-        const int ty = job.y / I.tiles_x;
-        J.x0 = (job.y - ty * I.tiles_x) * W;
-        J.y0 = ty * H;
-        SplitPar P{I.dx, I.dy, I.g, I.gamma, I.theta, sc.dt * I.dt_scale, B.substep, I.variant_beta};
-        bool unhealthy = false;
-        process_tile_dimsplit<SCHEME, W, H, NT, true, VAR, LPT, true>(Qs, &bar, phase, init, J, P, sc.do_cfl, sums,
-                                                                      B.err, my_cfl, my_sums, kWaitPolls,
-                                                                      B.is_last != 0, &unhealthy);
-        // ordered before this tile's arrival (tile_epilogue fences before it counts)
-        if (__syncthreads_or(unhealthy) && threadIdx.x == 0) atomicOr(&ctl->bad, 1);
-        init = false;
-        phase ^= 1u;
-        tile_epilogue<NT, NV>(ctl, I.block_cfl, I.block_sums, job.y, I.ntiles, B.is_last != 0, false, sc, my_cfl,
-                              my_sums, sums);
-        job = next;
-    }
-}
-
 // ------------------------------------------------------------------ unsplit stage kernel (LxF, KP07)
 
 __device__ __forceinline__ SweFace shfl_up_face(const SweFace& f, int d) {
@@ -1043,53 +952,38 @@ __device__ __forceinline__ SweFace shfl_up_face(const SweFace& f, int d) {
     return r;
 }
 
-// One pass over the tile, as column walkers (GPUSimulators/cuda/SWE2D_LxF.cu:102-165,
-// SWE2D_KP07.cu:136-232).  Lanes run along x: warp column wx of a row segment
-// covers tile columns 3+30wx .. 34+30wx; lanes 1..30 update interior columns
-// 30wx .. 30wx+29, lanes 0 and 31 supply the states of the columns beside
-// them.  At each row a lane builds the west and east face states of its cell;
-// the flux at its west face takes the east state of the lane to its left
-// (warp shuffle), and its east-face flux is the west-face flux of the lane
-// to its right, so each x face is computed once.  Along y each lane keeps a
-// sliding window: the north face state of the row above and the flux at the
-// south face carry over from the previous row.  The updated cells (KP07
-// stage 2 blended with the old output) go straight to global memory.
-template <int SCHEME, int W, int H, int NT>
-__global__ void __launch_bounds__(NT) unsplit_stage_kernel(const __grid_constant__ StageArgs A) {
+// Scheme constants of an unsplit tile.
+struct UnsplitPar {
+    float dx, dy, g, theta;
+    float kdt;    // kernel dt of this stage
+    int substep;  // RK stage (KP07)
+    int order;    // RK order (KP07)
+};
+
+// Load, ghost cells, the one-pass update and the stores of one tile of an
+// unsplit scheme (LxF, KP07); the per-thread CFL minimum and FP64 sums are
+// accumulated.  Returns false if the tile load gave up (nothing was written).
+// HEALTH (batched kernels): with `health` set, *unhealthy becomes true if a
+// written cell holds a non-finite value or a non-positive depth.
+template <int SCHEME, int W, int H, int NT, bool GLOBAL_TMAP = false, bool HEALTH = false>
+__device__ bool process_tile_unsplit(float* Qs, uint64_t* bar, uint32_t phase, bool init_bar, const TileJob& J,
+                                     const UnsplitPar& P, bool do_cfl, bool sums, int* err, float& my_cfl,
+                                     double (&my_sums)[3], uint32_t polls = kWaitPolls, bool health = false,
+                                     bool* unhealthy = nullptr) {
     constexpr int SP = W + 8, TR = H + 4, PS = SP * TR;
     constexpr int WX = W / 30, NSEG = NT / (32 * WX), R = H / NSEG;
     static_assert(W % 30 == 0 && NT % (32 * WX) == 0 && NSEG >= 1 && H % NSEG == 0,
                   "warps of 30 updated columns must tile the block");
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    float* Qs = reinterpret_cast<float*>(smem_raw);
-    __shared__ __align__(8) uint64_t bar;
-
-    grid_dependency_wait();  // the previous stage's state and control block
-    const StepCtl sc = read_step(A);
-    if (!sc.active) return;
-    const int x0 = blockIdx.x * W, y0 = (blockIdx.y + A.tile_row0) * H;
-    float my_cfl = __int_as_float(0x7f800000);
-    double my_sums[3] = {0.0, 0.0, 0.0};
-    const bool sums = A.want_sums && A.is_last;
-
-    TileJob J;
-    J.tmap = &A.tmap[sc.cur][0];
-    J.in = A.buf[sc.cur];
-    J.out = A.buf[sc.cur ^ 1];
-    J.nx = A.nx;
-    J.ny = A.ny;
-    J.pitch = A.pitch;
-    J.bc = A.bc;
-    J.x0 = x0;
-    J.y0 = y0;
-    if (load_tile<3, SP, TR>(Qs, J.tmap, x0, y0, &bar, 0, true, &A.ctl->error, wait_polls(A.wait_limit))) {
-        if (x0 == 0 || x0 + W + 2 > A.nx || y0 == 0 || y0 + H + 2 > A.ny) apply_boundary<3, W, H, NT>(Qs, J);
-        const float kdt = sc.dt * A.dt_scale;
-        const float g = A.g, half_g = 0.5f * g, theta2 = 2.0f * A.theta;
-        const float k4x = A.dx / (4.0f * kdt), k4y = A.dy / (4.0f * kdt);
-        const float kdx = kdt / A.dx, kdy = kdt / A.dy;
-        const int out = sc.cur ^ 1;
-        const bool blend = (SCHEME == KP07) && A.order == 2 && A.substep == 1;
+    const int x0 = J.x0, y0 = J.y0;
+    bool bad = false;
+    if (!load_tile<3, SP, TR, GLOBAL_TMAP>(Qs, J.tmap, x0, y0, bar, phase, init_bar, err, polls)) return false;
+    {
+        if (x0 == 0 || x0 + W + 2 > J.nx || y0 == 0 || y0 + H + 2 > J.ny) apply_boundary<3, W, H, NT>(Qs, J);
+        const float kdt = P.kdt;
+        const float g = P.g, half_g = fmul(0.5f, g), theta2 = fmul(2.0f, P.theta);
+        const float k4x = fdiv_fast(P.dx, fmul(4.0f, kdt)), k4y = fdiv_fast(P.dy, fmul(4.0f, kdt));
+        const float kdx = fdiv_fast(kdt, P.dx), kdy = fdiv_fast(kdt, P.dy);
+        const bool blend = (SCHEME == KP07) && P.order == 2 && P.substep == 1;
 
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
         const int wx = warp % WX, seg = warp / WX;
@@ -1159,12 +1053,12 @@ __global__ void __launch_bounds__(NT) unsplit_stage_kernel(const __grid_constant
 #pragma unroll 3
         for (int t = a; t < b; ++t) {
             const int y = y0 + t - 2;
-            const bool store = owner && x < A.nx && y < A.ny;
-            const long long gi = cell_index(y, x, A.pitch);
+            const bool store = owner && x < J.nx && y < J.ny;
+            const long long gi = cell_index(y, x, J.pitch);
             float old[3] = {0.0f, 0.0f, 0.0f};
             if (blend && store) {
 #pragma unroll
-                for (int v = 0; v < 3; ++v) old[v] = A.buf[out][v][gi];
+                for (int v = 0; v < 3; ++v) old[v] = J.out[v][gi];
             }
             // x faces of (t, s): west and east states
             SweFace fw, fe;
@@ -1203,10 +1097,13 @@ __global__ void __launch_bounds__(NT) unsplit_stage_kernel(const __grid_constant
 #pragma unroll
                 for (int v = 0; v < 3; ++v) {
                     const float o = blend ? 0.5f * (old[v] + qn[v]) : qn[v];
-                    A.buf[out][v][gi] = o;
+                    J.out[v][gi] = o;
                     if (sums) my_sums[v] += (double)o;
+                    if constexpr (HEALTH) {
+                        if (health) bad |= (v == 0) ? !(o > 0.0f) : !(fabsf(o) < __int_as_float(0x7f800000));
+                    }
                 }
-                if (sc.do_cfl) my_cfl = fminf(my_cfl, cell_cfl(qn[0], qn[1], qn[2], A.dx, A.dy, g));
+                if (do_cfl) my_cfl = fminf(my_cfl, cell_cfl(qn[0], qn[1], qn[2], P.dx, P.dy, g));
             }
 #pragma unroll
             for (int v = 0; v < 3; ++v) {
@@ -1219,7 +1116,150 @@ __global__ void __launch_bounds__(NT) unsplit_stage_kernel(const __grid_constant
             n_cur = n_nxt;
         }
     }
+    if constexpr (HEALTH) {
+        if (bad) *unhealthy = true;
+    }
+    return true;
+}
+
+// One pass over the tile, as column walkers (GPUSimulators/cuda/SWE2D_LxF.cu:102-165,
+// SWE2D_KP07.cu:136-232).  Lanes run along x: warp column wx of a row segment
+// covers tile columns 3+30wx .. 34+30wx; lanes 1..30 update interior columns
+// 30wx .. 30wx+29, lanes 0 and 31 supply the states of the columns beside
+// them.  At each row a lane builds the west and east face states of its cell;
+// the flux at its west face takes the east state of the lane to its left
+// (warp shuffle), and its east-face flux is the west-face flux of the lane
+// to its right, so each x face is computed once.  Along y each lane keeps a
+// sliding window: the north face state of the row above and the flux at the
+// south face carry over from the previous row.  The updated cells (KP07
+// stage 2 blended with the old output) go straight to global memory.
+template <int SCHEME, int W, int H, int NT>
+__global__ void __launch_bounds__(NT) unsplit_stage_kernel(const __grid_constant__ StageArgs A) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    float* Qs = reinterpret_cast<float*>(smem_raw);
+    __shared__ __align__(8) uint64_t bar;
+
+    grid_dependency_wait();  // the previous stage's state and control block
+    const StepCtl sc = read_step(A);
+    if (!sc.active) return;
+    float my_cfl = __int_as_float(0x7f800000);
+    double my_sums[3] = {0.0, 0.0, 0.0};
+    const bool sums = A.want_sums && A.is_last;
+
+    TileJob J;
+    J.tmap = &A.tmap[sc.cur][0];
+    J.in = A.buf[sc.cur];
+    J.out = A.buf[sc.cur ^ 1];
+    J.nx = A.nx;
+    J.ny = A.ny;
+    J.pitch = A.pitch;
+    J.bc = A.bc;
+    J.x0 = blockIdx.x * W;
+    J.y0 = (blockIdx.y + A.tile_row0) * H;
+    const UnsplitPar P{A.dx, A.dy, A.g, A.theta, sc.dt * A.dt_scale, A.substep, A.order};
+    process_tile_unsplit<SCHEME, W, H, NT>(Qs, &bar, 0, true, J, P, sc.do_cfl, sums, &A.ctl->error, my_cfl, my_sums,
+                                           wait_polls(A.wait_limit));
     stage_epilogue<NT, 3>(A, sc, my_cfl, my_sums, sums);
+}
+
+// ------------------------------------------------------------------ batched persistent stage kernel
+
+// One simulation of a batch, resident in device memory (64-byte aligned for
+// its tensor maps).
+struct alignas(64) BatchInstance {
+    CUtensorMap tmap[2][4];
+    float* buf[2][4];
+    SimCtl* ctl;
+    float* block_cfl;    // one float per tile of this simulation
+    double* block_sums;  // 4 doubles per tile
+    int nx, ny, pitch, bc;
+    int tiles_x, ntiles;
+    float dx, dy, g, gamma, theta, dt_scale;
+    float variant_beta;  // parameter of the Osher and Sweby limiters
+};
+
+struct BatchArgs {
+    const BatchInstance* inst;
+    SimCtl* ctl;          // control blocks, one per instance: inst[i].ctl == ctl + i
+    const int2* work;     // (instance, tile within instance) per work item
+    const int* nwork;     // number of work items (device scalar, updated between graph replays)
+    int substep;
+    int is_last;
+    int want_sums;
+    int order;  // RK order (KP07)
+    int* err;
+};
+
+// Persistent stage kernel of any scheme (one dimensional sweep of the split
+// schemes, one RK stage of LxF and KP07): the CTAs walk the work list of all
+// tiles of all simulations of the batch; each simulation keeps its own t, dt (its own
+// CFL every 100 of its steps) and t_end, and its last tile finalises its
+// control block exactly as the single-simulation kernel does.  Simulations
+// that reached t_end are skipped.  The work list lives in device memory, so
+// one captured CUDA graph serves any batch composition.
+template <int SCHEME, int W, int H, int NT, int VAR = 0, int LPT = 1>
+__global__ void __launch_bounds__(NT) batched_stage_kernel(const __grid_constant__ BatchArgs B) {
+    constexpr int NV = (SCHEME == EE2D) ? 4 : 3;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    float* Qs = reinterpret_cast<float*>(smem_raw);
+    __shared__ __align__(8) uint64_t bar;
+    grid_dependency_wait();  // the previous substep's states and control blocks
+    const int n = *B.nwork;
+    uint32_t phase = 0;
+    bool init = true;
+    // Tile prologue latency: the next work item is fetched a tile ahead, and
+    // a simulation's control block is addressed from its index (not through
+    // its instance record), so the control-block and instance loads of a
+    // tile issue together instead of one after the other.
+    int w = blockIdx.x;
+    int2 job = (w < n) ? B.work[w] : make_int2(0, 0);
+    for (; w < n; w += gridDim.x) {
+        const int wn = w + gridDim.x;
+        const int2 next = (wn < n) ? B.work[wn] : job;
+        const BatchInstance& I = B.inst[job.x];
+        SimCtl* const ctl = B.ctl + job.x;
+        StepCtl sc = read_step(ctl, false, 0.0f, false, B.is_last != 0);
+        if (!sc.active) {  // uniform across the CTA
+            job = next;
+            continue;
+        }
+        if (SCHEME == WAF) sc.do_cfl = false;
+        float my_cfl = __int_as_float(0x7f800000);
+        double my_sums[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) my_sums[v] = 0.0;
+        const bool sums = B.want_sums && B.is_last;
+        TileJob J;
+        J.tmap = &I.tmap[sc.cur][0];
+        J.in = I.buf[sc.cur];
+        J.out = I.buf[sc.cur ^ 1];
+        J.nx = I.nx;
+        J.ny = I.ny;
+        J.pitch = I.pitch;
+        J.bc = I.bc;
+        const int ty = job.y / I.tiles_x;
+        J.x0 = (job.y - ty * I.tiles_x) * W;
+        J.y0 = ty * H;
+        bool unhealthy = false;
+        if constexpr (SCHEME == LXF || SCHEME == KP07) {
+            const UnsplitPar P{I.dx, I.dy, I.g, I.theta, sc.dt * I.dt_scale, B.substep, B.order};
+            process_tile_unsplit<SCHEME, W, H, NT, true, true>(Qs, &bar, phase, init, J, P, sc.do_cfl, sums, B.err,
+                                                               my_cfl, my_sums, kWaitPolls, B.is_last != 0,
+                                                               &unhealthy);
+        } else {
+            const SplitPar P{I.dx, I.dy, I.g, I.gamma, I.theta, sc.dt * I.dt_scale, B.substep, I.variant_beta};
+            process_tile_dimsplit<SCHEME, W, H, NT, true, VAR, LPT, true>(Qs, &bar, phase, init, J, P, sc.do_cfl,
+                                                                          sums, B.err, my_cfl, my_sums, kWaitPolls,
+                                                                          B.is_last != 0, &unhealthy);
+        }
+        // ordered before this tile's arrival (tile_epilogue fences before it counts)
+        if (__syncthreads_or(unhealthy) && threadIdx.x == 0) atomicOr(&ctl->bad, 1);
+        init = false;
+        phase ^= 1u;
+        tile_epilogue<NT, NV>(ctl, I.block_cfl, I.block_sums, job.y, I.ntiles, B.is_last != 0, false, sc, my_cfl,
+                              my_sums, sums);
+        job = next;
+    }
 }
 
 }  // namespace fv

@@ -43,6 +43,8 @@ from .Simulator import BoundaryCondition
 
 # Default physical parameters per scheme; a request may set its own g and gamma.
 SCHEME_PARAMS = {
+    "LxF": dict(g=9.81, gamma=1.4),
+    "KP07": dict(g=9.81, gamma=1.4),
     "KP07_dimsplit": dict(g=9.81, gamma=1.4),
     "HLL": dict(g=9.81, gamma=1.4),
     "HLL2": dict(g=9.81, gamma=1.4),
@@ -165,7 +167,7 @@ class Server(object):
 
         for r in sorted(requests, key=lambda r: r.arrival):
             if r.scheme not in SCHEME_PARAMS:
-                finish(r, "rejected", "no batched kernels for scheme %r" % (r.scheme,))
+                finish(r, "rejected", "unknown scheme %r" % (r.scheme,))
             elif state_bytes(r.scheme, r.nx, r.ny) > self.budget:
                 finish(r, "rejected", "a %d x %d grid needs more device memory than the budget of %.3g bytes"
                        % (r.nx, r.ny, self.budget))

@@ -207,15 +207,15 @@ FV_API int fv_sim_info(fv_sim* sim, int* tile_w, int* tile_h, int* threads, int*
  * call, measured with CUDA events on the simulation's stream (0 if unknown). */
 FV_API int fv_sim_last_advance_ms(fv_sim* sim, double* ms);
 
-/* ---- Batches: many simulations of one split scheme advanced together.
+/* ---- Batches: many simulations of one scheme advanced together.
  * No counterpart in the reference (it runs one simulation per class instance);
  * each simulation in a batch follows exactly the reference's simulate(t_end)
  * semantics (own CFL dt every 100 of its own steps, last step shortened to
  * t_end), so its result equals a plain fv_sim_simulate of the same scenario. */
 typedef struct fv_batch fv_batch;
 
-/* Scheme: FV_FORCE, FV_HLL, FV_HLL2, FV_WAF, FV_KP07_DIMSPLIT or
- * FV_EE2D_KP07_DIMSPLIT; params->tile selects the batched kernel's tile shape. */
+/* Any scheme (params->order sets KP07's Runge-Kutta order for every
+ * simulation of the batch); params->tile selects the batched kernel's tile shape. */
 FV_API int fv_batch_create(fv_context* ctx, int scheme, const fv_params* params, int max_instances, fv_batch** out);
 FV_API int fv_batch_destroy(fv_batch* batch);
 /* Admits one simulation (initial state as for fv_sim_create) that runs until

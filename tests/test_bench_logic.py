@@ -45,7 +45,7 @@ def test_bench_legs_and_initial_states():
     import numpy as np
 
     for name in ("run_mine", "run_reference", "run_batched", "run_served", "cpu_baseline_leg",
-                 "reference_kernels_leg", "make_scheme_sim", "ICFeed"):
+                 "reference_kernels_leg", "schemes_leg", "rooflines", "make_scheme_sim", "ICFeed"):
         assert callable(getattr(bench, name)), name
     rng = np.random.default_rng(0)
     for make, nv in ((bench.bump_ic, 3), (bench.dam_ic, 3), (bench.kh_ic, 4)):
@@ -68,3 +68,29 @@ def test_ic_feed_serves_requests_in_order_with_skips_and_retries():
         assert feed.get(17) == 170  # a retried admission regenerates its state
     finally:
         feed.close()
+
+
+def test_rooflines_of_every_scheme():
+    """rooflines(): algorithmic bytes over the launch time against the
+    measured HBM peak, and the binding floor (the longer of the HBM and the
+    FP32-pipe lower bounds) over the launch time, for every scheme."""
+    import types
+
+    props = types.SimpleNamespace(multi_processor_count=148)
+    pk = {"hbm_gbs": 6500.0, "sm_max_mhz": 1965.0}
+    cells = 4096 * 4096
+    for scheme in bench.ALL_SCHEMES:
+        launch_s = 200e-6
+        roof, fp32 = bench.rooflines(scheme, cells, launch_s, pk, "measured", props)
+        alg = bench.BYTES_PER_CELL_LAUNCH[scheme] * cells
+        assert roof["algorithmic_bytes_per_launch"] == alg
+        assert abs(roof["achieved"] - alg / launch_s / 1e9) < 1e-6 * roof["achieved"]
+        assert abs(roof["frac"] - roof["achieved"] / 6500.0) < 1e-12
+        t_hbm = alg / 6500e9
+        t_pipe = bench.FP32_PIPE_OPS_PER_CELL_LAUNCH[scheme] * cells / (148 * 128 * 1965e6)
+        assert abs(fp32["pipe"]["floor_us_per_launch"] - t_pipe * 1e6) < 1e-9 * t_pipe * 1e6
+        assert roof["binding"] == ("fp32_pipe" if t_pipe > t_hbm else "hbm"), scheme
+        assert abs(roof["frac_of_binding"] - max(t_hbm, t_pipe) / launch_s) < 1e-12
+    # the headline kernel binds on its FP32 pipe operations (71.6 us against 62 us of HBM traffic)
+    roof, _ = bench.rooflines("KP07_dimsplit", cells, 155e-6, {"hbm_gbs": 6500.0}, "measured", props)
+    assert roof["binding"] == "fp32_pipe"

@@ -48,7 +48,8 @@ def plain(ctx, scheme, q, nx, ny, dx, dy, t_end, bc=None):
 SIZES = [(64, 64), (97, 150), (300, 70), (130, 131), (33, 200), (250, 250)]
 
 
-@pytest.mark.parametrize("scheme", ["KP07_dimsplit", "HLL", "EE2D_KP07_dimsplit", "HLL2", "WAF", "FORCE"])
+@pytest.mark.parametrize("scheme", ["KP07_dimsplit", "HLL", "EE2D_KP07_dimsplit", "HLL2", "WAF", "FORCE", "LxF",
+                                    "KP07"])
 def test_batch_equals_plain(ctx, scheme):
     b = Batch(ctx, scheme, g=0.0 if scheme == "EE2D_KP07_dimsplit" else 9.81, max_instances=16)
     bc = PERIODIC if scheme == "EE2D_KP07_dimsplit" else None
@@ -68,6 +69,24 @@ def test_batch_equals_plain(ctx, scheme):
         assert st["nt"] == nt and st["t"] == t, (slot, st, nt, t)
         for a, w in zip(got, want):
             assert np.array_equal(a, w), (scheme, slot, rel_linf(a, w))
+
+
+def test_batch_kp07_first_order_equals_plain(ctx):
+    """KP07 of order 1: one Runge-Kutta stage per step and computeDt's factor
+    1 (GPUSimulators/KP07.py:138), for every simulation of the batch."""
+    b = Batch(ctx, "KP07", order=1, cfl_scale=0.45, max_instances=4)
+    cases = {}
+    for k, (nx, ny) in enumerate([(97, 150), (130, 131)]):
+        q, dx, dy, t_end = scenario("KP07", nx, ny, "bump" if k else "dam", k)
+        cases[b.add(q, nx, ny, dx, dy, t_end)] = (q, nx, ny, dx, dy, t_end)
+    b.run_to_completion()
+    for slot, (q, nx, ny, dx, dy, t_end) in cases.items():
+        sim = fv.KP07.KP07(ctx, *q, nx, ny, dx, dy, 9.81, cfl_scale=0.45, order=1)
+        sim.simulate(t_end)
+        st = b.status(slot)
+        assert st["nt"] == sim.simSteps() and st["t"] == sim.simTime()
+        for a, w in zip(b.download(slot), sim.download()):
+            assert np.array_equal(a, w), (slot, rel_linf(a, w))
 
 
 def test_batch_matches_oracle(ctx):
@@ -210,14 +229,14 @@ def test_server_isolates_bad_requests(ctx):
     unknown scheme rejected; every other request equals its solo run."""
     reqs = []
     for i in range(9):
-        s = ("KP07_dimsplit", "HLL")[i % 2]
+        s = ("KP07_dimsplit", "HLL", "KP07", "LxF")[i % 4]
         nx, ny = 60 + 13 * i, 90 - 5 * i
         q, dx, dy, t_end = scenario(s, nx, ny, "bump" if i % 3 else "dam", 300 + i)
         reqs.append(Request(i, s, q, nx, ny, dx, dy, t_end, arrival=0.001 * i))
     reqs[2].variables = [a.copy() for a in reqs[2].variables]
     reqs[2].variables[1][3, 4] = np.inf  # corrupted momentum
     reqs[5].variables = [a[:-1] for a in reqs[5].variables]  # one row short
-    reqs[7].scheme = "KP07"  # unsplit: not served
+    reqs[7].scheme = "MUSCL"  # no such scheme
     results, stats = Server(ctx, budget_bytes=2e9, chunk_steps=4, max_instances=32).serve(reqs)
     by = {r.rid: r for r in results}
     assert len(results) == 9

@@ -154,10 +154,10 @@ def test_request_larger_than_the_budget_is_rejected(fake):
 
 def test_unknown_scheme_is_rejected(fake):
     reqs = requests(2, 0.0)
-    reqs[1].scheme = "LxF"  # unsplit: no batched kernels
+    reqs[1].scheme = "MUSCL"  # no such scheme
     results, _ = Server(None, budget_bytes=1e12, chunk_steps=1, schemes=("KP07_dimsplit",)).serve(reqs)
     by = {r.rid: r for r in results}
-    assert by[1].status == "rejected" and "LxF" in by[1].error
+    assert by[1].status == "rejected" and "MUSCL" in by[1].error
     assert done_ids(results) == [0]
 
 
