@@ -54,6 +54,49 @@ def test_bench_legs_and_initial_states():
         assert np.all(q[0] > 0)
 
 
+def test_initial_states_match_their_full_grid_formulas():
+    """The served leg's initial-state generators take shortcuts (a bump is
+    evaluated only near its centre, the Kelvin-Helmholtz rows are computed
+    once); they must give the bits of the plain full-grid formulas."""
+    import numpy as np
+
+    def bump(nx, ny, rng):
+        A = rng.uniform(0.1, 0.5)
+        cx, cy = rng.uniform(0.3, 0.7) * nx, rng.uniform(0.3, 0.7) * ny
+        x = np.arange(nx, dtype=np.float32) + 0.5
+        y = np.arange(ny, dtype=np.float32) + 0.5
+        h = 1.0 + A * np.exp(-((x[None, :] - cx) ** 2 + (y[:, None] - cy) ** 2) / (2 * 20.0 ** 2))
+        return [h.astype(np.float32)]
+
+    def dam(nx, ny, rng):
+        R = rng.uniform(0.1, 0.3) * nx
+        x = np.arange(nx, dtype=np.float32) + 0.5 - nx / 2.0
+        y = np.arange(ny, dtype=np.float32) + 0.5 - ny / 2.0
+        return [np.where(x[None, :] ** 2 + y[:, None] ** 2 < R * R, 1.0, 0.1).astype(np.float32)]
+
+    def kh(nx, ny, rng, gamma=1.4):
+        phi = rng.uniform(0, 2 * np.pi)
+        yy = (np.arange(ny, dtype=np.float32) + 0.5) / ny
+        xx = (np.arange(nx, dtype=np.float32) + 0.5) / nx
+        band = ((yy >= 0.25) & (yy < 0.75))[:, None]
+        rho = np.where(band, 2.0, 1.0) * np.ones((1, nx))
+        u = np.where(band, 0.5, -0.5) * np.ones((1, nx))
+        v = 0.01 * np.sin(4 * np.pi * xx[None, :] + phi) * np.ones((ny, 1))
+        E = 2.5 / (gamma - 1.0) + 0.5 * rho * (u ** 2 + v ** 2)
+        return [a.astype(np.float32) for a in (rho, rho * u, rho * v, E)]
+
+    for nx, ny in ((128, 128), (2048, 2048), (700, 300), (129, 2047), (1500, 131), (3, 5), (900, 64)):
+        for seed in range(4):
+            for fast, plain in ((bench.bump_ic, bump), (bench.dam_ic, dam), (bench.kh_ic, kh)):
+                got = fast(nx, ny, np.random.default_rng(seed))
+                want = plain(nx, ny, np.random.default_rng(seed))
+                for a, b in zip(got, want):
+                    assert a.dtype == np.float32 and a.shape == (ny, nx)
+                    assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (fast.__name__, nx, ny, seed)
+                if fast is not bench.kh_ic:
+                    assert not np.any(got[1]) and not np.any(got[2])
+
+
 def test_ic_feed_serves_requests_in_order_with_skips_and_retries():
     made = []
 
