@@ -1616,21 +1616,6 @@ int fv_batch_add(fv_batch* b, int nx, int ny, float dx, float dy, int bc, const 
     I.theta = b->p.theta;
     I.dt_scale = b->dt_scale;
     I.variant_beta = b->p.variant_beta;
-    auto enc = encode_fn();
-    for (int k = 0; k < 2; ++k)
-        for (int v = 0; v < b->nv; ++v) {
-            cuuint64_t dims[2] = {(cuuint64_t)(nx + 8), (cuuint64_t)(ny + 4)};
-            cuuint64_t strides[1] = {(cuuint64_t)pitch * sizeof(float)};
-            cuuint32_t box[2] = {(cuuint32_t)batch_box_w(*b->be), (cuuint32_t)(H + 4)};
-            cuuint32_t estr[2] = {1, 1};
-            CUresult r = enc(&I.tmap[k][v], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, I.buf[k][v], dims, strides, box, estr,
-                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-            if (r != CUDA_SUCCESS) {
-                cudaFreeAsync(mem, b->copy_stream);
-                return release(fail(FV_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r));
-            }
-        }
     const int off = halo ? gc : 0;
     for (int v = 0; v < b->nv; ++v)
         if (copy_h2d(b->ctx, b->copy_stream, I.buf[0][v] + fv::cell_index(-off, -off, pitch), pitch * sizeof(float),

@@ -89,6 +89,18 @@ __device__ __forceinline__ void fence_tmap_acquire(const void* tmap) {
                  : "memory");
 }
 
+// 16-byte asynchronous copy global -> shared (cached in L2 only) of the first
+// `src_bytes` (0..16) bytes at src; the rest of the 16 destination bytes are
+// zero-filled.  With src_bytes = 0 nothing is read.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)),
+                 "l"(reinterpret_cast<uint64_t>(src)), "r"(src_bytes)
+                 : "memory");
+}
+
+// Waits until this thread's asynchronous copies have landed in shared memory.
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ void prefetch_tmap(const void* tmap) {
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(tmap)) : "memory");
 }

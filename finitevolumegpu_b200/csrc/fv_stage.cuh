@@ -276,7 +276,7 @@ __device__ __forceinline__ void stage_epilogue(const StageArgs& A, const StepCtl
 
 // One tile of one simulation: where its input comes from and where it goes.
 struct TileJob {
-    const CUtensorMap* tmap;  // NV tensor maps of the input planes (parameter or global memory)
+    const CUtensorMap* tmap;  // NV tensor maps of the input planes (kernel parameters; unused by async loads)
     float* const* in;         // NV input planes
     float* const* out;        // NV output planes
     int nx, ny, pitch, bc;
@@ -287,7 +287,7 @@ struct TileJob {
 // wait of `polls` polls on `phase` of the mbarrier (initialised here when
 // `init`).  Returns false (uniformly across the CTA) if the wait gave up; *err
 // is then set, after a second bounded wait has let the copies in flight land.
-template <int NV, int SP, int TR, bool GLOBAL_TMAP = false>
+template <int NV, int SP, int TR>
 __device__ __forceinline__ bool load_tile(float* Qs, const CUtensorMap* tmap, int x0, int y0, uint64_t* bar,
                                           uint32_t phase, bool init, int* err, uint32_t polls = kWaitPolls) {
     constexpr int PS = SP * TR;
@@ -296,10 +296,6 @@ __device__ __forceinline__ bool load_tile(float* Qs, const CUtensorMap* tmap, in
     // multiple of 32 floats would misalign every plane after the first.
     static_assert((PS * sizeof(float)) % 128 == 0, "variable planes in shared memory must be 128-byte aligned");
     if (threadIdx.x == 0) {
-        if (GLOBAL_TMAP) {
-#pragma unroll
-            for (int v = 0; v < NV; ++v) fence_tmap_acquire(tmap + v);
-        }
         if (init) {
             mbar_init(bar, 1);
             fence_barrier_init();
@@ -321,6 +317,35 @@ __device__ __forceinline__ bool load_tile(float* Qs, const CUtensorMap* tmap, in
         return false;
     }
     return true;
+}
+
+// The same tile as load_tile, brought in by the CTA's threads with 16-byte
+// asynchronous copies instead of a tensor map: the box of SP x TR floats at
+// storage (x0, y0) of each input plane, with the tensor maps' extents
+// (nx + 8 columns, ny + 4 rows) and their zero fill beyond them, so the shared
+// tile holds the same values.  The batched kernels use it: their simulations
+// are only known on the device, and a tensor map in global memory needs a
+// proxy fence before every use, which measured about 10 us per tile.  Storage
+// rows start on 16-byte boundaries and x0 is a multiple of 4, so every chunk
+// is aligned; a chunk that straddles column nx + 8 copies its valid floats.
+template <int NV, int SP, int TR, int NT>
+__device__ __forceinline__ void load_tile_async(float* Qs, const TileJob& J) {
+    constexpr int PS = SP * TR, CH = SP / 4;
+    static_assert(SP % 4 == 0, "shared rows of whole 16-byte chunks");
+    const float* in[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) in[v] = J.in[v];
+    const int wx = J.nx + 8, hy = J.ny + 4;
+    for (int i = threadIdx.x; i < TR * CH; i += NT) {
+        const int t = i / CH, c = i - t * CH;
+        const int row = J.y0 + t, col = J.x0 + 4 * c;
+        const int valid = (row < hy) ? max(0, min(4, wx - col)) : 0;
+        const long long gi = valid ? (long long)row * J.pitch + col : 0;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) cp_async16(Qs + v * PS + t * SP + 4 * c, in[v] + gi, 4u * valid);
+    }
+    cp_async_wait_all();
+    __syncthreads();
 }
 
 __device__ __forceinline__ float sign_x(int v) { return v == 1 ? -1.0f : 1.0f; }
@@ -793,9 +818,11 @@ struct SplitPar {
 // (FORCE, HLL, HLL2, WAF, KP07_dimsplit, EE2D).  Accumulates the tile's CFL
 // minimum and FP64 sums into the per-thread values.  Returns false if the tile
 // load gave up (nothing was written).
+// ASYNC_LOAD (batched kernels): the tile comes in through load_tile_async
+// instead of the TMA (bar, phase, init_bar, err and polls are then unused).
 // HEALTH (batched kernels): with `health` set, *unhealthy becomes true if any
 // written cell holds a non-finite value or a non-positive depth (density).
-template <int SCHEME, int W, int H, int NT, bool GLOBAL_TMAP = false, int VAR = 0, int LPT = 1, bool HEALTH = false>
+template <int SCHEME, int W, int H, int NT, bool ASYNC_LOAD = false, int VAR = 0, int LPT = 1, bool HEALTH = false>
 __device__ bool process_tile_dimsplit(float* Qs, uint64_t* bar, uint32_t phase, bool init_bar, const TileJob& J,
                                       const SplitPar& P, bool do_cfl, bool sums, int* err, float& my_cfl,
                                       double (&my_sums)[(SCHEME == EE2D) ? 4 : 3], uint32_t polls = kWaitPolls,
@@ -810,7 +837,11 @@ __device__ bool process_tile_dimsplit(float* Qs, uint64_t* bar, uint32_t phase, 
     static_assert(LPT == 1 || (LPT == 2 && H % 2 == 0 &&
                                (SCHEME == KP07_DIMSPLIT || SCHEME == HLL2 || SCHEME == EE2D || SCHEME == WAF)),
                   "two lines per thread: MUSCL-Hancock schemes and WAF, with an even number of tile rows");
-    if (!load_tile<NV, SP, TR, GLOBAL_TMAP>(Qs, J.tmap, J.x0, J.y0, bar, phase, init_bar, err, polls)) return false;
+    if constexpr (ASYNC_LOAD) {
+        load_tile_async<NV, SP, TR, NT>(Qs, J);
+    } else {
+        if (!load_tile<NV, SP, TR>(Qs, J.tmap, J.x0, J.y0, bar, phase, init_bar, err, polls)) return false;
+    }
     const int x0 = J.x0, y0 = J.y0;
     if (x0 == 0 || x0 + W + 2 > J.nx || y0 == 0 || y0 + H + 2 > J.ny) apply_boundary<NV, W, H, NT, SP>(Qs, J);
 
@@ -835,9 +866,14 @@ __device__ bool process_tile_dimsplit(float* Qs, uint64_t* bar, uint32_t phase, 
         sweep_x<SCHEME, NV, W, H, NT, VAR, LPT>(Qs, 2, H + 2, p);
     }
 
-    // copy-out of the interior (+ gravity source, CFL, sums)
+    // copy-out of the interior (+ gravity source, CFL, sums); the output plane
+    // pointers are read once (for batched kernels they live in global memory,
+    // where a store through a float pointer could otherwise force a reload)
     constexpr int QW = W / 4;
     const float gg = (SCHEME == EE2D) ? P.gamma : P.g;
+    float* outp[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) outp[v] = J.out[v];
     for (int i = threadIdx.x; i < H * QW; i += NT) {
         const int r = i / QW, q = i - r * QW;
         const int y = y0 + r, x = x0 + 4 * q;
@@ -864,12 +900,12 @@ __device__ bool process_tile_dimsplit(float* Qs, uint64_t* bar, uint32_t phase, 
         const int nvalid = min(4, J.nx - x);
         if (nvalid == 4) {
 #pragma unroll
-            for (int v = 0; v < NV; ++v) *reinterpret_cast<float4*>(J.out[v] + gi) = val[v];
+            for (int v = 0; v < NV; ++v) *reinterpret_cast<float4*>(outp[v] + gi) = val[v];
         } else {
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 const float* e = &val[v].x;
-                for (int j = 0; j < nvalid; ++j) J.out[v][gi + j] = e[j];
+                for (int j = 0; j < nvalid; ++j) outp[v][gi + j] = e[j];
             }
         }
         if constexpr (HEALTH) {
@@ -963,9 +999,10 @@ struct UnsplitPar {
 // Load, ghost cells, the one-pass update and the stores of one tile of an
 // unsplit scheme (LxF, KP07); the per-thread CFL minimum and FP64 sums are
 // accumulated.  Returns false if the tile load gave up (nothing was written).
+// ASYNC_LOAD (batched kernels): the tile comes in through load_tile_async.
 // HEALTH (batched kernels): with `health` set, *unhealthy becomes true if a
 // written cell holds a non-finite value or a non-positive depth.
-template <int SCHEME, int W, int H, int NT, bool GLOBAL_TMAP = false, bool HEALTH = false>
+template <int SCHEME, int W, int H, int NT, bool ASYNC_LOAD = false, bool HEALTH = false>
 __device__ bool process_tile_unsplit(float* Qs, uint64_t* bar, uint32_t phase, bool init_bar, const TileJob& J,
                                      const UnsplitPar& P, bool do_cfl, bool sums, int* err, float& my_cfl,
                                      double (&my_sums)[3], uint32_t polls = kWaitPolls, bool health = false,
@@ -976,7 +1013,11 @@ __device__ bool process_tile_unsplit(float* Qs, uint64_t* bar, uint32_t phase, b
                   "warps of 30 updated columns must tile the block");
     const int x0 = J.x0, y0 = J.y0;
     bool bad = false;
-    if (!load_tile<3, SP, TR, GLOBAL_TMAP>(Qs, J.tmap, x0, y0, bar, phase, init_bar, err, polls)) return false;
+    if constexpr (ASYNC_LOAD) {
+        load_tile_async<3, SP, TR, NT>(Qs, J);
+    } else {
+        if (!load_tile<3, SP, TR>(Qs, J.tmap, x0, y0, bar, phase, init_bar, err, polls)) return false;
+    }
     {
         if (x0 == 0 || x0 + W + 2 > J.nx || y0 == 0 || y0 + H + 2 > J.ny) apply_boundary<3, W, H, NT>(Qs, J);
         const float kdt = P.kdt;
@@ -1049,6 +1090,9 @@ __device__ bool process_tile_unsplit(float* Qs, uint64_t* bar, uint32_t phase, b
         ystates(qm, q0, qp, bdy, s_cur, n_cur);  // row a
         float Gs[3];
         yflux(n_prev, s_cur, Gs);  // south face of row a
+        float* outp[3];  // read once (batched kernels keep them in global memory)
+#pragma unroll
+        for (int v = 0; v < 3; ++v) outp[v] = J.out[v];
         // unrolled by the row window's length: its rotation becomes renaming
 #pragma unroll 3
         for (int t = a; t < b; ++t) {
@@ -1058,7 +1102,7 @@ __device__ bool process_tile_unsplit(float* Qs, uint64_t* bar, uint32_t phase, b
             float old[3] = {0.0f, 0.0f, 0.0f};
             if (blend && store) {
 #pragma unroll
-                for (int v = 0; v < 3; ++v) old[v] = J.out[v][gi];
+                for (int v = 0; v < 3; ++v) old[v] = outp[v][gi];
             }
             // x faces of (t, s): west and east states
             SweFace fw, fe;
@@ -1097,7 +1141,7 @@ __device__ bool process_tile_unsplit(float* Qs, uint64_t* bar, uint32_t phase, b
 #pragma unroll
                 for (int v = 0; v < 3; ++v) {
                     const float o = blend ? 0.5f * (old[v] + qn[v]) : qn[v];
-                    J.out[v][gi] = o;
+                    outp[v][gi] = o;
                     if (sums) my_sums[v] += (double)o;
                     if constexpr (HEALTH) {
                         if (health) bad |= (v == 0) ? !(o > 0.0f) : !(fabsf(o) < __int_as_float(0x7f800000));
@@ -1164,10 +1208,9 @@ __global__ void __launch_bounds__(NT) unsplit_stage_kernel(const __grid_constant
 
 // ------------------------------------------------------------------ batched persistent stage kernel
 
-// One simulation of a batch, resident in device memory (64-byte aligned for
-// its tensor maps).
+// One simulation of a batch, resident in device memory.  Its tiles are loaded
+// with load_tile_async, so it carries no tensor maps.
 struct alignas(64) BatchInstance {
-    CUtensorMap tmap[2][4];
     float* buf[2][4];
     SimCtl* ctl;
     float* block_cfl;    // one float per tile of this simulation
@@ -1197,8 +1240,10 @@ struct BatchArgs {
 // control block exactly as the single-simulation kernel does.  Simulations
 // that reached t_end are skipped.  The work list lives in device memory, so
 // one captured CUDA graph serves any batch composition.
+// At most 128 registers per thread (the launch bound), so that four 128-thread
+// (two 256-thread) CTAs fit an SM as their shared tiles allow.
 template <int SCHEME, int W, int H, int NT, int VAR = 0, int LPT = 1>
-__global__ void __launch_bounds__(NT) batched_stage_kernel(const __grid_constant__ BatchArgs B) {
+__global__ void __launch_bounds__(NT, 65536 / (NT * 128)) batched_stage_kernel(const __grid_constant__ BatchArgs B) {
     constexpr int NV = (SCHEME == EE2D) ? 4 : 3;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     float* Qs = reinterpret_cast<float*>(smem_raw);
@@ -1230,7 +1275,7 @@ __global__ void __launch_bounds__(NT) batched_stage_kernel(const __grid_constant
         for (int v = 0; v < NV; ++v) my_sums[v] = 0.0;
         const bool sums = B.want_sums && B.is_last;
         TileJob J;
-        J.tmap = &I.tmap[sc.cur][0];
+        J.tmap = nullptr;
         J.in = I.buf[sc.cur];
         J.out = I.buf[sc.cur ^ 1];
         J.nx = I.nx;
