@@ -135,14 +135,9 @@ __device__ __forceinline__ int4 ld_relaxed_v4(const void* p) {
     return r;
 }
 
-__device__ __forceinline__ StepCtl read_step(const SimCtl* ctl, bool explicit_dt, float dt_step, bool force_cfl,
-                                             bool is_last) {
-    static_assert(offsetof(SimCtl, t_end) == 8 && offsetof(SimCtl, nt) == 16 && offsetof(SimCtl, dt) == 24 &&
-                      offsetof(SimCtl, update_dt) == 40 && offsetof(SimCtl, cur) == 44,
-                  "read_step's vector loads follow SimCtl's layout");
-    const int4 w0 = ld_relaxed_v4(ctl);                                          // t, t_end
-    const int4 w1 = ld_relaxed_v4(reinterpret_cast<const char*>(ctl) + 16);      // nt, dt, cfl_min
-    const int4 w2 = ld_relaxed_v4(reinterpret_cast<const char*>(ctl) + 32);      // factor, cfl_scale, update_dt, cur
+// The step of a control block from its first 48 bytes (w0, w1, w2).
+__device__ __forceinline__ StepCtl step_from_words(const int4& w0, const int4& w1, const int4& w2, bool explicit_dt,
+                                                   float dt_step, bool force_cfl, bool is_last) {
     StepCtl s;
     s.cur = w2.w;
     const double t = __hiloint2double(w0.y, w0.x);
@@ -161,6 +156,17 @@ __device__ __forceinline__ StepCtl read_step(const SimCtl* ctl, bool explicit_dt
     const bool sched = w2.z && ((nt + 1) % 100 == 0);
     s.do_cfl = force_cfl || (is_last && !explicit_dt && (sched || !(s.t_new < t_end)));
     return s;
+}
+
+__device__ __forceinline__ StepCtl read_step(const SimCtl* ctl, bool explicit_dt, float dt_step, bool force_cfl,
+                                             bool is_last) {
+    static_assert(offsetof(SimCtl, t_end) == 8 && offsetof(SimCtl, nt) == 16 && offsetof(SimCtl, dt) == 24 &&
+                      offsetof(SimCtl, update_dt) == 40 && offsetof(SimCtl, cur) == 44,
+                  "read_step's vector loads follow SimCtl's layout");
+    const int4 w0 = ld_relaxed_v4(ctl);                                          // t, t_end
+    const int4 w1 = ld_relaxed_v4(reinterpret_cast<const char*>(ctl) + 16);      // nt, dt, cfl_min
+    const int4 w2 = ld_relaxed_v4(reinterpret_cast<const char*>(ctl) + 32);      // factor, cfl_scale, update_dt, cur
+    return step_from_words(w0, w1, w2, explicit_dt, dt_step, force_cfl, is_last);
 }
 
 __device__ __forceinline__ StepCtl read_step(const StageArgs& A) {
@@ -330,19 +336,25 @@ __device__ __forceinline__ bool load_tile(float* Qs, const CUtensorMap* tmap, in
 // is aligned; a chunk that straddles column nx + 8 copies its valid floats.
 template <int NV, int SP, int TR, int NT>
 __device__ __forceinline__ void load_tile_async(float* Qs, const TileJob& J) {
-    constexpr int PS = SP * TR, CH = SP / 4;
-    static_assert(SP % 4 == 0, "shared rows of whole 16-byte chunks");
-    const float* in[NV];
+    constexpr int PS = SP * TR, CH = SP / 4, G = NT / CH;  // G rows of CH chunks at a time
+    static_assert(SP % 4 == 0 && G >= 1, "shared rows of whole 16-byte chunks, one chunk per thread");
+    // thread k copies chunk c = k % CH of tile rows g, g + G, g + 2G, ... (g = k / CH)
+    const int c = threadIdx.x % CH, g = threadIdx.x / CH;
+    if (g < G) {
+        const float* in[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) in[v] = J.in[v];
-    const int wx = J.nx + 8, hy = J.ny + 4;
-    for (int i = threadIdx.x; i < TR * CH; i += NT) {
-        const int t = i / CH, c = i - t * CH;
-        const int row = J.y0 + t, col = J.x0 + 4 * c;
-        const int valid = (row < hy) ? max(0, min(4, wx - col)) : 0;
-        const long long gi = valid ? (long long)row * J.pitch + col : 0;
+        for (int v = 0; v < NV; ++v) in[v] = J.in[v];
+        const int col = J.x0 + 4 * c;
+        const uint32_t bytes = 4u * (uint32_t)max(0, min(4, J.nx + 8 - col));  // the tensor maps' nx + 8 columns
+        const int rows = J.ny + 4 - J.y0;                                       // and ny + 4 rows
+        long long gi = (long long)(J.y0 + g) * J.pitch + col;
+        const long long gstep = (long long)G * J.pitch;
+        float* dst = Qs + g * SP + 4 * c;
+        for (int t = g; t < TR; t += G, gi += gstep, dst += G * SP) {
+            const bool in_rows = t < rows;
 #pragma unroll
-        for (int v = 0; v < NV; ++v) cp_async16(Qs + v * PS + t * SP + 4 * c, in[v] + gi, 4u * valid);
+            for (int v = 0; v < NV; ++v) cp_async16(dst + v * PS, in[v] + (in_rows ? gi : 0), in_rows ? bytes : 0u);
+        }
     }
     cp_async_wait_all();
     __syncthreads();
@@ -1233,6 +1245,31 @@ struct BatchArgs {
     int* err;
 };
 
+// The part of a work item's records a batched tile reads before its load: the
+// first 48 bytes of the simulation's control block (read_step's words) and
+// the instance record up to its last field, prefetched into shared memory a
+// tile ahead (BatchTileMeta).
+constexpr int kInstPrefix = 144;
+static_assert(offsetof(BatchInstance, variant_beta) + sizeof(float) <= kInstPrefix &&
+                  kInstPrefix % 16 == 0 && sizeof(BatchInstance) >= kInstPrefix && sizeof(SimCtl) % 16 == 0,
+              "the prefetched instance prefix holds every field, in whole 16-byte chunks");
+struct alignas(64) BatchTileMeta {
+    unsigned char inst[kInstPrefix];  // read as a BatchInstance (same alignment)
+    int4 ctl[3];
+};
+
+// Issues (threads 0..11) the asynchronous copies of `job`'s metadata into m.
+__device__ __forceinline__ void prefetch_tile_meta(BatchTileMeta& m, const BatchInstance* inst, const SimCtl* ctl,
+                                                   int2 job) {
+    constexpr int NI = kInstPrefix / 16;
+    const int i = threadIdx.x;
+    if (i < NI) {
+        cp_async16(m.inst + 16 * i, reinterpret_cast<const char*>(inst + job.x) + 16 * i, 16);
+    } else if (i < NI + 3) {
+        cp_async16(&m.ctl[i - NI], reinterpret_cast<const char*>(ctl + job.x) + 16 * (i - NI), 16);
+    }
+}
+
 // Persistent stage kernel of any scheme (one dimensional sweep of the split
 // schemes, one RK stage of LxF and KP07): the CTAs walk the work list of all
 // tiles of all simulations of the batch; each simulation keeps its own t, dt (its own
@@ -1245,65 +1282,79 @@ struct BatchArgs {
 template <int SCHEME, int W, int H, int NT, int VAR = 0, int LPT = 1>
 __global__ void __launch_bounds__(NT, 65536 / (NT * 128)) batched_stage_kernel(const __grid_constant__ BatchArgs B) {
     constexpr int NV = (SCHEME == EE2D) ? 4 : 3;
+    static_assert(NT >= 3 + kInstPrefix / 16, "one thread per prefetched 16-byte chunk");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     float* Qs = reinterpret_cast<float*>(smem_raw);
     __shared__ __align__(8) uint64_t bar;
+    __shared__ BatchTileMeta meta[2];
     grid_dependency_wait();  // the previous substep's states and control blocks
     const int n = *B.nwork;
-    uint32_t phase = 0;
-    bool init = true;
-    // Tile prologue latency: the next work item is fetched a tile ahead, and
-    // a simulation's control block is addressed from its index (not through
-    // its instance record), so the control-block and instance loads of a
-    // tile issue together instead of one after the other.
+    const int G = gridDim.x;
+    // Tile prologue latency: the work list is read two tiles ahead, and the
+    // next tile's control-block words and instance fields are copied into
+    // shared memory while this tile is computed, so a tile's load can be
+    // issued as soon as the previous tile is done.  A control block read
+    // early holds the values of this launch's start: it changes in this
+    // launch only once every tile of its simulation has arrived, and the
+    // prefetched tile has not.
     int w = blockIdx.x;
-    int2 job = (w < n) ? B.work[w] : make_int2(0, 0);
-    for (; w < n; w += gridDim.x) {
-        const int wn = w + gridDim.x;
-        const int2 next = (wn < n) ? B.work[wn] : job;
-        const BatchInstance& I = B.inst[job.x];
+    if (w >= n) return;
+    int2 job = B.work[w];
+    int2 next = (w + G < n) ? B.work[w + G] : job;
+    prefetch_tile_meta(meta[0], B.inst, B.ctl, job);
+    cp_async_wait_all();
+    __syncthreads();
+    int slot = 0;
+    for (; w < n; w += G) {
+        const int2 next2 = (w + 2 * G < n) ? B.work[w + 2 * G] : next;
+        if (w + G < n) prefetch_tile_meta(meta[slot ^ 1], B.inst, B.ctl, next);
+        const BatchTileMeta& M = meta[slot];
+        const BatchInstance& I = *reinterpret_cast<const BatchInstance*>(M.inst);
         SimCtl* const ctl = B.ctl + job.x;
-        StepCtl sc = read_step(ctl, false, 0.0f, false, B.is_last != 0);
-        if (!sc.active) {  // uniform across the CTA
-            job = next;
-            continue;
-        }
-        if (SCHEME == WAF) sc.do_cfl = false;
-        float my_cfl = __int_as_float(0x7f800000);
-        double my_sums[NV];
+        StepCtl sc = step_from_words(M.ctl[0], M.ctl[1], M.ctl[2], false, 0.0f, false, B.is_last != 0);
+        if (sc.active) {  // uniform across the CTA
+            if (SCHEME == WAF) sc.do_cfl = false;
+            float my_cfl = __int_as_float(0x7f800000);
+            double my_sums[NV];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) my_sums[v] = 0.0;
-        const bool sums = B.want_sums && B.is_last;
-        TileJob J;
-        J.tmap = nullptr;
-        J.in = I.buf[sc.cur];
-        J.out = I.buf[sc.cur ^ 1];
-        J.nx = I.nx;
-        J.ny = I.ny;
-        J.pitch = I.pitch;
-        J.bc = I.bc;
-        const int ty = job.y / I.tiles_x;
-        J.x0 = (job.y - ty * I.tiles_x) * W;
-        J.y0 = ty * H;
-        bool unhealthy = false;
-        if constexpr (SCHEME == LXF || SCHEME == KP07) {
-            const UnsplitPar P{I.dx, I.dy, I.g, I.theta, sc.dt * I.dt_scale, B.substep, B.order};
-            process_tile_unsplit<SCHEME, W, H, NT, true, true>(Qs, &bar, phase, init, J, P, sc.do_cfl, sums, B.err,
-                                                               my_cfl, my_sums, kWaitPolls, B.is_last != 0,
-                                                               &unhealthy);
-        } else {
-            const SplitPar P{I.dx, I.dy, I.g, I.gamma, I.theta, sc.dt * I.dt_scale, B.substep, I.variant_beta};
-            process_tile_dimsplit<SCHEME, W, H, NT, true, VAR, LPT, true>(Qs, &bar, phase, init, J, P, sc.do_cfl,
-                                                                          sums, B.err, my_cfl, my_sums, kWaitPolls,
-                                                                          B.is_last != 0, &unhealthy);
+            for (int v = 0; v < NV; ++v) my_sums[v] = 0.0;
+            const bool sums = B.want_sums && B.is_last;
+            TileJob J;
+            J.tmap = nullptr;
+            J.in = I.buf[sc.cur];
+            J.out = I.buf[sc.cur ^ 1];
+            J.nx = I.nx;
+            J.ny = I.ny;
+            J.pitch = I.pitch;
+            J.bc = I.bc;
+            const int ty = job.y / I.tiles_x;
+            J.x0 = (job.y - ty * I.tiles_x) * W;
+            J.y0 = ty * H;
+            bool unhealthy = false;
+            if constexpr (SCHEME == LXF || SCHEME == KP07) {
+                const UnsplitPar P{I.dx, I.dy, I.g, I.theta, sc.dt * I.dt_scale, B.substep, B.order};
+                process_tile_unsplit<SCHEME, W, H, NT, true, true>(Qs, &bar, 0, false, J, P, sc.do_cfl, sums, B.err,
+                                                                   my_cfl, my_sums, kWaitPolls, B.is_last != 0,
+                                                                   &unhealthy);
+            } else {
+                const SplitPar P{I.dx, I.dy, I.g, I.gamma, I.theta, sc.dt * I.dt_scale, B.substep, I.variant_beta};
+                process_tile_dimsplit<SCHEME, W, H, NT, true, VAR, LPT, true>(Qs, &bar, 0, false, J, P, sc.do_cfl,
+                                                                              sums, B.err, my_cfl, my_sums,
+                                                                              kWaitPolls, B.is_last != 0,
+                                                                              &unhealthy);
+            }
+            // ordered before this tile's arrival (tile_epilogue fences before it counts)
+            if (__syncthreads_or(unhealthy) && threadIdx.x == 0) atomicOr(&ctl->bad, 1);
+            tile_epilogue<NT, NV>(ctl, I.block_cfl, I.block_sums, job.y, I.ntiles, B.is_last != 0, false, sc,
+                                  my_cfl, my_sums, sums);
         }
-        // ordered before this tile's arrival (tile_epilogue fences before it counts)
-        if (__syncthreads_or(unhealthy) && threadIdx.x == 0) atomicOr(&ctl->bad, 1);
-        init = false;
-        phase ^= 1u;
-        tile_epilogue<NT, NV>(ctl, I.block_cfl, I.block_sums, job.y, I.ntiles, B.is_last != 0, false, sc, my_cfl,
-                              my_sums, sums);
+        // the next tile's metadata has landed and every thread is done with
+        // this slot, which the tile after next overwrites
+        cp_async_wait_all();
+        __syncthreads();
+        slot ^= 1;
         job = next;
+        next = next2;
     }
 }
 
