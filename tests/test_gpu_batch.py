@@ -71,6 +71,33 @@ def test_batch_equals_plain(ctx, scheme):
             assert np.array_equal(a, w), (scheme, slot, rel_linf(a, w))
 
 
+RAGGED = [(2, 2), (3, 200), (200, 3), (99, 57), (125, 29), (61, 61), (131, 7)]
+
+
+@pytest.mark.parametrize("scheme", ["KP07_dimsplit", "HLL", "EE2D_KP07_dimsplit", "LxF", "KP07"])
+def test_batch_ragged_sizes_equal_plain(ctx, scheme):
+    """Batched tiles are copied into shared memory by the threads (16-byte
+    chunks) where the plain kernels use a tensor copy; on degenerate and ragged
+    grids (a chunk straddling the tensor map's nx + 8 columns, tiles reaching
+    past the stored rows, strips narrower than a tile) both must hold the same
+    values, so the results are equal bit for bit."""
+    b = Batch(ctx, scheme, g=0.0 if scheme == "EE2D_KP07_dimsplit" else 9.81, max_instances=16)
+    cases = {}
+    for k, (nx, ny) in enumerate(RAGGED):
+        q, dx, dy, t_end = scenario(scheme, nx, ny, "bump" if k % 2 else "dam", 100 + k)
+        bc = PERIODIC if (scheme == "EE2D_KP07_dimsplit" or k % 3 == 1) else None
+        slot = b.add(q, nx, ny, dx, dy, t_end, bc)
+        cases[slot] = (q, nx, ny, dx, dy, t_end, bc)
+    b.run_to_completion()
+    for slot, (q, nx, ny, dx, dy, t_end, bc) in cases.items():
+        st = b.status(slot)
+        got = b.download(slot)
+        want, nt, t = plain(ctx, scheme, q, nx, ny, dx, dy, t_end, bc)
+        assert st["nt"] == nt and st["t"] == t, (scheme, nx, ny, st, nt, t)
+        for a, w in zip(got, want):
+            assert np.array_equal(a, w, equal_nan=True), (scheme, nx, ny, rel_linf(a, w))
+
+
 def test_batch_kp07_first_order_equals_plain(ctx):
     """KP07 of order 1: one Runge-Kutta stage per step and computeDt's factor
     1 (GPUSimulators/KP07.py:138), for every simulation of the batch."""
