@@ -228,6 +228,16 @@ __device__ __forceinline__ float vmax3_nan(float a, float b, float c) {
     asm("max.ftz.NaN.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
     return d;
 }
+__device__ __forceinline__ float vmin3_nan(float a, float b, float c) {
+    float d;
+    asm("min.ftz.NaN.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+__device__ __forceinline__ float vmin_nan(float a, float b) {
+    float d;
+    asm("min.ftz.NaN.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+    return d;
+}
 __device__ __forceinline__ float vmax3(float a, float b, float c) {
     float d;
     asm("max.ftz.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));

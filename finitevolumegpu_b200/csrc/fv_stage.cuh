@@ -923,12 +923,26 @@ __device__ bool process_tile_dimsplit(float* Qs, uint64_t* bar, uint32_t phase, 
         if constexpr (HEALTH) {
             if (health) {
                 bool bad = false;
+                if (nvalid == 4) {
+                    // NaN-propagating minimum of the depths (densities) and
+                    // maximum of the other variables' magnitudes: the same
+                    // verdict as the per-value tests below, in fewer instructions
+                    const float hmin = vmin_nan(vmin3_nan(val[0].x, val[0].y, val[0].z), val[0].w);
+                    float qmax = 0.0f;
 #pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    if (j < nvalid) {
-                        bad |= !((&val[0].x)[j] > 0.0f);
+                    for (int v = 1; v < NV; ++v)
+                        qmax = vmax3_nan(qmax, vmax3_nan(fabsf(val[v].x), fabsf(val[v].y), fabsf(val[v].z)),
+                                         fabsf(val[v].w));
+                    bad = !(hmin > 0.0f) || !(qmax < __int_as_float(0x7f800000));
+                } else {
 #pragma unroll
-                        for (int v = 1; v < NV; ++v) bad |= !(fabsf((&val[v].x)[j]) < __int_as_float(0x7f800000));
+                    for (int j = 0; j < 4; ++j) {
+                        if (j < nvalid) {
+                            bad |= !((&val[0].x)[j] > 0.0f);
+#pragma unroll
+                            for (int v = 1; v < NV; ++v)
+                                bad |= !(fabsf((&val[v].x)[j]) < __int_as_float(0x7f800000));
+                        }
                     }
                 }
                 if (bad) *unhealthy = true;
