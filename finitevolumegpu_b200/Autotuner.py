@@ -45,11 +45,11 @@ TILE_CONFIGS = {
 BATCH_TILE_CONFIGS = {
     "LxF": 2,
     "KP07": 2,
-    "KP07_dimsplit": 4,
+    "KP07_dimsplit": 5,
     "HLL": 4,
-    "EE2D_KP07_dimsplit": 3,
-    "HLL2": 3,
-    "WAF": 3,
+    "EE2D_KP07_dimsplit": 4,
+    "HLL2": 4,
+    "WAF": 4,
     "FORCE": 3,
 }
 

@@ -184,6 +184,11 @@ const BEntry kBatchTable[] = {
     {FV_FORCE, 60, 28, 128, fv::batched_stage_kernel<fv::FORCE, 60, 28, 128>},
     {FV_FORCE, 124, 28, 128, fv::batched_stage_kernel<fv::FORCE, 124, 28, 128>},
     {FV_FORCE, 28, 28, 128, fv::batched_stage_kernel<fv::FORCE, 28, 28, 128>},
+    // 60 x 60, two lines per thread in packed FP32 (same cells, bit for bit)
+    {FV_KP07_DIMSPLIT, 60, 60, 128, fv::batched_stage_kernel<fv::KP07_DIMSPLIT, 60, 60, 128, 0, 2>},
+    {FV_HLL2, 60, 60, 128, fv::batched_stage_kernel<fv::HLL2, 60, 60, 128, 0, 2>},
+    {FV_WAF, 60, 60, 128, fv::batched_stage_kernel<fv::WAF, 60, 60, 128, 0, 2>},
+    {FV_EE2D_KP07_DIMSPLIT, 60, 60, 128, fv::batched_stage_kernel<fv::EE2D, 60, 60, 128, 0, 2>},
 };
 constexpr int kNumBatchEntries = sizeof(kBatchTable) / sizeof(kBatchTable[0]);
 
