@@ -15,8 +15,8 @@ are downloaded and released by return threads, so host-to-device uploads of
 new requests, device-to-host reads of results and the queuing of the next
 chunk overlap.
 
-Failures stay with their request.  A request that cannot run (a scheme
-without batched kernels, a grid larger than the whole budget, the wrong
+Failures stay with their request.  A request that cannot run (an unknown
+scheme, a grid larger than the whole budget, the wrong
 number or shape of arrays, a GPU with no room even when nothing else is
 resident) comes back with status "rejected" and its reason; a scenario whose
 state goes bad on the GPU (a non-finite value or a non-positive depth after
