@@ -319,7 +319,7 @@ def kh_ic(nx, ny, rng, gamma=1.4):
 
 def run_batched(ctx, n_inst=512, seed=4, check=8):
     """Config 4: 512 KP07_dimsplit simulations, sides log-uniform in [64, 1024], bump or dam break,
-    t_end ~ U(5, 50): one batch of the persistent kernel vs the plain simulators one after another."""
+    t_end ~ U(5, 50): one batch (one batched launch per substep, CUDA graphs) vs the plain simulators one after another."""
     from finitevolumegpu_b200 import KP07_dimsplit
     from finitevolumegpu_b200.batch import Batch
 

@@ -41,11 +41,11 @@ TILE_CONFIGS = {
     "LxF": 4,
     "KP07": 4,
 }
-# Tile configurations of the batched (persistent) kernels per scheme.
+# Tile configurations of the batched kernels per scheme.
 BATCH_TILE_CONFIGS = {
     "LxF": 2,
     "KP07": 2,
-    "KP07_dimsplit": 5,
+    "KP07_dimsplit": 7,
     "HLL": 4,
     "EE2D_KP07_dimsplit": 4,
     "HLL2": 4,

@@ -2,9 +2,9 @@
 
 The reference runs one simulator per class instance, one kernel launch per
 substep.  A ``Batch`` holds many simulations of one scheme (any of the eight)
-resident in HBM and advances all of them with one persistent kernel per
-substep (one per Runge-Kutta stage for KP07) that walks a tile work list; the
-step sequence is replayed from CUDA graphs.  Each simulation
+resident in HBM and advances all of them with one kernel launch per substep
+(one per Runge-Kutta stage for KP07) over a device-resident tile work list;
+the step sequence is replayed from CUDA graphs.  Each simulation
 follows the reference's ``simulate(t_end)`` semantics on its own: its own CFL
 time step recomputed every 100 of its steps, its last step shortened to hit
 its t_end (GPUSimulators/Simulator.py:176-217).  Its result is therefore the
@@ -30,7 +30,7 @@ def _L():
 
 
 class Batch(object):
-    """Simulations of one scheme advanced together by a persistent kernel.
+    """Simulations of one scheme advanced together by one batched kernel launch per substep.
     ``order`` is KP07's Runge-Kutta order (1 or 2, GPUSimulators/KP07.py:62),
     the same for every simulation of the batch."""
 

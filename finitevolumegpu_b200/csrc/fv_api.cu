@@ -22,6 +22,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <utility>
 #include <vector>
 
 #include "../../include/fvgpu.h"
@@ -157,8 +158,9 @@ struct BEntry {
     int scheme;
     int W, H, NT;
     BatchFn fn;
+    bool persistent = false;  // resident CTAs striding over the work list (else one CTA per entry)
 };
-// Batched (persistent) kernels; the first entry of a scheme is its default.
+// Batched kernels; the first entry of a scheme is its default.
 const BEntry kBatchTable[] = {
     {FV_LXF, 60, 28, 128, fv::batched_stage_kernel<fv::LXF, 60, 28, 128>},
     {FV_LXF, 120, 28, 128, fv::batched_stage_kernel<fv::LXF, 120, 28, 128>},
@@ -189,6 +191,9 @@ const BEntry kBatchTable[] = {
     {FV_HLL2, 60, 60, 128, fv::batched_stage_kernel<fv::HLL2, 60, 60, 128, 0, 2>},
     {FV_WAF, 60, 60, 128, fv::batched_stage_kernel<fv::WAF, 60, 60, 128, 0, 2>},
     {FV_EE2D_KP07_DIMSPLIT, 60, 60, 128, fv::batched_stage_kernel<fv::EE2D, 60, 60, 128, 0, 2>},
+    // persistent forms of the KP07_dimsplit tiles (timed against the one-tile-per-CTA forms)
+    {FV_KP07_DIMSPLIT, 60, 60, 128, fv::batched_stage_kernel<fv::KP07_DIMSPLIT, 60, 60, 128, 0, 2, true>, true},
+    {FV_KP07_DIMSPLIT, 124, 28, 128, fv::batched_stage_kernel<fv::KP07_DIMSPLIT, 124, 28, 128, 0, 1, true>, true},
 };
 constexpr int kNumBatchEntries = sizeof(kBatchTable) / sizeof(kBatchTable[0]);
 
@@ -1278,11 +1283,12 @@ int fv_host_free(void* ptr) {
 
 // ====================================================================== batches
 //
-// A batch advances many simulations of one scheme together: the
-// persistent kernel walks a device-resident work list of (simulation, tile)
+// A batch advances many simulations of one scheme together: each launch of
+// the batched kernel covers a device-resident work list of (simulation, tile)
 // pairs, every simulation keeps its own control block (t, dt, t_end, buffer
 // parity), and graphs of 1 and 16 steps are captured once.  Adding or
-// removing a simulation rewrites the work list between graph replays.
+// removing a simulation rewrites the work list between graph replays and sets
+// the graphs' launch grid to its new length (one CTA per entry).
 
 struct fv_batch {
     fv_context* ctx = nullptr;
@@ -1315,8 +1321,12 @@ struct fv_batch {
     std::vector<void*> slot_mem;          // per-slot device allocation (planes + tile scratch)
     std::vector<size_t> slot_bytes;
     size_t bytes = 0;
-    int grid = 0;
+    // Graphs of 1 and 16 steps, kept with their executables so that the grid
+    // of their kernel nodes (one CTA per work-list entry) follows the list.
+    cudaGraph_t g1 = nullptr, g16 = nullptr;
     cudaGraphExec_t graph1 = nullptr, graph16 = nullptr;
+    int graph_grid = 0;  // grid the executables launch
+    int resident_grid = 0;  // CTAs resident on the GPU at once (the persistent form's grid)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0.0;
     // Guards the slot bookkeeping (used, done_at_sync, slot_mem, bytes, dirty,
@@ -1331,7 +1341,18 @@ namespace {
 void batch_drop_graphs(fv_batch* b) {
     if (b->graph1) cudaGraphExecDestroy(b->graph1);
     if (b->graph16) cudaGraphExecDestroy(b->graph16);
+    if (b->g1) cudaGraphDestroy(b->g1);
+    if (b->g16) cudaGraphDestroy(b->g16);
     b->graph1 = b->graph16 = nullptr;
+    b->g1 = b->g16 = nullptr;
+    b->graph_grid = 0;
+}
+
+// CTAs of one batched launch: one per entry of the published work list, or
+// for the persistent form every CTA the GPU holds at once.
+int batch_grid(const fv_batch* b) {
+    if (b->be->persistent) return b->resident_grid;
+    return b->nwork > 0 ? b->nwork : 1;
 }
 
 // 0 running, 1 reached t_end (simulate()'s stopping rule), 2 failed: a step
@@ -1358,13 +1379,15 @@ int batch_launch_step(fv_batch* b) {
         a.order = b->p.order;
         a.err = b->d_err;
         void* kargs[] = {&a};
-        FV_CK(launch_dependent(reinterpret_cast<const void*>(b->be->fn), dim3(b->grid), dim3(b->be->NT), kargs,
+        FV_CK(launch_dependent(reinterpret_cast<const void*>(b->be->fn), dim3(batch_grid(b)), dim3(b->be->NT), kargs,
                                batch_smem(*b->be), b->stream));
     }
     return FV_OK;
 }
 
-int batch_build_graph(fv_batch* b, int nsteps, cudaGraphExec_t* out) {
+// Captures nsteps steps into *graph and instantiates it into *out; the graph
+// is kept for batch_set_graph_grid.
+int batch_build_graph(fv_batch* b, int nsteps, cudaGraph_t* graph, cudaGraphExec_t* out) {
     cudaGraph_t g = nullptr;
     FV_CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     int rc = FV_OK;
@@ -1376,8 +1399,45 @@ int batch_build_graph(fv_batch* b, int nsteps, cudaGraphExec_t* out) {
     }
     if (e != cudaSuccess) return fail(FV_ERR_CUDA, "batch graph capture: %s", cudaGetErrorString(e));
     e = cudaGraphInstantiate(out, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) return fail(FV_ERR_CUDA, "batch graph instantiate: %s", cudaGetErrorString(e));
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return fail(FV_ERR_CUDA, "batch graph instantiate: %s", cudaGetErrorString(e));
+    }
+    *graph = g;
+    return FV_OK;
+}
+
+// Sets the grid of every kernel node of the executable graphs to the current
+// work list's length.  An update applies to later launches only; launches
+// already queued keep the grid (and, by stream order, the work list) they
+// were queued with.  If an update fails the graphs are dropped and rebuilt on
+// the next run.
+int batch_set_graph_grid(fv_batch* b) {
+    const int grid = batch_grid(b);
+    if (!b->graph1 || b->graph_grid == grid) return FV_OK;
+    const std::pair<cudaGraph_t, cudaGraphExec_t> graphs[2] = {{b->g1, b->graph1}, {b->g16, b->graph16}};
+    for (const auto& ge : graphs) {
+        size_t count = 0;
+        cudaError_t e = cudaGraphGetNodes(ge.first, nullptr, &count);
+        std::vector<cudaGraphNode_t> nodes(count);
+        if (e == cudaSuccess && count > 0) e = cudaGraphGetNodes(ge.first, nodes.data(), &count);
+        for (size_t i = 0; i < count && e == cudaSuccess; ++i) {
+            cudaGraphNodeType type;
+            e = cudaGraphNodeGetType(nodes[i], &type);
+            if (e != cudaSuccess || type != cudaGraphNodeTypeKernel) continue;
+            cudaKernelNodeParams kp;
+            e = cudaGraphKernelNodeGetParams(nodes[i], &kp);
+            if (e != cudaSuccess) break;
+            kp.gridDim = dim3(grid);
+            e = cudaGraphExecKernelNodeSetParams(ge.second, nodes[i], &kp);
+        }
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            batch_drop_graphs(b);
+            return FV_OK;
+        }
+    }
+    b->graph_grid = grid;
     return FV_OK;
 }
 
@@ -1473,7 +1533,7 @@ int fv_batch_create(fv_context* ctx, int scheme, const fv_params* params, int ma
     b->p = *params;
     b->be = be;
     b->max_inst = max_instances;
-    b->grid = per_sm * ctx->sm_count;
+    b->resident_grid = per_sm * ctx->sm_count;
     b->used.assign(max_instances, 0);
     b->slot_mem.assign(max_instances, nullptr);
     b->slot_bytes.assign(max_instances, 0);
@@ -1683,8 +1743,13 @@ int fv_batch_run(fv_batch* b, int n_steps) {
         FV_TRY(batch_publish(b));
         b->dirty = false;
     }
-    if (!b->graph1) FV_TRY(batch_build_graph(b, 1, &b->graph1));
-    if (!b->graph16) FV_TRY(batch_build_graph(b, 16, &b->graph16));
+    FV_TRY(batch_set_graph_grid(b));
+    if (!b->graph1 || !b->graph16) {
+        batch_drop_graphs(b);
+        FV_TRY(batch_build_graph(b, 1, &b->g1, &b->graph1));
+        FV_TRY(batch_build_graph(b, 16, &b->g16, &b->graph16));
+        b->graph_grid = batch_grid(b);
+    }
     FV_CK(cudaEventRecord(b->ev0, b->stream));
     int k = n_steps;
     while (k >= 16) {
@@ -1786,7 +1851,7 @@ int fv_batch_tile(fv_batch* b, int* tile_w, int* tile_h, int* threads, int* grid
     if (tile_w) *tile_w = b->be->W;
     if (tile_h) *tile_h = b->be->H;
     if (threads) *threads = b->be->NT;
-    if (grid) *grid = b->grid;
+    if (grid) *grid = batch_grid(b);
     return FV_OK;
 }
 

@@ -1261,8 +1261,8 @@ struct BatchArgs {
 
 // The part of a work item's records a batched tile reads before its load: the
 // first 48 bytes of the simulation's control block (read_step's words) and
-// the instance record up to its last field, prefetched into shared memory a
-// tile ahead (BatchTileMeta).
+// the instance record up to its last field, copied into shared memory by the
+// CTA's first threads (BatchTileMeta).
 constexpr int kInstPrefix = 144;
 static_assert(offsetof(BatchInstance, variant_beta) + sizeof(float) <= kInstPrefix &&
                   kInstPrefix % 16 == 0 && sizeof(BatchInstance) >= kInstPrefix && sizeof(SimCtl) % 16 == 0,
@@ -1284,91 +1284,113 @@ __device__ __forceinline__ void prefetch_tile_meta(BatchTileMeta& m, const Batch
     }
 }
 
-// Persistent stage kernel of any scheme (one dimensional sweep of the split
-// schemes, one RK stage of LxF and KP07): the CTAs walk the work list of all
-// tiles of all simulations of the batch; each simulation keeps its own t, dt (its own
-// CFL every 100 of its steps) and t_end, and its last tile finalises its
-// control block exactly as the single-simulation kernel does.  Simulations
-// that reached t_end are skipped.  The work list lives in device memory, so
-// one captured CUDA graph serves any batch composition.
+// One tile of a batched launch: work item `job` (simulation, tile within it),
+// whose control-block words and instance fields are in shared memory (M).
+// Simulations that reached t_end are skipped (uniformly across the CTA).
+template <int SCHEME, int W, int H, int NT, int VAR, int LPT>
+__device__ __forceinline__ void batched_tile(float* Qs, uint64_t* bar, const BatchTileMeta& M, int2 job,
+                                             const BatchArgs& B) {
+    constexpr int NV = (SCHEME == EE2D) ? 4 : 3;
+    const BatchInstance& I = *reinterpret_cast<const BatchInstance*>(M.inst);
+    SimCtl* const ctl = B.ctl + job.x;
+    StepCtl sc = step_from_words(M.ctl[0], M.ctl[1], M.ctl[2], false, 0.0f, false, B.is_last != 0);
+    if (!sc.active) return;
+    if (SCHEME == WAF) sc.do_cfl = false;
+    float my_cfl = __int_as_float(0x7f800000);
+    double my_sums[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) my_sums[v] = 0.0;
+    const bool sums = B.want_sums && B.is_last;
+    TileJob J;
+    J.tmap = nullptr;
+    J.in = I.buf[sc.cur];
+    J.out = I.buf[sc.cur ^ 1];
+    J.nx = I.nx;
+    J.ny = I.ny;
+    J.pitch = I.pitch;
+    J.bc = I.bc;
+    const int ty = job.y / I.tiles_x;
+    J.x0 = (job.y - ty * I.tiles_x) * W;
+    J.y0 = ty * H;
+    bool unhealthy = false;
+    if constexpr (SCHEME == LXF || SCHEME == KP07) {
+        const UnsplitPar P{I.dx, I.dy, I.g, I.theta, sc.dt * I.dt_scale, B.substep, B.order};
+        process_tile_unsplit<SCHEME, W, H, NT, true, true>(Qs, bar, 0, false, J, P, sc.do_cfl, sums, B.err, my_cfl,
+                                                           my_sums, kWaitPolls, B.is_last != 0, &unhealthy);
+    } else {
+        const SplitPar P{I.dx, I.dy, I.g, I.gamma, I.theta, sc.dt * I.dt_scale, B.substep, I.variant_beta};
+        process_tile_dimsplit<SCHEME, W, H, NT, true, VAR, LPT, true>(Qs, bar, 0, false, J, P, sc.do_cfl, sums,
+                                                                      B.err, my_cfl, my_sums, kWaitPolls,
+                                                                      B.is_last != 0, &unhealthy);
+    }
+    // ordered before this tile's arrival (tile_epilogue fences before it counts)
+    if (__syncthreads_or(unhealthy) && threadIdx.x == 0) atomicOr(&ctl->bad, 1);
+    tile_epilogue<NT, NV>(ctl, I.block_cfl, I.block_sums, job.y, I.ntiles, B.is_last != 0, false, sc, my_cfl,
+                          my_sums, sums);
+}
+
+// Stage kernel of any scheme over a batch (one dimensional sweep of the split
+// schemes, one RK stage of LxF and KP07): one launch covers the work list of
+// all tiles of all simulations of the batch; each simulation keeps its own t,
+// dt (its own CFL every 100 of its steps) and t_end, and its last tile
+// finalises its control block exactly as the single-simulation kernel does.
+// The work list and its length live in device memory, so one pair of captured
+// CUDA graphs serves any batch composition.  Two forms of the walk:
+//  * PERSIST = false: CTA w takes entry w; the host launches one CTA per entry
+//    and sets the grid of the graphs' kernel nodes to the list's length when
+//    the list changes.  The CTAs resident on an SM (four of 128 threads)
+//    overlap one tile's metadata and tile loads with the others' sweeps, as
+//    in the single-simulation kernels.
+//  * PERSIST = true: a fixed grid of resident CTAs (occupancy x SMs) strides
+//    over the list, copying the next tile's metadata into shared memory while
+//    the current tile is computed.  Inside that loop the compiler keeps far
+//    more registers live for the same sweeps (242 against 122 for the packed
+//    60 x 60 tile, 184 against 80 for the one-line 124 x 28), so under the
+//    128-register bound the packed form spills; on config-4 mixes the
+//    one-tile form measured 14-49 % faster per scheme, and the autotuner
+//    times both.
 // At most 128 registers per thread (the launch bound), so that four 128-thread
 // (two 256-thread) CTAs fit an SM as their shared tiles allow.
-template <int SCHEME, int W, int H, int NT, int VAR = 0, int LPT = 1>
+template <int SCHEME, int W, int H, int NT, int VAR = 0, int LPT = 1, bool PERSIST = false>
 __global__ void __launch_bounds__(NT, 65536 / (NT * 128)) batched_stage_kernel(const __grid_constant__ BatchArgs B) {
-    constexpr int NV = (SCHEME == EE2D) ? 4 : 3;
-    static_assert(NT >= 3 + kInstPrefix / 16, "one thread per prefetched 16-byte chunk");
+    static_assert(NT >= 3 + kInstPrefix / 16, "one thread per copied 16-byte chunk");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     float* Qs = reinterpret_cast<float*>(smem_raw);
     __shared__ __align__(8) uint64_t bar;
-    __shared__ BatchTileMeta meta[2];
+    __shared__ BatchTileMeta meta[PERSIST ? 2 : 1];
     grid_dependency_wait();  // the previous substep's states and control blocks
     const int n = *B.nwork;
-    const int G = gridDim.x;
-    // Tile prologue latency: the work list is read two tiles ahead, and the
-    // next tile's control-block words and instance fields are copied into
-    // shared memory while this tile is computed, so a tile's load can be
-    // issued as soon as the previous tile is done.  A control block read
-    // early holds the values of this launch's start: it changes in this
-    // launch only once every tile of its simulation has arrived, and the
-    // prefetched tile has not.
     int w = blockIdx.x;
     if (w >= n) return;
     int2 job = B.work[w];
-    int2 next = (w + G < n) ? B.work[w + G] : job;
-    prefetch_tile_meta(meta[0], B.inst, B.ctl, job);
-    cp_async_wait_all();
-    __syncthreads();
-    int slot = 0;
-    for (; w < n; w += G) {
-        const int2 next2 = (w + 2 * G < n) ? B.work[w + 2 * G] : next;
-        if (w + G < n) prefetch_tile_meta(meta[slot ^ 1], B.inst, B.ctl, next);
-        const BatchTileMeta& M = meta[slot];
-        const BatchInstance& I = *reinterpret_cast<const BatchInstance*>(M.inst);
-        SimCtl* const ctl = B.ctl + job.x;
-        StepCtl sc = step_from_words(M.ctl[0], M.ctl[1], M.ctl[2], false, 0.0f, false, B.is_last != 0);
-        if (sc.active) {  // uniform across the CTA
-            if (SCHEME == WAF) sc.do_cfl = false;
-            float my_cfl = __int_as_float(0x7f800000);
-            double my_sums[NV];
-#pragma unroll
-            for (int v = 0; v < NV; ++v) my_sums[v] = 0.0;
-            const bool sums = B.want_sums && B.is_last;
-            TileJob J;
-            J.tmap = nullptr;
-            J.in = I.buf[sc.cur];
-            J.out = I.buf[sc.cur ^ 1];
-            J.nx = I.nx;
-            J.ny = I.ny;
-            J.pitch = I.pitch;
-            J.bc = I.bc;
-            const int ty = job.y / I.tiles_x;
-            J.x0 = (job.y - ty * I.tiles_x) * W;
-            J.y0 = ty * H;
-            bool unhealthy = false;
-            if constexpr (SCHEME == LXF || SCHEME == KP07) {
-                const UnsplitPar P{I.dx, I.dy, I.g, I.theta, sc.dt * I.dt_scale, B.substep, B.order};
-                process_tile_unsplit<SCHEME, W, H, NT, true, true>(Qs, &bar, 0, false, J, P, sc.do_cfl, sums, B.err,
-                                                                   my_cfl, my_sums, kWaitPolls, B.is_last != 0,
-                                                                   &unhealthy);
-            } else {
-                const SplitPar P{I.dx, I.dy, I.g, I.gamma, I.theta, sc.dt * I.dt_scale, B.substep, I.variant_beta};
-                process_tile_dimsplit<SCHEME, W, H, NT, true, VAR, LPT, true>(Qs, &bar, 0, false, J, P, sc.do_cfl,
-                                                                              sums, B.err, my_cfl, my_sums,
-                                                                              kWaitPolls, B.is_last != 0,
-                                                                              &unhealthy);
-            }
-            // ordered before this tile's arrival (tile_epilogue fences before it counts)
-            if (__syncthreads_or(unhealthy) && threadIdx.x == 0) atomicOr(&ctl->bad, 1);
-            tile_epilogue<NT, NV>(ctl, I.block_cfl, I.block_sums, job.y, I.ntiles, B.is_last != 0, false, sc,
-                                  my_cfl, my_sums, sums);
-        }
-        // the next tile's metadata has landed and every thread is done with
-        // this slot, which the tile after next overwrites
+    if constexpr (!PERSIST) {
+        prefetch_tile_meta(meta[0], B.inst, B.ctl, job);
         cp_async_wait_all();
         __syncthreads();
-        slot ^= 1;
-        job = next;
-        next = next2;
+        batched_tile<SCHEME, W, H, NT, VAR, LPT>(Qs, &bar, meta[0], job, B);
+    } else {
+        // The work list is read two tiles ahead.  A control block read early
+        // holds the values of this launch's start: it changes in this launch
+        // only once every tile of its simulation has arrived, and the
+        // prefetched tile has not.
+        const int G = gridDim.x;
+        int2 next = (w + G < n) ? B.work[w + G] : job;
+        prefetch_tile_meta(meta[0], B.inst, B.ctl, job);
+        cp_async_wait_all();
+        __syncthreads();
+        int slot = 0;
+        for (; w < n; w += G) {
+            const int2 next2 = (w + 2 * G < n) ? B.work[w + 2 * G] : next;
+            if (w + G < n) prefetch_tile_meta(meta[slot ^ 1], B.inst, B.ctl, next);
+            batched_tile<SCHEME, W, H, NT, VAR, LPT>(Qs, &bar, meta[slot], job, B);
+            // the next tile's metadata has landed and every thread is done with
+            // this slot, which the tile after next overwrites
+            cp_async_wait_all();
+            __syncthreads();
+            slot ^= 1;
+            job = next;
+            next = next2;
+        }
     }
 }
 

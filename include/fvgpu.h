@@ -225,7 +225,8 @@ FV_API int fv_batch_add(fv_batch* batch, int nx, int ny, float dx, float dy, int
                         int host_rows, int host_cols, double t_end, int* slot);
 FV_API int fv_batch_remove(fv_batch* batch, int slot);
 /* Queues n_steps steps for every simulation of the batch (CUDA graphs of the
- * persistent kernel); simulations that reached t_end do nothing. Asynchronous.
+ * batched kernel, one launch per substep over the tile work list);
+ * simulations that reached t_end do nothing. Asynchronous.
  * Simulations admitted or removed since the last run join or leave the tile
  * work list first; FV_ERR_NOMEM means the list could not grow, nothing was
  * queued and the batch is unchanged (a later call retries). */
@@ -245,7 +246,9 @@ FV_API int fv_batch_download(fv_batch* batch, int slot, int var, float* host, in
 /* Device bytes held, simulations in the batch, work-list length, device time
  * of the last fv_batch_run (ms, valid after fv_batch_sync). */
 FV_API int fv_batch_info(fv_batch* batch, size_t* device_bytes, int* active, int* work_items, double* last_run_ms);
-/* Tile shape, threads per CTA and persistent grid size of the batch's kernel. */
+/* Tile shape, threads per CTA and CTAs per launch of the batch's kernel (one
+ * per tile of the last published work list, or the resident grid of a
+ * persistent tile configuration). */
 FV_API int fv_batch_tile(fv_batch* batch, int* tile_w, int* tile_h, int* threads, int* grid);
 
 /* One KP07_dimsplit substep that allocates no memory, for callers that may
