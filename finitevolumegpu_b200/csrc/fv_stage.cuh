@@ -1346,9 +1346,9 @@ __device__ __forceinline__ void batched_tile(float* Qs, uint64_t* bar, const Bat
 //    the current tile is computed.  Inside that loop the compiler keeps far
 //    more registers live for the same sweeps (242 against 122 for the packed
 //    60 x 60 tile, 184 against 80 for the one-line 124 x 28), so under the
-//    128-register bound the packed form spills; on config-4 mixes the
-//    one-tile form measured 14-49 % faster per scheme, and the autotuner
-//    times both.
+//    128-register bound the packed form spills; on mixes of 128 grids with
+//    sides of 64 to 1024 cells the one-tile form measured 14-49 % faster per
+//    scheme, and the autotuner times both.
 // At most 128 registers per thread (the launch bound), so that four 128-thread
 // (two 256-thread) CTAs fit an SM as their shared tiles allow.
 template <int SCHEME, int W, int H, int NT, int VAR = 0, int LPT = 1, bool PERSIST = false>
