@@ -1851,7 +1851,10 @@ int fv_batch_tile(fv_batch* b, int* tile_w, int* tile_h, int* threads, int* grid
     if (tile_w) *tile_w = b->be->W;
     if (tile_h) *tile_h = b->be->H;
     if (threads) *threads = b->be->NT;
-    if (grid) *grid = batch_grid(b);
+    if (grid) {
+        std::lock_guard<std::mutex> lock(b->mu);  // nwork changes when the list is republished
+        *grid = batch_grid(b);
+    }
     return FV_OK;
 }
 
